@@ -1,0 +1,214 @@
+/*
+ * lightbaker-b200 C ABI.
+ *
+ * The drop-in seam for the bake passes of lightbaker: every function below replaces one piece of
+ * the reference's `gpu::Gpu` boundary (crates/lightbaker/src/gpu/mod.rs) or of the bake entry point
+ * built on it (crates/lightbaker/src/bake.rs, crates/lightbaker/src/lib.rs). Plain C types only:
+ * pointers, sizes and the POD records the reference's shader reads, byte for byte.
+ *
+ * Conventions (mirroring the reference's anyhow::Result):
+ *   - functions returning `int` give LB_OK (0) on success and a negative LB_E* code on failure;
+ *     functions returning a handle give NULL on failure. Either way `lb_last_error()` holds a
+ *     message for the calling thread.
+ *   - the caller owns every host buffer passed in; it is only borrowed for the call.
+ *   - a handle is used from one thread at a time (the reference drives its Gpu from the bake thread).
+ */
+#ifndef LIGHTBAKER_H
+#define LIGHTBAKER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- records the passes read and write (sizes and field order are the reference's) ---- */
+
+/* BVH node, 32 bytes: crates/lightbaker/src/bvh.rs:12-22. count 0: inner node whose children are
+ * `first` and `first + 1`; count > 0: leaf of `count` triangles from `first`. */
+typedef struct lb_node {
+    float min[3];
+    uint32_t first;
+    float max[3];
+    uint32_t count;
+} lb_node;
+
+/* Triangle, 48 bytes: crates/lightbaker/src/bvh.rs:24-33. v0.w: material index bits;
+ * e1.w: chart index bits (0xffffffff: none). */
+typedef struct lb_tri {
+    float v0[4];
+    float e1[4];
+    float e2[4];
+} lb_tri;
+
+/* Texel (or probe), 64 bytes: crates/lightbaker/src/raster.rs:11-22. pos.w: 1 where covered;
+ * normal.w: chart index bits (a probe: its index in the volume). */
+typedef struct lb_texel {
+    float pos[4];
+    float normal[4];
+    float dx[4];
+    float dy[4];
+} lb_texel;
+
+/* The passes' uniform block, 144 bytes: crates/lightbaker/src/gpu/mod.rs:11-23 and
+ * crates/lightbaker/src/gpu/trace.wgsl:12-22. */
+typedef struct lb_params {
+    float sun_dir[4];   /* xyz towards the sun, w: tan of the disc's radius */
+    float sun_irr[4];
+    float zenith[4];
+    float horizon[4];
+    float ground[4];    /* w: reach of the inside-a-solid test (m) */
+    float fallback[4];
+    uint32_t counts[4]; /* sun grid side, ao rays, gather rays, items in this batch */
+    float reach[4];     /* ao reach, gather reach, lift, seed bits */
+    uint32_t atlas[4];  /* atlas width, height, first item, insideShare bits */
+} lb_params;
+
+/* crates/lightbaker/src/gpu/mod.rs:26-33; the result width is 1, 1 and 4 records a item. */
+enum lb_pass { LB_PASS_DIRECT = 0, LB_PASS_GATHER = 1, LB_PASS_VOLUME = 2 };
+
+enum lb_status {
+    LB_OK = 0,
+    LB_EINVAL = -1,    /* bad argument */
+    LB_ENODEV = -2,    /* no CUDA device ("no GPU adapter", gpu/mod.rs:83) */
+    LB_ECUDA = -3,     /* a CUDA call failed */
+    LB_ENOMEM = -4,    /* device memory */
+    LB_ETIMEOUT = -5,  /* a bounded device wait ran out (persistent kernels) */
+    LB_EIO = -6,       /* file or format error */
+    LB_ESCRATCH = -7   /* request larger than a fixed scratch area */
+};
+
+typedef struct lb_gpu lb_gpu;
+typedef struct lb_scene lb_scene;
+
+/* Message for the last failure on this thread ("" if none). */
+const char *lb_last_error(void);
+
+/* Gpu::new (gpu/mod.rs:74-127): opens CUDA device `device` (an sm_100 part) and writes its name
+ * (the reference's `pub adapter: String`, gpu/mod.rs:62) into name[0..cap). */
+lb_gpu *lb_gpu_open(int device, char *name, size_t cap);
+void lb_gpu_close(lb_gpu *gpu);
+
+/* Gpu::scene (gpu/mod.rs:129-136): uploads the BVH, the materials (albedo rgb, opacity) and the
+ * charts' affine rows (two float4 a chart). Empty charts: a one-chart dummy, as the reference. */
+lb_scene *lb_scene_upload(lb_gpu *gpu, const lb_node *nodes, size_t n_nodes, const lb_tri *tris,
+                          size_t n_tris, const float *materials /* 4 a material */, size_t n_materials,
+                          const float *charts /* 8 a chart */, size_t n_charts);
+void lb_scene_free(lb_scene *scene);
+
+/* Gpu::run (gpu/mod.rs:140-196): runs `pass` over `n` items, reading `light` (4 floats an atlas
+ * texel; may be empty), writing n * width float4 records into the caller's `out` (width 4 for
+ * LB_PASS_VOLUME, else 1). params->counts[3] and atlas[2] are set per batch as the reference does. */
+int lb_run(lb_gpu *gpu, lb_scene *scene, int pass, const lb_params *params, const lb_texel *items,
+           size_t n, const float *light, size_t n_light, float *out);
+
+/* Rays traced and BVH work done by the last lb_run (or bake) on this handle, counted on the device
+ * when counting is on (lb_set_counting). rays: every trace() call; nodes: node records fetched;
+ * tris: triangles tested; mats: material records read by accepted candidates. */
+typedef struct lb_counters {
+    uint64_t rays, nodes, tris, mats;
+} lb_counters;
+int lb_set_counting(lb_gpu *gpu, int on);
+int lb_get_counters(lb_gpu *gpu, lb_counters *out);
+
+/* The handle's CUDA stream (a cudaStream_t), on which every pass is enqueued. No counterpart in the
+ * reference (wgpu hides its queue); it lets a caller order its own work and events with the passes. */
+void *lb_gpu_stream(lb_gpu *gpu);
+/* Waits for the handle's stream, then moves the last pass's counters into lb_get_counters. */
+int lb_gpu_sync(lb_gpu *gpu);
+/* Gpu::run on items already in device memory: `items`, `light` and `out` are device pointers; the pass
+ * is enqueued on the handle's stream and not waited for. `base` is the index of items[0] in the whole
+ * list (it keys the sample sequence, as the shader's P.atlas.z + i). */
+int lb_run_async(lb_gpu *gpu, lb_scene *scene, int pass, const lb_params *params, const lb_texel *items,
+                 size_t n, uint32_t base, const float *light, size_t n_light, float *out);
+/* Bytes this handle copied host to device and device to host since the last reset. */
+int lb_get_transfer(lb_gpu *gpu, uint64_t *h2d, uint64_t *d2h, int reset);
+
+
+/* ---- the host pipeline (crates/lightbaker/src/bake.rs, lib.rs) ---- */
+
+/* A scene read and laid out, with everything the passes read: the reference's steps before its
+ * first Gpu::run (bake.rs:94-120): Scene::read (scene.rs:140-161), Layout::build, each chart's affine,
+ * Bvh::build, the materials and the Params. */
+typedef struct lb_prepared lb_prepared;
+lb_prepared *lb_prepare(const uint8_t *scene, size_t len);
+void lb_prepared_free(lb_prepared *p);
+
+typedef struct lb_prepared_info {
+    size_t n_nodes, n_tris, n_materials, n_charts, n_tiles, n_triangles;
+    uint32_t atlas_width, atlas_height, indirect_downscale, padding;
+    uint32_t gi_bounces, has_volume;
+    lb_params params;
+} lb_prepared_info;
+int lb_prepared_get_info(const lb_prepared *p, lb_prepared_info *out);
+/* Copies of the prepared arrays (caller-allocated, sized from the info). */
+int lb_prepared_get_bvh(const lb_prepared *p, lb_node *nodes, lb_tri *tris);
+int lb_prepared_get_materials(const lb_prepared *p, float *materials /* 4 a material */);
+int lb_prepared_get_charts(const lb_prepared *p, float *charts /* 8 a chart */);
+/* Tile t's rectangle (x, y, w, h in the atlas) and key. */
+int lb_prepared_get_tile(const lb_prepared *p, size_t t, uint32_t rect[4], int32_t key[2]);
+/* raster.rs:39-100: tile t's texels (w * h records, row by row). */
+int lb_prepared_rasterize(const lb_prepared *p, size_t t, lb_texel *out);
+
+/* A pass runner the bake can use in place of a device (the reference's `bake(scene, &Gpu, …)`
+ * takes its device the same way): upload the scene, then run passes. Return 0 on success. */
+typedef struct lb_tracer {
+    void *ctx;
+    int (*scene)(void *ctx, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+                 const float *materials, size_t n_materials, const float *charts, size_t n_charts);
+    int (*run)(void *ctx, int pass, const lb_params *params, const lb_texel *items, size_t n,
+               const float *light, size_t n_light, float *out, uint64_t *rays);
+} lb_tracer;
+
+typedef struct lb_bake_options {
+    const char *cache_dir;                      /* NULL: no cache (bake.rs:30-34) */
+    void (*log)(void *ctx, const char *line);   /* NULL: quiet */
+    void *log_ctx;
+} lb_bake_options;
+
+typedef struct lb_bake lb_bake;
+/* bake() (bake.rs:94-432) with the passes on `gpu`. */
+lb_bake *lb_bake_run(lb_gpu *gpu, const uint8_t *scene, size_t len, const lb_bake_options *opts);
+/* The same with the passes on a caller's runner. */
+lb_bake *lb_bake_run_with(const lb_tracer *tracer, const uint8_t *scene, size_t len, const lb_bake_options *opts);
+void lb_bake_free(lb_bake *b);
+
+typedef struct lb_bake_info {
+    uint32_t width, height, indirect_width, indirect_height;
+    uint32_t has_volume, volume_size[3];
+    float volume_origin[3], volume_step;
+    uint64_t tiles, tiles_baked, texels_baked, chunks, chunks_baked;
+    double seconds;
+    uint64_t rays_direct, rays_gather, rays_volume;
+    double t_layout, t_direct, t_bounces, t_volume, t_composite;
+    uint64_t n_charts, n_triangles;
+} lb_bake_info;
+int lb_bake_get_info(const lb_bake *b, lb_bake_info *out);
+int lb_bake_get_direct(const lb_bake *b, float *out /* 2 an atlas texel: field, ao */);
+int lb_bake_get_indirect(const lb_bake *b, float *out /* 3 a texel of the smaller atlas */);
+int lb_bake_get_validity(const lb_bake *b, uint8_t *out);
+int lb_bake_get_volume(const lb_bake *b, float *out /* 16 a probe */);
+/* The layout the bake used: each chart's affine rows (8 floats a chart, layout.rs:76-85) and each
+ * scene triangle's chart (meshes in order, 0xffffffff: none; layout.rs:64-65). */
+int lb_bake_get_charts(const lb_bake *b, float *out);
+int lb_bake_get_tri_charts(const lb_bake *b, uint32_t *out);
+/* output::write (output.rs:95-154): the .lbake file. *out is malloc'd; free with lb_free. */
+int lb_bake_write(const lb_bake *b, uint8_t **out, size_t *len);
+void lb_free(void *p);
+
+/* Scene::write (scene.rs:164-181) from a JSON header and positions: for tools and tests that make
+ * scenes. header_json is the header as the file holds it. */
+int lb_scene_encode(const char *header_json, const float *const *positions, const size_t *n_floats,
+                    size_t n_meshes, uint8_t **out, size_t *len);
+/* blake3 of a byte string (the hash the cache is keyed by), 32 bytes. */
+void lb_blake3(const uint8_t *data, size_t len, uint8_t out[32]);
+/* encode.rs: RGB9E5 and BC4 blocks, for format tests. */
+uint32_t lb_rgb9e5(const float c[3]);
+void lb_rgb9e5_decode(uint32_t p, float out[3]);
+void lb_bc4_block(const uint8_t v[16], uint8_t out[8]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,354 @@
+"""lightbaker-b200: the bake passes of lightbaker (sun shadows as a distance field, ambient occlusion,
+bounced light, an L1 irradiance volume) on B200, behind the reference's own `Gpu` boundary.
+
+The Python surface mirrors the reference crate's (crates/lightbaker/src/lib.rs:8-23):
+
+    gpu = Gpu.new()                                  # gpu/mod.rs:74
+    buffers = gpu.scene(nodes, tris, materials, charts)   # gpu/mod.rs:129
+    out = gpu.run(Pass.DIRECT, buffers, params, texels, light)   # gpu/mod.rs:140
+    baked = bake(scene_bytes, gpu, cache=..., log=print)      # bake.rs:94
+    baked.write()                                    # output.rs:95
+
+Everything runs in the native library (lightbaker_b200/liblightbaker_b200.so): CUDA kernels for the
+passes, C++ for the host pipeline. Importing this package without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import json
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from ._native import NODE, TEXEL, TRI, LightbakerError, Params
+
+__all__ = ["Pass", "Gpu", "SceneBuffers", "Prepared", "prepare", "bake", "Bake", "encode_scene", "blake3",
+           "rgb9e5", "rgb9e5_decode", "bc4_block", "Params", "NODE", "TRI", "TEXEL", "LightbakerError"]
+
+
+class Pass(enum.IntEnum):
+    """crates/lightbaker/src/gpu/mod.rs:26-33"""
+    DIRECT = 0
+    GATHER = 1
+    VOLUME = 2
+
+    @property
+    def width(self) -> int:
+        return 4 if self == Pass.VOLUME else 1
+
+
+class SceneBuffers:
+    """The scene as the passes read it, on the device (gpu/mod.rs:65-71)."""
+
+    def __init__(self, handle: int, gpu: "Gpu"):
+        self._h = handle
+        self._gpu = gpu
+
+    def close(self) -> None:
+        if self._h:
+            N.lib().lb_scene_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Gpu:
+    """One CUDA device (gpu/mod.rs:57-63). `adapter` names it."""
+
+    def __init__(self, handle: int, adapter: str):
+        self._h = handle
+        self.adapter = adapter
+
+    @staticmethod
+    def new(device: int = 0) -> "Gpu":
+        buf = C.create_string_buffer(256)
+        h = N.lib().lb_gpu_open(device, buf, 256)
+        if not h:
+            raise LightbakerError(N.last_error())
+        return Gpu(h, buf.value.decode())
+
+    def close(self) -> None:
+        if self._h:
+            N.lib().lb_gpu_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def scene(self, nodes: np.ndarray, tris: np.ndarray, materials: np.ndarray, charts: np.ndarray) -> SceneBuffers:
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        tris = np.ascontiguousarray(tris, dtype=TRI)
+        materials = np.ascontiguousarray(materials, dtype=np.float32).reshape(-1, 4)
+        charts = np.ascontiguousarray(charts, dtype=np.float32).reshape(-1, 8)
+        h = N.lib().lb_scene_upload(self._h, N.ptr(nodes), len(nodes), N.ptr(tris), len(tris), N.ptr(materials),
+                                    len(materials), N.ptr(charts) if len(charts) else None, len(charts))
+        if not h:
+            raise LightbakerError(N.last_error())
+        return SceneBuffers(h, self)
+
+    def run(self, pass_: Pass, scene: SceneBuffers, params: Params, texels: np.ndarray,
+            light: np.ndarray | None = None) -> np.ndarray:
+        """Each item's results: an (n * width, 4) float32 array (gpu/mod.rs:140-196)."""
+        pass_ = Pass(pass_)
+        texels = np.ascontiguousarray(texels, dtype=TEXEL)
+        n = len(texels)
+        out = np.zeros((n * pass_.width, 4), dtype=np.float32)
+        if light is None or len(light) == 0:
+            light_arr, nl = None, 0
+        else:
+            light_arr = np.ascontiguousarray(light, dtype=np.float32).reshape(-1, 4)
+            nl = len(light_arr)
+        N.check(N.lib().lb_run(self._h, scene._h, int(pass_), C.byref(params), N.ptr(texels), n,
+                               N.ptr(light_arr), nl, N.ptr(out)), "GPU")
+        return out
+
+    @property
+    def stream(self) -> int:
+        """The handle's cudaStream_t, as an integer (every pass is enqueued on it)."""
+        return N.lib().lb_gpu_stream(self._h) or 0
+
+    def sync(self) -> None:
+        N.check(N.lib().lb_gpu_sync(self._h), "lb_gpu_sync")
+
+    def run_async(self, pass_: Pass, scene: SceneBuffers, params: Params, items_ptr: int, n: int, base: int,
+                  light_ptr: int, n_light: int, out_ptr: int) -> None:
+        """A pass over device-resident items (device pointers), enqueued on `stream`, not waited for."""
+        N.check(N.lib().lb_run_async(self._h, scene._h, int(pass_), C.byref(params), C.c_void_p(items_ptr), n,
+                                     base, C.c_void_p(light_ptr), n_light, C.c_void_p(out_ptr)), "GPU")
+
+    def transfer(self, reset: bool = False) -> tuple:
+        """(host-to-device bytes, device-to-host bytes) this handle copied."""
+        h, d = C.c_uint64(), C.c_uint64()
+        N.check(N.lib().lb_get_transfer(self._h, C.byref(h), C.byref(d), int(reset)), "lb_get_transfer")
+        return h.value, d.value
+
+    def set_counting(self, on: bool) -> None:
+        N.check(N.lib().lb_set_counting(self._h, int(on)), "lb_set_counting")
+
+    def counters(self) -> dict:
+        c = N.Counters()
+        N.check(N.lib().lb_get_counters(self._h, C.byref(c)), "lb_get_counters")
+        return {"rays": c.rays, "nodes": c.nodes, "tris": c.tris, "mats": c.mats}
+
+
+class Prepared:
+    """A scene read and laid out with the BVH, materials, charts and Params the passes read
+    (bake.rs:94-120)."""
+
+    def __init__(self, scene: bytes):
+        self._h = N.lib().lb_prepare(scene, len(scene))
+        if not self._h:
+            raise LightbakerError(N.last_error())
+        info = N.PreparedInfo()
+        N.check(N.lib().lb_prepared_get_info(self._h, C.byref(info)), "lb_prepared_get_info")
+        self.info = info
+        self.params = info.params.copy()
+        self.nodes = np.zeros(info.n_nodes, NODE)
+        self.tris = np.zeros(info.n_tris, TRI)
+        N.check(N.lib().lb_prepared_get_bvh(self._h, N.ptr(self.nodes), N.ptr(self.tris)), "bvh")
+        self.materials = np.zeros((info.n_materials, 4), np.float32)
+        if info.n_materials:
+            N.check(N.lib().lb_prepared_get_materials(self._h, N.ptr(self.materials)), "materials")
+        self.charts = np.zeros((info.n_charts, 8), np.float32)
+        if info.n_charts:
+            N.check(N.lib().lb_prepared_get_charts(self._h, N.ptr(self.charts)), "charts")
+        self.tiles = []
+        for t in range(info.n_tiles):
+            rect = (C.c_uint32 * 4)()
+            key = (C.c_int32 * 2)()
+            N.check(N.lib().lb_prepared_get_tile(self._h, t, rect, key), "tile")
+            self.tiles.append({"x": rect[0], "y": rect[1], "w": rect[2], "h": rect[3], "key": (key[0], key[1])})
+
+    def rasterize(self, t: int) -> np.ndarray:
+        """raster.rs:39-100: tile t's texels, (h, w) records."""
+        tile = self.tiles[t]
+        out = np.zeros(tile["w"] * tile["h"], TEXEL)
+        N.check(N.lib().lb_prepared_rasterize(self._h, t, N.ptr(out)), "rasterize")
+        return out.reshape(tile["h"], tile["w"])
+
+    def covered_texels(self, tiles=None) -> np.ndarray:
+        """The direct pass's items: every covered texel of the given tiles, in tile order then row-major
+        (bake.rs:149)."""
+        parts = []
+        for t in range(len(self.tiles)) if tiles is None else tiles:
+            tx = self.rasterize(t).reshape(-1)
+            parts.append(tx[tx["pos"][:, 3] > 0.5])
+        return np.concatenate(parts) if parts else np.zeros(0, TEXEL)
+
+    def close(self):
+        if self._h:
+            N.lib().lb_prepared_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def prepare(scene: bytes) -> Prepared:
+    return Prepared(scene)
+
+
+@dataclass
+class Stats:
+    tiles: int
+    tiles_baked: int
+    texels_baked: int
+    chunks: int
+    chunks_baked: int
+    seconds: float
+    rays_direct: int
+    rays_gather: int
+    rays_volume: int
+    t_layout: float
+    t_direct: float
+    t_bounces: float
+    t_volume: float
+    t_composite: float
+
+    @property
+    def rays(self) -> int:
+        return self.rays_direct + self.rays_gather + self.rays_volume
+
+
+class Bake:
+    """A bake's results (bake.rs:36-47): `direct` (h, w, 2) field and occlusion, `indirect` (ih, iw, 3),
+    `validity` (h, w), `volume` (probes, 4, 4) or None, `stats`."""
+
+    def __init__(self, handle: int):
+        self._h = handle
+        info = N.BakeInfo()
+        N.check(N.lib().lb_bake_get_info(handle, C.byref(info)), "lb_bake_get_info")
+        self.info = info
+        w, h, iw, ih = info.width, info.height, info.indirect_width, info.indirect_height
+        self.width, self.height, self.indirect_size = w, h, (iw, ih)
+        self.direct = np.zeros((h, w, 2), np.float32)
+        N.check(N.lib().lb_bake_get_direct(handle, N.ptr(self.direct)), "direct")
+        self.indirect = np.zeros((ih, iw, 3), np.float32)
+        N.check(N.lib().lb_bake_get_indirect(handle, N.ptr(self.indirect)), "indirect")
+        self.validity = np.zeros((h, w), np.uint8)
+        N.check(N.lib().lb_bake_get_validity(handle, N.ptr(self.validity)), "validity")
+        self.volume = None
+        if info.has_volume:
+            nx, ny, nz = info.volume_size
+            self.volume = np.zeros((nx * ny * nz, 4, 4), np.float32)
+            N.check(N.lib().lb_bake_get_volume(handle, N.ptr(self.volume)), "volume")
+            self.volume_size = (nx, ny, nz)
+            self.volume_origin = tuple(info.volume_origin)
+            self.volume_step = info.volume_step
+        self.charts = np.zeros((info.n_charts, 8), np.float32)
+        if info.n_charts:
+            N.check(N.lib().lb_bake_get_charts(handle, N.ptr(self.charts)), "charts")
+        self.tri_charts = np.zeros(info.n_triangles, np.uint32)
+        if info.n_triangles:
+            N.check(N.lib().lb_bake_get_tri_charts(handle, N.ptr(self.tri_charts)), "triangle charts")
+        self.stats = Stats(info.tiles, info.tiles_baked, info.texels_baked, info.chunks, info.chunks_baked,
+                           info.seconds, info.rays_direct, info.rays_gather, info.rays_volume, info.t_layout,
+                           info.t_direct, info.t_bounces, info.t_volume, info.t_composite)
+
+    def write(self) -> bytes:
+        """The .lbake file (output.rs:95-154)."""
+        p = C.POINTER(C.c_uint8)()
+        n = C.c_size_t()
+        N.check(N.lib().lb_bake_write(self._h, C.byref(p), C.byref(n)), "lb_bake_write")
+        try:
+            return C.string_at(p, n.value)
+        finally:
+            N.lib().lb_free(p)
+
+    def close(self):
+        if self._h:
+            N.lib().lb_bake_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _options(cache, log):
+    opts = N.BakeOptions()
+    opts.cache_dir = str(cache).encode() if cache else None
+    keep = None
+    if log is not None:
+        keep = N.LOG_CB(lambda ctx, line: log(line.decode("utf-8", "replace")))
+        opts.log = keep
+    return opts, keep
+
+
+def bake(scene: bytes, gpu: Gpu, cache=None, log=None) -> Bake:
+    """bake() (bake.rs:94-432): the whole bake with the passes on `gpu`."""
+    opts, keep = _options(cache, log)
+    h = N.lib().lb_bake_run(gpu.handle, scene, len(scene), C.byref(opts))
+    del keep
+    if not h:
+        raise LightbakerError(N.last_error())
+    return Bake(h)
+
+
+def bake_with(scene: bytes, tracer: "N.Tracer", cache=None, log=None) -> Bake:
+    """The same bake with the passes on a caller's runner (an lb_tracer)."""
+    opts, keep = _options(cache, log)
+    h = N.lib().lb_bake_run_with(C.byref(tracer), scene, len(scene), C.byref(opts))
+    del keep
+    if not h:
+        raise LightbakerError(N.last_error())
+    return Bake(h)
+
+
+def encode_scene(header: dict, positions: list) -> bytes:
+    """Scene::write (scene.rs:164-181): an .lbscene from a header (the JSON object, camelCase keys) and
+    each mesh's positions (float32, three vertices a triangle). The file is read back to validate it."""
+    head = json.dumps(header, separators=(",", ":")).encode()
+    arrs = [np.ascontiguousarray(p, dtype=np.float32).reshape(-1) for p in positions]
+    ptrs = (C.c_void_p * max(1, len(arrs)))(*[a.ctypes.data for a in arrs])
+    counts = (C.c_size_t * max(1, len(arrs)))(*[a.size for a in arrs])
+    p = C.POINTER(C.c_uint8)()
+    n = C.c_size_t()
+    N.check(N.lib().lb_scene_encode(head, ptrs, counts, len(arrs), C.byref(p), C.byref(n)), "scene")
+    try:
+        return C.string_at(p, n.value)
+    finally:
+        N.lib().lb_free(p)
+
+
+def blake3(data: bytes) -> bytes:
+    out = (C.c_uint8 * 32)()
+    N.lib().lb_blake3(data, len(data), out)
+    return bytes(out)
+
+
+def rgb9e5(c) -> int:
+    a = (C.c_float * 3)(*[float(x) for x in c])
+    return int(N.lib().lb_rgb9e5(a))
+
+
+def rgb9e5_decode(p: int):
+    out = (C.c_float * 3)()
+    N.lib().lb_rgb9e5_decode(p, out)
+    return [out[0], out[1], out[2]]
+
+
+def bc4_block(v) -> bytes:
+    a = np.ascontiguousarray(v, dtype=np.uint8)
+    assert a.size == 16
+    out = np.zeros(8, np.uint8)
+    N.lib().lb_bc4_block(N.ptr(a), N.ptr(out))
+    return out.tobytes()

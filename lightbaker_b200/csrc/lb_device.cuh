@@ -1,0 +1,236 @@
+// Device-side building blocks of the bake passes: the sample sequence, the ray frames, the sky, and
+// the walk of the reference's BVH2 (crates/lightbaker/src/gpu/trace.wgsl:41-168). Every float
+// operation is written in the shader's source order and this code is built with -fmad=false, so a
+// result rounds exactly as the shader's source says (no contraction into fused multiply-adds).
+#pragma once
+#include <cstdint>
+
+#include "../../include/lightbaker.h"
+
+namespace lbd {
+
+constexpr float PI = 3.14159265f;       // trace.wgsl:33
+constexpr float FAR = 1e30f;            // :34
+constexpr uint32_t NONE = 0xffffffffu;  // :35
+constexpr float PUSH = 0.03f;           // :37
+constexpr int STACK = 48;               // :86
+
+// The scene as the kernels read it: float4 records, 16-byte aligned (node: 2, triangle: 3,
+// material: 1, chart: 2).
+struct Scene {
+    const float4 *nodes;
+    const float4 *tris;
+    const float4 *mats;
+    const float4 *charts;
+    uint32_t n_nodes, n_tris, n_mats, n_charts;
+};
+
+// Work counters a thread keeps when counting is on (lb_counters).
+struct Count {
+    uint32_t rays, nodes, tris, mats;
+    __device__ void zero() { rays = nodes = tris = mats = 0; }
+};
+
+__device__ __forceinline__ float3 mk(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 add(float3 a, float3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 sub(float3 a, float3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 scl(float3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 mulv(float3 a, float3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float3 norm3(float3 v) { return scl(v, 1.0f / sqrtf(dot3(v, v))); }
+__device__ __forceinline__ float3 xyz(float4 v) { return mk(v.x, v.y, v.z); }
+__device__ __forceinline__ float3 xyz(const float *p) { return mk(p[0], p[1], p[2]); }
+__device__ __forceinline__ float fract(float x) { return x - floorf(x); }
+
+// trace.wgsl:41-45
+__device__ __forceinline__ uint32_t pcg(uint32_t v) {
+    uint32_t s = v * 747796405u + 2891336453u;
+    uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+    return (w >> 22u) ^ w;
+}
+// trace.wgsl:46; u32 to f32 rounds to nearest, times 2^-32 (exact)
+__device__ __forceinline__ float rnd(uint32_t a, uint32_t b, uint32_t seed) {
+    return __uint2float_rn(pcg(a ^ pcg(b + seed))) * 0x1p-32f;
+}
+// trace.wgsl:49
+__device__ __forceinline__ float radical(uint32_t i) { return __uint2float_rn(__brev(i)) * 0x1p-32f; }
+
+// Sine and cosine of a (a >= 0), one algorithm for the kernels and the CPU oracle: Cody-Waite
+// reduction by pi/2 (pi/2 split in three floats of 12, 12 and 24 significant bits), then Taylor
+// polynomials of sin (to r^9) and cos (to r^10) on |r| <= pi/4 by Horner. Truncation < 3e-9.
+__device__ __forceinline__ void sincos32(float a, float *s, float *c) {
+    const float TWO_OVER_PI = 0x1.45f306p-1f;
+    const float P1 = 0x1.92p+0f, P2 = 0x1.fb4p-12f, P3 = 0x1.4442d2p-24f;
+    float k = rintf(a * TWO_OVER_PI);
+    float r = ((a - k * P1) - k * P2) - k * P3;
+    float r2 = r * r;
+    float sp = r + r * r2 * (-0x1.555556p-3f + r2 * (0x1.111112p-7f + r2 * (-0x1.a01a02p-13f + r2 * 0x1.71de3ap-19f)));
+    float cp = 1.0f + r2 * (-0.5f + r2 * (0x1.555556p-5f + r2 * (-0x1.6c16c2p-10f + r2 * (0x1.a01a02p-16f + r2 * -0x1.27e4fcp-22f))));
+    int q = int(k) & 3;
+    float ss = (q & 1) ? cp : sp, cc = (q & 1) ? sp : cp;
+    *s = (q & 2) ? -ss : ss;
+    *c = (q == 1 || q == 2) ? -cc : cc;
+}
+
+struct Frame {
+    float3 t, b, n;
+};
+// trace.wgsl:51-55
+__device__ __forceinline__ Frame frame(float3 n) {
+    float3 a = fabsf(n.y) > 0.9f ? mk(1.0f, 0.0f, 0.0f) : mk(0.0f, 1.0f, 0.0f);
+    float3 t = norm3(cross3(a, n));
+    return Frame{t, cross3(n, t), n};
+}
+// mat3x3f(t, b, n) * (x, y, z), columns summed in order
+__device__ __forceinline__ float3 apply(const Frame &f, float x, float y, float z) {
+    return add(add(scl(f.t, x), scl(f.b, y)), scl(f.n, z));
+}
+// trace.wgsl:57-61
+__device__ __forceinline__ float3 cosine(float u, float v, const Frame &f) {
+    float r = sqrtf(u);
+    float a = v * 2.0f * PI;
+    float s, c;
+    sincos32(a, &s, &c);
+    return norm3(apply(f, r * c, r * s, sqrtf(fmaxf(0.0f, 1.0f - u))));
+}
+// trace.wgsl:63-66; mix(h, z, t) = h * (1 - t) + z * t
+__device__ __forceinline__ float3 sky(const lb_params &P, float3 d) {
+    if (d.y < 0.0f) return xyz(P.ground);
+    return add(scl(xyz(P.horizon), 1.0f - d.y), scl(xyz(P.zenith), d.y));
+}
+// trace.wgsl:219-221 and :314-316: spiral sample k of gg on the sun's disc
+__device__ __forceinline__ float3 sun_disc(const lb_params &P, const Frame &sf, uint32_t k, uint32_t gg) {
+    float a = __uint2float_rn(k) * 2.399963f;
+    float r = P.sun_dir[3] * sqrtf((__uint2float_rn(k) + 0.5f) / __uint2float_rn(gg));
+    float s, c;
+    sincos32(a, &s, &c);
+    return norm3(add(add(xyz(P.sun_dir), scl(scl(sf.t, c), r)), scl(scl(sf.b, s), r)));
+}
+// trace.wgsl:152-156
+__device__ __forceinline__ float2 offset(uint32_t q) {
+    if (q <= 4u) return make_float2((q & 1u) ? 0.3f : -0.3f, q > 2u ? 0.3f : -0.3f);
+    switch (q) {
+    case 5: return make_float2(-0.45f, 0.0f);
+    case 6: return make_float2(0.45f, 0.0f);
+    case 7: return make_float2(0.0f, -0.45f);
+    default: return make_float2(0.0f, 0.45f);
+    }
+}
+
+struct Hit {
+    float t;
+    uint32_t tri;
+    bool back;
+};
+
+// trace.wgsl:69-72
+template <bool COUNT>
+__device__ __forceinline__ bool stops(const Scene &S, uint32_t tri, float v0w, uint32_t ray, uint32_t seed, Count &c) {
+    if (COUNT) c.mats++;
+    uint32_t m = __float_as_uint(v0w);
+    float op = m < S.n_mats ? __ldg(&S.mats[m]).w : 1.0f;
+    return op >= 1.0f || rnd(tri * 9781u, ray, seed) < op;
+}
+
+// trace.wgsl:74-80
+__device__ __forceinline__ float box(float3 o, float3 inv, float4 mn, float4 mx, float tmax) {
+    float ax = (mn.x - o.x) * inv.x, ay = (mn.y - o.y) * inv.y, az = (mn.z - o.z) * inv.z;
+    float bx = (mx.x - o.x) * inv.x, by = (mx.y - o.y) * inv.y, bz = (mx.z - o.z) * inv.z;
+    float lo = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
+    float hi = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+    float l0 = fmaxf(lo, 0.0f);
+    return (hi >= l0 && lo < tmax) ? l0 : FAR;
+}
+
+// trace.wgsl:83-130: the nearest hit within tmax (any: the first accepted). A thread's own walk with
+// a 48-entry stack; a far child that finds it full is dropped as in the shader. Child records are
+// carried into the next step instead of being read again; a popped node is read once. The root's box
+// is never tested (the shader starts at its children). An inner node whose children lie past the
+// array ends the walk (the reference's one-node BVH of an empty scene).
+template <bool COUNT>
+__device__ __forceinline__ Hit trace(const Scene &S, float3 o, float3 d, float tmax, bool any, uint32_t ray,
+                                     uint32_t seed, Count &c) {
+    Hit hit{tmax, NONE, false};
+    c.rays++;
+    if (COUNT) c.nodes++;
+    float3 dd = mk(fabsf(d.x) < 1e-12f ? 1e-12f : d.x, fabsf(d.y) < 1e-12f ? 1e-12f : d.y,
+                   fabsf(d.z) < 1e-12f ? 1e-12f : d.z);
+    float3 inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+    uint32_t stack[STACK];
+    int sp = 0;
+    float4 nlo = __ldg(&S.nodes[0]), nhi = __ldg(&S.nodes[1]);
+    for (;;) {
+        uint32_t first = __float_as_uint(nlo.w), count = __float_as_uint(nhi.w);
+        bool moved = false;
+        if (count > 0u) {
+            for (uint32_t i = first; i < first + count; i++) {
+                if (COUNT) c.tris++;
+                float4 v0 = __ldg(&S.tris[3 * i]), e1 = __ldg(&S.tris[3 * i + 1]), e2 = __ldg(&S.tris[3 * i + 2]);
+                float3 p = cross3(d, xyz(e2));
+                float det = dot3(xyz(e1), p);
+                if (fabsf(det) < 1e-12f) continue;
+                float id = 1.0f / det;
+                float3 s = sub(o, xyz(v0));
+                float u = dot3(s, p) * id;
+                if (u < 0.0f || u > 1.0f) continue;
+                float3 q = cross3(s, xyz(e1));
+                float v = dot3(d, q) * id;
+                if (v < 0.0f || u + v > 1.0f) continue;
+                float t = dot3(xyz(e2), q) * id;
+                if (t > 1e-4f && t < hit.t && stops<COUNT>(S, i, v0.w, ray, seed, c)) {
+                    hit = Hit{t, i, det < 0.0f};
+                    if (any) return hit;
+                }
+            }
+        } else if (first + 1u < S.n_nodes) {
+            if (COUNT) c.nodes += 2;
+            float4 alo = __ldg(&S.nodes[2 * first]), ahi = __ldg(&S.nodes[2 * first + 1]);
+            float4 blo = __ldg(&S.nodes[2 * first + 2]), bhi = __ldg(&S.nodes[2 * first + 3]);
+            float ta = box(o, inv, alo, ahi, hit.t);
+            float tb = box(o, inv, blo, bhi, hit.t);
+            bool a_near = ta <= tb;
+            float tn = fminf(ta, tb), tf = fmaxf(ta, tb);
+            if (tn < FAR) {
+                if (tf < FAR && sp < STACK) stack[sp++] = a_near ? first + 1u : first;
+                nlo = a_near ? alo : blo;
+                nhi = a_near ? ahi : bhi;
+                moved = true;
+            }
+        }
+        if (moved) continue;
+        if (sp == 0) break;
+        uint32_t n = stack[--sp];
+        nlo = __ldg(&S.nodes[2 * n]);
+        nhi = __ldg(&S.nodes[2 * n + 1]);
+    }
+    return hit;
+}
+
+// trace.wgsl:133-148
+__device__ __forceinline__ float3 bounced(const Scene &S, const lb_params &P, const float4 *light, uint32_t n_light,
+                                          float3 o, float3 d, const Hit &h) {
+    float4 v0 = __ldg(&S.tris[3 * h.tri]), e1 = __ldg(&S.tris[3 * h.tri + 1]);
+    uint32_t m = __float_as_uint(v0.w);
+    float4 mat = m < S.n_mats ? __ldg(&S.mats[m]) : make_float4(0.f, 0.f, 0.f, 1.f);
+    uint32_t ch = __float_as_uint(e1.w);
+    float3 e = xyz(P.fallback);
+    if (ch != NONE && ch < S.n_charts) {
+        float3 p = add(o, scl(d, h.t));
+        float4 r0 = __ldg(&S.charts[2 * ch]), r1 = __ldg(&S.charts[2 * ch + 1]);
+        float x = r0.x * p.x + r0.y * p.y + r0.z * p.z + r0.w * 1.0f;
+        float y = r1.x * p.x + r1.y * p.y + r1.z * p.z + r1.w * 1.0f;
+        int ix = min(max(int(floorf(x)), 0), int(P.atlas[0]) - 1);
+        int iy = min(max(int(floorf(y)), 0), int(P.atlas[1]) - 1);
+        uint32_t li = uint32_t(iy) * P.atlas[0] + uint32_t(ix);
+        if (li < n_light) {
+            float4 l = __ldg(&light[li]);
+            if (l.w > 0.5f) e = mk(l.x, l.y, l.z);
+        }
+    }
+    return mulv(mk(mat.x / PI, mat.y / PI, mat.z / PI), e);
+}
+
+}  // namespace lbd

@@ -1,0 +1,42 @@
+// The C ABI's handles and the runtime helpers the host code shares.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/lightbaker.h"
+
+// A device buffer kept by a handle and grown on demand.
+struct lb_buffer {
+    void *ptr = nullptr;
+    size_t cap = 0;
+};
+
+struct lb_gpu {
+    int device = 0;
+    int sms = 0;
+    char name[256] = {0};
+    cudaStream_t stream = nullptr;
+    bool counting = false;
+    unsigned long long *counters = nullptr;       // device: rays, nodes, tris, mats
+    unsigned long long *host_counters = nullptr;  // pinned copy, written by the stream
+    lb_counters last = {};
+    uint64_t h2d = 0, d2h = 0;  // bytes copied by this handle
+    lb_buffer items, out, light;
+};
+
+// The scene's buffers (gpu/mod.rs:65-71).
+struct lb_scene {
+    lb_gpu *gpu = nullptr;
+    void *nodes = nullptr, *tris = nullptr, *mats = nullptr, *charts = nullptr;
+    uint32_t n_nodes = 0, n_tris = 0, n_mats = 0, n_charts = 0;
+};
+
+void lb_set_error(const std::string &msg);
+int lb_cuda_fail(cudaError_t e, const char *what);
+int lb_buffer_reserve(lb_buffer &b, size_t bytes);
+void lb_buffer_free(lb_buffer &b);
+int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const float4 *items, uint32_t n, uint32_t base,
+                  const float4 *light, uint32_t n_light, float4 *out);
+void lb_collect_counters(lb_gpu *g);

@@ -1,0 +1,280 @@
+// The C ABI's device side: open a device, upload a scene, run a pass (crates/lightbaker/src/gpu/mod.rs).
+//
+// The reference runs a pass in batches of 65536 / 16384 / 8192 items, each with a new uniform buffer,
+// result buffer and bind group, submitted and waited on before the next (gpu/mod.rs:140-196). Here a
+// pass is one launch over every item: the shader keys its samples by P.atlas.z + i, the item's index
+// in the whole list, so the batch split never changes a result, and there is no display watchdog to
+// keep dispatches short for on a compute GPU. Device buffers are kept by the handle and grown, not
+// allocated per call.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "lb_device.cuh"
+#include "lb_kernels.h"
+#include "lb_runtime.h"
+
+static thread_local std::string g_error;
+
+void lb_set_error(const std::string &msg) { g_error = msg; }
+
+int lb_cuda_fail(cudaError_t e, const char *what) {
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+    g_error = buf;
+    return e == cudaErrorMemoryAllocation ? LB_ENOMEM : LB_ECUDA;
+}
+
+#define LB_CUDA(call, what)                                          \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return lb_cuda_fail(e_, what);        \
+    } while (0)
+
+int lb_buffer_reserve(lb_buffer &b, size_t bytes) {
+    if (bytes <= b.cap) return LB_OK;
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.cap = 0;
+    size_t want = bytes + bytes / 4;
+    cudaError_t e = cudaMalloc(&b.ptr, want);
+    if (e != cudaSuccess) {
+        b.ptr = nullptr;
+        return lb_cuda_fail(e, "cudaMalloc");
+    }
+    b.cap = want;
+    return LB_OK;
+}
+
+void lb_buffer_free(lb_buffer &b) {
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.cap = 0;
+}
+
+extern "C" {
+
+const char *lb_last_error(void) { return g_error.c_str(); }
+
+lb_gpu *lb_gpu_open(int device, char *name, size_t cap) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        lb_set_error(std::string("no GPU adapter: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "no CUDA device"));
+        return nullptr;
+    }
+    if (device < 0 || device >= count) {
+        lb_set_error("no GPU device " + std::to_string(device));
+        return nullptr;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        lb_set_error("no GPU device: cudaGetDeviceProperties failed");
+        return nullptr;
+    }
+    if (prop.major != 10 || prop.minor != 0) {
+        lb_set_error(std::string("no GPU device: ") + prop.name + " is sm_" + std::to_string(prop.major) +
+                     std::to_string(prop.minor) + "; this build is for sm_100a (B200)");
+        return nullptr;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) {
+        lb_set_error("no GPU device: cudaSetDevice failed");
+        return nullptr;
+    }
+    lb_gpu *g = new lb_gpu();
+    g->device = device;
+    g->sms = prop.multiProcessorCount;
+    snprintf(g->name, sizeof g->name, "%s (CUDA, sm_%d%d, %d SMs)", prop.name, prop.major, prop.minor, prop.multiProcessorCount);
+    if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&g->counters, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMallocHost(&g->host_counters, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMemset(g->counters, 0, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+        lb_set_error("no GPU device: stream or counter allocation failed");
+        delete g;
+        return nullptr;
+    }
+    if (name && cap) {
+        strncpy(name, g->name, cap - 1);
+        name[cap - 1] = 0;
+    }
+    return g;
+}
+
+void lb_gpu_close(lb_gpu *g) {
+    if (!g) return;
+    cudaSetDevice(g->device);
+    cudaStreamSynchronize(g->stream);
+    lb_buffer_free(g->items);
+    lb_buffer_free(g->out);
+    lb_buffer_free(g->light);
+    if (g->counters) cudaFree(g->counters);
+    if (g->host_counters) cudaFreeHost(g->host_counters);
+    cudaStreamDestroy(g->stream);
+    delete g;
+}
+
+lb_scene *lb_scene_upload(lb_gpu *g, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+                          const float *materials, size_t n_materials, const float *charts, size_t n_charts) {
+    if (!g || !nodes || n_nodes == 0 || (n_tris && !tris) || (n_materials && !materials) || (n_charts && !charts)) {
+        lb_set_error("lb_scene_upload: bad arguments");
+        return nullptr;
+    }
+    if (n_nodes > 0x7fffffffu || n_tris > 0x7fffffffu) {
+        lb_set_error("lb_scene_upload: more than 2^31 nodes or triangles");
+        return nullptr;
+    }
+    cudaSetDevice(g->device);
+    lb_scene *s = new lb_scene();
+    s->gpu = g;
+    // an empty list still gets one record, as the reference's dummy chart (gpu/mod.rs:134)
+    static const float zero[8] = {0};
+    struct Part {
+        void **dst;
+        const void *src;
+        size_t bytes;
+    } parts[4] = {
+        {&s->nodes, nodes, n_nodes * sizeof(lb_node)},
+        {&s->tris, n_tris ? (const void *)tris : zero, (n_tris ? n_tris : 1) * sizeof(lb_tri)},
+        {&s->mats, n_materials ? (const void *)materials : zero, (n_materials ? n_materials : 1) * 16},
+        {&s->charts, n_charts ? (const void *)charts : zero, (n_charts ? n_charts : 1) * 32},
+    };
+    static const lb_tri zero_tri = {};
+    if (!n_tris) parts[1].src = &zero_tri;
+    for (auto &p : parts) {
+        cudaError_t e = cudaMalloc(p.dst, p.bytes);
+        if (e == cudaSuccess) e = cudaMemcpy(*p.dst, p.src, p.bytes, cudaMemcpyHostToDevice);
+        g->h2d += p.bytes;
+        if (e != cudaSuccess) {
+            lb_cuda_fail(e, "lb_scene_upload");
+            lb_scene_free(s);
+            return nullptr;
+        }
+    }
+    s->n_nodes = uint32_t(n_nodes);
+    s->n_tris = uint32_t(n_tris);
+    s->n_mats = uint32_t(n_materials);
+    s->n_charts = uint32_t(n_charts);
+    return s;
+}
+
+void lb_scene_free(lb_scene *s) {
+    if (!s) return;
+    cudaSetDevice(s->gpu->device);
+    for (void *p : {s->nodes, s->tris, s->mats, s->charts})
+        if (p) cudaFree(p);
+    delete s;
+}
+
+int lb_run(lb_gpu *g, lb_scene *s, int pass, const lb_params *params, const lb_texel *items, size_t n,
+           const float *light, size_t n_light, float *out) {
+    if (!g || !s || !params || pass < 0 || pass > 2 || (n && (!items || !out)) || (n_light && !light)) {
+        lb_set_error("lb_run: bad arguments");
+        return LB_EINVAL;
+    }
+    if (n == 0) return LB_OK;  // gpu/mod.rs:143-145
+    if (n > 0xffffffffu / 8) {
+        lb_set_error("lb_run: more than 2^29 items in one pass");
+        return LB_EINVAL;
+    }
+    LB_CUDA(cudaSetDevice(g->device), "cudaSetDevice");
+    size_t width = pass == LB_PASS_VOLUME ? 4 : 1;
+    int rc;
+    if ((rc = lb_buffer_reserve(g->items, n * sizeof(lb_texel))) != LB_OK) return rc;
+    if ((rc = lb_buffer_reserve(g->out, n * width * 16)) != LB_OK) return rc;
+    size_t nl = n_light ? n_light : 1;
+    if ((rc = lb_buffer_reserve(g->light, nl * 16)) != LB_OK) return rc;
+    LB_CUDA(cudaMemcpyAsync(g->items.ptr, items, n * sizeof(lb_texel), cudaMemcpyHostToDevice, g->stream), "copy items");
+    g->h2d += n * sizeof(lb_texel);
+    if (n_light) {
+        LB_CUDA(cudaMemcpyAsync(g->light.ptr, light, n_light * 16, cudaMemcpyHostToDevice, g->stream), "copy light");
+        g->h2d += n_light * 16;
+    } else {
+        LB_CUDA(cudaMemsetAsync(g->light.ptr, 0, 16, g->stream), "clear light");
+    }
+    lb_params P = *params;
+    P.counts[3] = uint32_t(n);
+    P.atlas[2] = 0;
+    rc = lb_run_device(g, s, pass, P, (const float4 *)g->items.ptr, uint32_t(n), 0, (const float4 *)g->light.ptr,
+                       uint32_t(nl), (float4 *)g->out.ptr);
+    if (rc != LB_OK) return rc;
+    LB_CUDA(cudaMemcpyAsync(out, g->out.ptr, n * width * 16, cudaMemcpyDeviceToHost, g->stream), "copy results");
+    g->d2h += n * width * 16;
+    LB_CUDA(cudaStreamSynchronize(g->stream), "lb_run");
+    lb_collect_counters(g);
+    return LB_OK;
+}
+
+void *lb_gpu_stream(lb_gpu *g) { return g ? (void *)g->stream : nullptr; }
+
+int lb_gpu_sync(lb_gpu *g) {
+    if (!g) return LB_EINVAL;
+    LB_CUDA(cudaStreamSynchronize(g->stream), "lb_gpu_sync");
+    lb_collect_counters(g);
+    return LB_OK;
+}
+
+int lb_run_async(lb_gpu *g, lb_scene *s, int pass, const lb_params *params, const lb_texel *items, size_t n,
+                 uint32_t base, const float *light, size_t n_light, float *out) {
+    if (!g || !s || !params || pass < 0 || pass > 2 || (n && (!items || !out)) || !light || n_light == 0) {
+        lb_set_error("lb_run_async: bad arguments (light must hold at least one record)");
+        return LB_EINVAL;
+    }
+    if (n == 0) return LB_OK;
+    if (n > 0xffffffffu / 8) {
+        lb_set_error("lb_run_async: more than 2^29 items in one pass");
+        return LB_EINVAL;
+    }
+    LB_CUDA(cudaSetDevice(g->device), "cudaSetDevice");
+    lb_params P = *params;
+    P.counts[3] = uint32_t(n);
+    P.atlas[2] = base;
+    return lb_run_device(g, s, pass, P, (const float4 *)items, uint32_t(n), base, (const float4 *)light,
+                         uint32_t(n_light), (float4 *)out);
+}
+
+int lb_get_transfer(lb_gpu *g, uint64_t *h2d, uint64_t *d2h, int reset) {
+    if (!g) return LB_EINVAL;
+    if (h2d) *h2d = g->h2d;
+    if (d2h) *d2h = g->d2h;
+    if (reset) g->h2d = g->d2h = 0;
+    return LB_OK;
+}
+
+int lb_set_counting(lb_gpu *g, int on) {
+    if (!g) return LB_EINVAL;
+    g->counting = on != 0;
+    return LB_OK;
+}
+
+int lb_get_counters(lb_gpu *g, lb_counters *out) {
+    if (!g || !out) return LB_EINVAL;
+    *out = g->last;
+    return LB_OK;
+}
+
+}  // extern "C"
+
+// A pass over items already on the device, on the handle's stream. The pass's counters (rays always;
+// the walk's work when counting is on) land in g->host_counters once the stream reaches them; call
+// lb_collect_counters after a sync to move them into g->last.
+int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const float4 *items, uint32_t n, uint32_t base,
+                  const float4 *light, uint32_t n_light, float4 *out) {
+    lbd::Scene S{(const float4 *)s->nodes, (const float4 *)s->tris, (const float4 *)s->mats, (const float4 *)s->charts,
+                 s->n_nodes, s->n_tris, s->n_mats, s->n_charts};
+    LB_CUDA(cudaMemsetAsync(g->counters, 0, 4 * sizeof(unsigned long long), g->stream), "counters");
+    LB_CUDA(lb_launch_pass_bvh2(pass, S, P, items, n, base, light, n_light, out, g->counters, g->counting, g->stream),
+            "pass launch");
+    LB_CUDA(cudaMemcpyAsync(g->host_counters, g->counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            g->stream),
+            "counters");
+    return LB_OK;
+}
+
+void lb_collect_counters(lb_gpu *g) {
+    g->last.rays = g->host_counters[0];
+    g->last.nodes = g->host_counters[1];
+    g->last.tris = g->host_counters[2];
+    g->last.mats = g->host_counters[3];
+}

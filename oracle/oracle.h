@@ -1,0 +1,82 @@
+/*
+ * ORACLE — test infrastructure only. Nothing in the lightbaker_b200 package links, imports or calls
+ * this; only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg do, as the checker.
+ *
+ * A scalar CPU restatement of the reference's bake passes:
+ *   trace_ref.cpp   crates/lightbaker/src/gpu/trace.wgsl:41-324 (direct, gather, volume; trace()),
+ *                   in FP32 with the shader's operation order, and the same walk in FP64
+ *   filter_ref.cpp  crates/lightbaker/src/filter.rs:20-141 (smooth, fill, sun_field) and the per-tile
+ *                   texel work of crates/lightbaker/src/bake.rs:197-445
+ *
+ * Parity status: the reference is Rust + wgpu and cannot run here (no Rust toolchain, no graphics
+ * stack), and its tests hold no numeric golden vectors for these passes. The restatement is pinned by
+ * the reference's own property tests (crates/lightbaker/tests/bake.rs:95-154, restated in
+ * tests/test_bake_properties.py), its encode known-answer tests (encode.rs:150-180) and internal
+ * consistency (FP64 twin); numeric parity with the WGSL is otherwise "parity unpinned".
+ *
+ * Build: oracle/build.sh (g++ -O2 -ffp-contract=off -fopenmp): no fused multiply-add, so every
+ * float operation rounds as the shader's source orders it.
+ */
+#ifndef LB_ORACLE_H
+#define LB_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../include/lightbaker.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Work the walk did, counted as lb_counters counts it on the device. */
+typedef struct or_counters {
+    uint64_t rays, nodes, tris, mats, overflows;
+} or_counters;
+
+/* One pass over n items, as Gpu::run: out gets n * width float4 records. threads <= 0: all cores. */
+int or_run(int pass, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+           const float *materials, size_t n_materials, const float *charts, size_t n_charts,
+           const lb_params *params, const lb_texel *items, size_t n, const float *light,
+           size_t n_light, float *out, int threads, or_counters *counters);
+
+/* One ray through the scene, in FP32 (precision 32) or FP64 (64); writes t, triangle
+ * (0xffffffff: none), back face. `any`: the first accepted hit. */
+int or_trace(int precision, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+             const float *materials, size_t n_materials, const lb_params *params, const float o[3],
+             const float d[3], float tmax, int any, uint32_t ray, double *t, uint32_t *tri, int *back);
+
+/* Is this ray within `eps` of deciding differently: does it pass, in FP64, within eps (barycentric)
+ * of the edge of a triangle that stops it, or meet one within eps (relative) of 1e-4 or tmax? */
+int or_ray_ambiguous(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+                     const float *materials, size_t n_materials, const lb_params *params,
+                     const float o[3], const float d[3], float tmax, uint32_t ray, double eps);
+
+/* The rays a pass casts for item i (origin, direction, tmax, any-hit flag, ray key), in the order the
+ * shader casts them, for items whose outcome does not change the rays that follow: the sun and
+ * occlusion rays of a direct item from its sample point (pick given), the gather rays, the volume's.
+ * Returns the number of rays (at most cap). kind: 0 inside-test rays at the chosen point, 1 hard sun,
+ * 2 soft sun, 3 occlusion, 4 gather, 5 volume sphere, 6 volume sun. */
+size_t or_item_rays(int pass, const lb_params *params, const lb_texel *item, size_t index,
+                    uint32_t pick, float *o, float *d, float *tmax, int *any, uint32_t *key,
+                    int *kind, size_t cap);
+
+/* The shader's own helpers, for unit tests: pcg (trace.wgsl:41-45), rand (:46), radical (:49),
+ * the sine and cosine both sides use. */
+uint32_t or_pcg(uint32_t v);
+float or_rand(uint32_t a, uint32_t b, uint32_t seed_bits);
+float or_radical(uint32_t i);
+void or_sincos(float a, float *s, float *c);
+
+/* filter.rs restated (N channels interleaved). valid/known are bytes (0/1). */
+void or_smooth(int w, int h, const uint32_t *chart, const float *normal /* 3 a texel */,
+               const float *v, int channels, const uint8_t *valid, int r, float *out);
+void or_fill(int w, int h, const uint32_t *chart, float *v, int channels, uint8_t *valid,
+             int rings);
+void or_sun_field(int w, int h, const uint32_t *chart, const float *normal, const uint32_t *hard,
+                  const uint8_t *covered, int g, float radius, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
