@@ -122,6 +122,9 @@ int lb_gpu_sync(lb_gpu *gpu);
  * list (it keys the sample sequence, as the shader's P.atlas.z + i). */
 int lb_run_async(lb_gpu *gpu, lb_scene *scene, int pass, const lb_params *params, const lb_texel *items,
                  size_t n, uint32_t base, const float *light, size_t n_light, float *out);
+/* Which kernels lb_run and lb_run_async use: 0 (default) one thread an item, as the shader is
+ * dispatched; 1 one warp an item (the device-resident bake's kernels). Results are identical. */
+int lb_set_pass_kernel(lb_gpu *gpu, int kind);
 /* Bytes this handle copied host to device and device to host since the last reset. */
 int lb_get_transfer(lb_gpu *gpu, uint64_t *h2d, uint64_t *d2h, int reset);
 
@@ -196,6 +199,26 @@ int lb_bake_get_tri_charts(const lb_bake *b, uint32_t *out);
 /* output::write (output.rs:95-154): the .lbake file. *out is malloc'd; free with lb_free. */
 int lb_bake_write(const lb_bake *b, uint8_t **out, size_t *len);
 void lb_free(void *p);
+
+/* ---- the device-resident bake (the batched mode) ---- */
+
+/* bake() with every dirty tile rebaked in one CUDA graph on `gpu`: the host lays out, builds the BVH,
+ * hashes and rasterises (bake.rs:94-149); the device runs the ray passes over all dirty tiles at once,
+ * the texel passes, the bounces, the volume and the atlas. Results equal lb_bake_run's. */
+lb_bake *lb_bake_device(lb_gpu *gpu, const uint8_t *scene, size_t len, const lb_bake_options *opts);
+
+/* The same in steps, for a caller that rebakes the same dirty set: create (host work, uploads, the
+ * graph captured), launch (the graph enqueued on the handle's stream; may be repeated), result (waits,
+ * downloads, writes the cache; a bake handle). lb_plan_rays gives the rays of the last launch a pass:
+ * direct, gather (all bounces), volume. */
+typedef struct lb_plan lb_plan;
+lb_plan *lb_plan_create(lb_gpu *gpu, const uint8_t *scene, size_t len, const lb_bake_options *opts);
+int lb_plan_launch(lb_plan *plan);
+int lb_plan_rays(lb_plan *plan, uint64_t rays[3]);
+lb_bake *lb_plan_result(lb_plan *plan);
+/* Kernel launches in one launch of the plan's graph. */
+int lb_plan_kernels(const lb_plan *plan);
+void lb_plan_free(lb_plan *plan);
 
 /* Scene::write (scene.rs:164-181) from a JSON header and positions: for tools and tests that make
  * scenes. header_json is the header as the file holds it. */

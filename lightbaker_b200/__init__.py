@@ -135,6 +135,10 @@ class Gpu:
         N.check(N.lib().lb_get_transfer(self._h, C.byref(h), C.byref(d), int(reset)), "lb_get_transfer")
         return h.value, d.value
 
+    def set_pass_kernel(self, kind: int) -> None:
+        """0: one thread an item (as the shader); 1: one warp an item. Same results."""
+        N.check(N.lib().lb_set_pass_kernel(self._h, int(kind)), "lb_set_pass_kernel")
+
     def set_counting(self, on: bool) -> None:
         N.check(N.lib().lb_set_counting(self._h, int(on)), "lb_set_counting")
 
@@ -301,6 +305,52 @@ def bake(scene: bytes, gpu: Gpu, cache=None, log=None) -> Bake:
     if not h:
         raise LightbakerError(N.last_error())
     return Bake(h)
+
+
+def bake_device(scene: bytes, gpu: Gpu, cache=None, log=None) -> Bake:
+    """The device-resident bake: every dirty tile rebaked in one CUDA graph (same results as bake())."""
+    opts, keep = _options(cache, log)
+    h = N.lib().lb_bake_device(gpu.handle, scene, len(scene), C.byref(opts))
+    del keep
+    if not h:
+        raise LightbakerError(N.last_error())
+    return Bake(h)
+
+
+class Plan:
+    """A device bake in steps: the host work and the graph once (`Plan(scene, gpu)`), then `launch()`
+    (the graph enqueued on gpu.stream; repeatable), `rays()`, `result()`."""
+
+    def __init__(self, scene: bytes, gpu: Gpu, cache=None, log=None):
+        self._opts, self._keep = _options(cache, log)
+        self._h = N.lib().lb_plan_create(gpu.handle, scene, len(scene), C.byref(self._opts))
+        if not self._h:
+            raise LightbakerError(N.last_error())
+
+    def launch(self) -> None:
+        N.check(N.lib().lb_plan_launch(self._h), "lb_plan_launch")
+
+    def rays(self) -> tuple:
+        r = (C.c_uint64 * 3)()
+        N.check(N.lib().lb_plan_rays(self._h, r), "lb_plan_rays")
+        return r[0], r[1], r[2]
+
+    def result(self) -> Bake:
+        h = N.lib().lb_plan_result(self._h)
+        if not h:
+            raise LightbakerError(N.last_error())
+        return Bake(h)
+
+    def close(self) -> None:
+        if self._h:
+            N.lib().lb_plan_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def bake_with(scene: bytes, tracer: "N.Tracer", cache=None, log=None) -> Bake:

@@ -83,6 +83,7 @@ SIGNATURES = {
     "lb_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(Params), C.c_void_p, C.c_size_t, C.c_void_p,
                          C.c_size_t, C.c_void_p]),
     "lb_set_counting": (C.c_int, [C.c_void_p, C.c_int]),
+    "lb_set_pass_kernel": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_get_counters": (C.c_int, [C.c_void_p, C.POINTER(Counters)]),
     "lb_gpu_stream": (C.c_void_p, [C.c_void_p]),
     "lb_gpu_sync": (C.c_int, [C.c_void_p]),
@@ -100,6 +101,13 @@ SIGNATURES = {
     "lb_bake_run": (C.c_void_p, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(BakeOptions)]),
     "lb_bake_run_with": (C.c_void_p, [C.POINTER(Tracer), C.c_char_p, C.c_size_t, C.POINTER(BakeOptions)]),
     "lb_bake_free": (None, [C.c_void_p]),
+    "lb_bake_device": (C.c_void_p, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(BakeOptions)]),
+    "lb_plan_create": (C.c_void_p, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(BakeOptions)]),
+    "lb_plan_launch": (C.c_int, [C.c_void_p]),
+    "lb_plan_rays": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "lb_plan_result": (C.c_void_p, [C.c_void_p]),
+    "lb_plan_free": (None, [C.c_void_p]),
+    "lb_plan_kernels": (C.c_int, [C.c_void_p]),
     "lb_bake_get_info": (C.c_int, [C.c_void_p, C.POINTER(BakeInfo)]),
     "lb_bake_get_direct": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lb_bake_get_indirect": (C.c_int, [C.c_void_p, C.c_void_p]),

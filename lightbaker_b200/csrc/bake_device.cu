@@ -1,0 +1,639 @@
+// The device-resident bake (the batched mode): every dirty tile rebaked in one CUDA graph.
+//
+// The host does what only it can do cheaply before the first ray: read the scene, lay out the charts,
+// build the BVH, hash the tiles against the cache and rasterise the dirty ones (the reference's steps,
+// crates/lightbaker/src/bake.rs:94-149). Then one graph runs the rest on the device with no host round
+// trip: the direct pass over every dirty texel at once (tiles of any size in one persistent launch), the
+// texel passes, the gather selection and its compaction, every bounce (gather pass, smoothing, fill,
+// the atlas rewritten), the volume and its fill, the fallback and the atlas composite. The graph is
+// captured once per scene and can be replayed (a rebake of the same dirty set).
+//
+// Results equal the drop-in bake's (the host passes) record for record: the ray passes are the
+// shader's arithmetic in its order, the texel passes the host's.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+#include "host/bake.h"
+#include "host/cache.h"
+#include "host/deps.h"
+#include "host/handles.h"
+#include "host/raster.h"
+#include "lb_device.cuh"
+#include "lb_kernels.h"
+#include "lb_post.h"
+#include "lb_runtime.h"
+
+namespace {
+
+void ck(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// A device allocation freed with the plan.
+struct DBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    void alloc(size_t n) {
+        bytes = n ? n : 16;
+        ck(cudaMalloc(&p, bytes), "cudaMalloc");
+    }
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+    template <class T> T *as() const { return (T *)p; }
+};
+
+std::vector<float> gauss_weights(int r) {
+    // filter.rs:28-41: exp(-(dx^2 + dy^2) / sigma2), sigma2 = 2 (0.75 r)^2, as the host computes it
+    std::vector<float> w(size_t(2 * r + 1) * (2 * r + 1), 0.0f);
+    if (r == 0) return w;
+    float q = float(r) * 0.75f;
+    float sigma2 = 2.0f * (q * q);
+    for (int dy = -r; dy <= r; dy++)
+        for (int dx = -r; dx <= r; dx++) {
+            float fx = float(dx), fy = float(dy);
+            w[size_t(dy + r) * (2 * r + 1) + (dx + r)] = std::exp(-(fx * fx + fy * fy) / sigma2);
+        }
+    return w;
+}
+
+double since(std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+}
+
+}  // namespace
+
+struct lb_plan {
+    lb_gpu *g = nullptr;
+    lb::Scene scene;
+    lb::Prepared P;
+    lb::Options opt;
+    lb_scene *dscene = nullptr;
+    std::vector<size_t> dirty, order;          // order: dirty tiles, then cached ones
+    std::vector<lb::Hash> hashes;
+    std::vector<std::optional<lb::TileLight>> lights;
+    std::vector<DTile> tiles_all;              // in `order`
+    uint32_t n_dirty_texels = 0, n_all = 0, n_cov = 0;
+    std::vector<uint32_t> cov_counts;          // covered texels per dirty tile
+    // volume
+    bool has_volume = false;
+    std::array<uint32_t, 3> vsize{};
+    uint32_t n_probes = 0, n_todo = 0;
+    std::map<lb::TileKey, std::vector<uint32_t>> chunks;
+    std::vector<std::pair<lb::Hash, std::vector<uint32_t>>> chunk_keys;
+    size_t n_chunks = 0;
+    // device arrays
+    DBuf tiles_d, tex, cov_idx, cov_k, direct_out, chart, valid, state, known, known_tmp, gathered, hard, gk, soft,
+        ao_raw, ao, field, dl, ind, posg, light, w1, wr, gath_idx, gath_count, gather_out, select_temp;
+    DBuf s_ka, s_kb, s_f1, s_f2, s_v4, s_e0, s_e1;
+    DBuf probes, probes_init, probes_b, probe_items, probe_slot, pk_a, pk_b;
+    DBuf owner, direct_atlas, validity, indirect, indirect_b, has, has_b, counters;
+    size_t select_bytes = 0;
+    uint32_t aw = 0, ah = 0, iw = 0, ih = 0, ds = 1;
+    int blocks_direct = 0, blocks_gather = 0, blocks_volume = 0;
+    int kernel_nodes = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double t_prepare = 0;
+    lb::Stats stats;
+    ~lb_plan() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (dscene) lb_scene_free(dscene);
+    }
+};
+
+namespace {
+
+int warp_blocks(lb_gpu *g, int pass) {
+    WarpPass w{};
+    w.pass = pass;
+    w.sms = g->sms;
+    return lb_warp_pass_blocks(w);
+}
+
+void build(lb_plan &p) {
+    auto t0 = std::chrono::steady_clock::now();
+    const lb::SceneHeader &h = p.scene.header;
+    const lb::BakeSettings &b = h.bake;
+    const lb::LightmapSettings &lm = h.lightmap;
+    p.P = lb::prepare(p.scene);
+    lb::Layout &layout = p.P.layout;
+    p.aw = layout.width;
+    p.ah = layout.height;
+    p.ds = lm.indirect_downscale;
+    p.iw = (p.aw + p.ds - 1) / p.ds;
+    p.ih = (p.ah + p.ds - 1) / p.ds;
+    p.dscene = lb_scene_upload(p.g, p.P.bvh.nodes.data(), p.P.bvh.nodes.size(), p.P.bvh.tris.data(),
+                               p.P.bvh.tris.size(), p.P.materials.data(), p.P.materials.size() / 4,
+                               p.P.affines.data(), p.P.affines.size() / 8);
+    if (!p.dscene) throw std::runtime_error(lb_last_error());
+
+    // the cache (bake.rs:123-136)
+    lb::Cache cache(p.opt.cache);
+    lb::Boxes boxes(p.scene);
+    lb::Hash global = lb::global_hash(p.scene);
+    float reach = b.gi_bounces > 0 ? std::fmax(b.gi_reach, b.ao_reach) : b.ao_reach;
+    size_t nt = layout.tiles.size();
+    p.hashes.resize(nt);
+    p.lights.resize(nt);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long ti = 0; ti < (long long)nt; ti++) {
+        const lb::Tile &t = layout.tiles[ti];
+        p.hashes[ti] = lb::hash_reach(p.scene, boxes, global, lb::tile_box(p.scene, layout, t.charts), reach,
+                                      lb::tile_seed(p.scene, layout, t.key, t.charts));
+        if (auto bytes = cache.get("tile", p.hashes[ti])) p.lights[ti] = lb::TileLight::unpack(*bytes, size_t(t.w) * t.h);
+    }
+    for (size_t i = 0; i < nt; i++)
+        if (!p.lights[i]) p.dirty.push_back(i);
+    p.order = p.dirty;
+    for (size_t i = 0; i < nt; i++)
+        if (p.lights[i]) p.order.push_back(i);
+
+    // device texel layout: dirty tiles first
+    uint32_t off = 0;
+    for (size_t k = 0; k < p.order.size(); k++) {
+        const lb::Tile &t = layout.tiles[p.order[k]];
+        p.tiles_all.push_back(DTile{t.x, t.y, t.w, t.h, off});
+        off += t.w * t.h;
+        if (k + 1 == p.dirty.size()) p.n_dirty_texels = off;
+    }
+    p.n_all = off;
+    if (p.dirty.empty()) p.n_dirty_texels = 0;
+
+    // rasterise the dirty tiles (bake.rs:138-149)
+    std::vector<lb_texel> tex(p.n_dirty_texels);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long wi = 0; wi < (long long)p.dirty.size(); wi++) {
+        std::vector<lb_texel> v = lb::rasterize(p.scene, layout, layout.tiles[p.dirty[wi]]);
+        std::memcpy(&tex[p.tiles_all[wi].off], v.data(), v.size() * sizeof(lb_texel));
+    }
+    std::vector<uint32_t> cov_idx, cov_k(p.n_dirty_texels, 0xffffffffu);
+    for (uint32_t i = 0; i < p.n_dirty_texels; i++)
+        if (lb::covered(tex[i])) {
+            cov_k[i] = uint32_t(cov_idx.size());
+            cov_idx.push_back(i);
+        }
+    p.n_cov = uint32_t(cov_idx.size());
+
+    // cached tiles' light, the atlas owner map and the atlas the first bounce reads
+    std::vector<uint8_t> known(p.n_all, 0), state(p.n_all, 0);
+    std::vector<float> field(p.n_all, 0.0f), ao(p.n_all, 0.0f);
+    std::vector<float> dl(size_t(p.n_all) * 4, 0.0f), ind(size_t(p.n_all) * 4, 0.0f);
+    std::vector<uint32_t> owner(size_t(p.aw) * p.ah, 0xffffffffu);
+    std::vector<float> light(size_t(p.aw) * p.ah * 4, 0.0f);
+    for (size_t k = 0; k < p.order.size(); k++) {
+        size_t ti = p.order[k];
+        const DTile &t = p.tiles_all[k];
+        for (uint32_t y = 0; y < t.h; y++)
+            for (uint32_t x = 0; x < t.w; x++) owner[size_t(t.y + y) * p.aw + t.x + x] = t.off + y * t.w + x;
+        if (!p.lights[ti]) continue;
+        const lb::TileLight &l = *p.lights[ti];
+        for (uint32_t i = 0; i < t.w * t.h; i++) {
+            uint32_t d = t.off + i;
+            known[d] = l.known[i];
+            state[d] = l.state[i];
+            field[d] = l.field[i];
+            ao[d] = l.ao[i];
+            for (int c = 0; c < 3; c++) {
+                dl[size_t(d) * 4 + c] = l.direct[i][c];
+                ind[size_t(d) * 4 + c] = l.indirect[i][c];
+            }
+        }
+        lb::write_light(layout, ti, l, light);
+    }
+
+    // the volume's probes: cached chunks, the rest to bake (volume.rs:34-84)
+    std::vector<float> probes_init;
+    std::vector<lb_texel> probe_items;
+    std::vector<uint32_t> probe_slot;
+    if (h.volume) {
+        const lb::VolumeSettings &v = *h.volume;
+        p.has_volume = true;
+        auto n = [&](int a) { return uint32_t(std::round((v.max[a] - v.min[a]) / v.step)) + 1; };
+        p.vsize = {std::max(n(0), 2u), std::max(n(1), 2u), std::max(n(2), 2u)};
+        size_t nx = p.vsize[0], nz = p.vsize[2];
+        p.n_probes = p.vsize[0] * p.vsize[1] * p.vsize[2];
+        auto at = [&](size_t k) {
+            return lb::Vec3(v.min[0] + float(k % nx) * v.step, v.min[1] + float(k / (nx * nz)) * v.step,
+                            v.min[2] + float((k / nx) % nz) * v.step);
+        };
+        for (size_t k = 0; k < p.n_probes; k++) p.chunks[lb::tile_of(at(k), lm.tile_size)].push_back(uint32_t(k));
+        probes_init.assign(size_t(p.n_probes) * 16, 0.0f);
+        std::string vjson = lb::to_json(v).dump();
+        for (auto &kv : p.chunks) {
+            lb::Aabb bx;
+            for (uint32_t k : kv.second) bx.add(at(k));
+            std::vector<uint8_t> seed(8);
+            std::memcpy(seed.data(), &kv.first.first, 4);
+            std::memcpy(seed.data() + 4, &kv.first.second, 4);
+            seed.insert(seed.end(), vjson.begin(), vjson.end());
+            lb::Hash hash = lb::hash_reach(p.scene, boxes, global, bx, b.gi_reach, seed);
+            auto got = cache.get("probes", hash);
+            if (got && got->size() == kv.second.size() * 64) {
+                for (size_t i = 0; i < kv.second.size(); i++)
+                    std::memcpy(&probes_init[size_t(kv.second[i]) * 16], got->data() + i * 64, 64);
+            } else {
+                for (uint32_t k : kv.second) {
+                    lb::Vec3 q = at(k);
+                    probe_items.push_back(lb_texel{{q.x, q.y, q.z, 1.0f}, {0.0f, 1.0f, 0.0f, lb::u2f(k)}, {0, 0, 0, 0}, {0, 0, 0, 0}});
+                    probe_slot.push_back(k);
+                }
+                p.chunk_keys.emplace_back(hash, kv.second);
+            }
+        }
+        p.n_chunks = p.chunks.size();
+        p.n_todo = uint32_t(probe_items.size());
+    }
+
+    // device memory
+    size_t N = p.n_dirty_texels ? p.n_dirty_texels : 1, A = p.n_all ? p.n_all : 1;
+    std::vector<DTile> dirty_tiles(p.tiles_all.begin(), p.tiles_all.begin() + p.dirty.size());
+    p.tiles_d.alloc(std::max<size_t>(1, p.tiles_all.size()) * sizeof(DTile));
+    p.tex.alloc(N * 64);
+    p.cov_idx.alloc(std::max<size_t>(1, cov_idx.size()) * 4);
+    p.cov_k.alloc(N * 4);
+    p.direct_out.alloc(std::max<size_t>(1, cov_idx.size()) * 16);
+    p.chart.alloc(A * 4);
+    for (DBuf *d : {&p.valid, &p.known_tmp, &p.gathered}) d->alloc(N);
+    for (DBuf *d : {&p.state, &p.known}) d->alloc(A);
+    for (DBuf *d : {&p.hard, &p.gk, &p.soft, &p.ao_raw}) d->alloc(N * 4);
+    for (DBuf *d : {&p.ao, &p.field}) d->alloc(A * 4);
+    for (DBuf *d : {&p.dl, &p.ind}) d->alloc(A * 16);
+    p.posg.alloc(N * 16);
+    p.light.alloc(size_t(p.aw) * p.ah * 16);
+    std::vector<float> w1 = gauss_weights(1), wr = gauss_weights(int(b.gi_filter * p.ds));
+    p.w1.alloc(w1.size() * 4);
+    p.wr.alloc(wr.size() * 4);
+    p.gath_idx.alloc(N * 4);
+    p.gath_count.alloc(16);
+    p.gather_out.alloc(std::max<size_t>(1, cov_idx.size()) * 16);
+    p.select_bytes = lb_select_temp_bytes(uint32_t(N));
+    p.select_temp.alloc(p.select_bytes);
+    for (DBuf *d : {&p.s_ka, &p.s_kb}) d->alloc(N);
+    for (DBuf *d : {&p.s_f1, &p.s_f2}) d->alloc(N * 4);
+    for (DBuf *d : {&p.s_v4, &p.s_e0, &p.s_e1}) d->alloc(N * 16);
+    size_t NP = p.n_probes ? p.n_probes : 1;
+    p.probes.alloc(NP * 64);
+    p.probes_init.alloc(NP * 64);
+    p.probes_b.alloc(NP * 64);
+    p.probe_items.alloc(std::max<size_t>(1, probe_items.size()) * 64);
+    p.probe_slot.alloc(std::max<size_t>(1, probe_slot.size()) * 4);
+    p.pk_a.alloc(NP);
+    p.pk_b.alloc(NP);
+    p.owner.alloc(owner.size() * 4);
+    p.direct_atlas.alloc(size_t(p.aw) * p.ah * 8);
+    p.validity.alloc(size_t(p.aw) * p.ah);
+    p.indirect.alloc(size_t(p.iw) * p.ih * 16);
+    p.indirect_b.alloc(size_t(p.iw) * p.ih * 16);
+    p.has.alloc(size_t(p.iw) * p.ih);
+    p.has_b.alloc(size_t(p.iw) * p.ih);
+    p.counters.alloc(12 * 8);
+
+    cudaStream_t st = p.g->stream;
+    auto up = [&](DBuf &d, const void *src, size_t bytes) {
+        if (bytes) {
+            ck(cudaMemcpyAsync(d.p, src, bytes, cudaMemcpyHostToDevice, st), "upload");
+            p.g->h2d += bytes;
+        }
+    };
+    up(p.tiles_d, p.tiles_all.data(), p.tiles_all.size() * sizeof(DTile));
+    up(p.tex, tex.data(), tex.size() * 64);
+    up(p.cov_idx, cov_idx.data(), cov_idx.size() * 4);
+    up(p.cov_k, cov_k.data(), cov_k.size() * 4);
+    up(p.known, known.data(), known.size());
+    up(p.state, state.data(), state.size());
+    up(p.field, field.data(), field.size() * 4);
+    up(p.ao, ao.data(), ao.size() * 4);
+    up(p.dl, dl.data(), dl.size() * 4);
+    up(p.ind, ind.data(), ind.size() * 4);
+    up(p.owner, owner.data(), owner.size() * 4);
+    up(p.light, light.data(), light.size() * 4);
+    up(p.w1, w1.data(), w1.size() * 4);
+    up(p.wr, wr.data(), wr.size() * 4);
+    up(p.probes_init, probes_init.data(), probes_init.size() * 4);
+    up(p.probe_items, probe_items.data(), probe_items.size() * 64);
+    up(p.probe_slot, probe_slot.data(), probe_slot.size() * 4);
+    ck(cudaStreamSynchronize(st), "upload");
+    p.blocks_direct = warp_blocks(p.g, LB_PASS_DIRECT);
+    p.blocks_gather = warp_blocks(p.g, LB_PASS_GATHER);
+    p.blocks_volume = warp_blocks(p.g, LB_PASS_VOLUME);
+    p.t_prepare = since(t0);
+}
+
+// The graph: everything from the direct pass to the atlas.
+void capture(lb_plan &p) {
+    const lb::SceneHeader &h = p.scene.header;
+    const lb::BakeSettings &b = h.bake;
+    cudaStream_t st = p.g->stream;
+    lbd::Scene S{(const float4 *)p.dscene->nodes, (const float4 *)p.dscene->tris, (const float4 *)p.dscene->mats,
+                 (const float4 *)p.dscene->charts, p.dscene->n_nodes, p.dscene->n_tris, p.dscene->n_mats,
+                 p.dscene->n_charts};
+    const lb_params &params = p.P.params;
+    lb_params pvol = params;
+    if (h.volume) pvol.counts[2] = h.volume->rays;
+    PostArgs a{};
+    a.tiles = p.tiles_d.as<DTile>();
+    a.n_tiles = int(p.dirty.size());
+    a.n_texels = p.n_dirty_texels;
+    a.tex = p.tex.as<float4>();
+    a.cov_k = p.cov_k.as<uint32_t>();
+    a.direct_out = p.direct_out.as<float4>();
+    a.chart = p.chart.as<uint32_t>();
+    a.valid = p.valid.as<uint8_t>();
+    a.state = p.state.as<uint8_t>();
+    a.known = p.known.as<uint8_t>();
+    a.known_tmp = p.known_tmp.as<uint8_t>();
+    a.gathered = p.gathered.as<uint8_t>();
+    a.hard = p.hard.as<uint32_t>();
+    a.gk = p.gk.as<uint32_t>();
+    a.soft = p.soft.as<float>();
+    a.ao_raw = p.ao_raw.as<float>();
+    a.ao = p.ao.as<float>();
+    a.field = p.field.as<float>();
+    a.dl = p.dl.as<float4>();
+    a.ind = p.ind.as<float4>();
+    a.posg = p.posg.as<float4>();
+    a.light = p.light.as<float4>();
+    a.aw = p.aw;
+    a.w1 = p.w1.as<float>();
+    a.inside_share = b.inside_share;
+    a.ao_strength = b.ao_strength;
+    a.ao_contrast = b.ao_contrast;
+    a.ao_floor = b.ao_floor;
+    a.sdf_radius = b.sdf_radius;
+    a.g = p.P.g;
+    a.ds = p.ds;
+    a.sun = make_float3(p.P.sun.x, p.P.sun.y, p.P.sun.z);
+    a.irr = make_float3(h.sun.irradiance[0], h.sun.irradiance[1], h.sun.irradiance[2]);
+    PostScratch s{p.s_ka.as<uint8_t>(), p.s_kb.as<uint8_t>(), p.s_f1.as<float>(), p.s_f2.as<float>(),
+                  p.s_v4.as<float4>(), p.s_e0.as<float4>(), p.s_e1.as<float4>()};
+    unsigned long long *cnt = p.counters.as<unsigned long long>();
+
+    ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        ck(cudaMemsetAsync(cnt, 0, 12 * 8, st), "counters");
+        WarpPass w{};
+        w.S = &S;
+        w.sms = p.g->sms;
+        w.full_count = false;
+        if (p.n_cov) {
+            w.pass = LB_PASS_DIRECT;
+            w.P = &params;
+            w.tex = p.tex.as<float4>();
+            w.idx = p.cov_idx.as<uint32_t>();
+            w.n_host = p.n_cov;
+            w.out = p.direct_out.as<float4>();
+            w.counters = cnt;
+            w.blocks = p.blocks_direct;
+            ck(lb_launch_pass_warp(w, st), "direct pass");
+        }
+        ck(lb_post_direct(a, int(h.lightmap.padding) + 4, s, st), "direct texel passes");
+        ck(lb_select_gathered(a, p.select_temp.p, p.select_bytes, p.gath_idx.as<uint32_t>(), p.gath_count.as<uint32_t>(),
+                              st),
+           "gather selection");
+        for (uint32_t bounce = 0; bounce < b.gi_bounces && p.n_dirty_texels; bounce++) {
+            WarpPass gw{};
+            gw.pass = LB_PASS_GATHER;
+            gw.S = &S;
+            gw.P = &params;
+            gw.tex = p.tex.as<float4>();
+            gw.idx = p.gath_idx.as<uint32_t>();
+            gw.pos = p.posg.as<float4>();
+            gw.n_dev = p.gath_count.as<uint32_t>();
+            gw.light = p.light.as<float4>();
+            gw.n_light = p.aw * p.ah;
+            gw.out = p.gather_out.as<float4>();
+            gw.counters = cnt + 4;
+            gw.sms = p.g->sms;
+            gw.blocks = p.blocks_gather;
+            ck(lb_launch_pass_warp(gw, st), "gather pass");
+            ck(lb_post_bounce(a, p.gather_out.as<float4>(), int(b.gi_filter * p.ds), p.wr.as<float>(),
+                              int(h.lightmap.padding + 2 * p.ds + 2), s, st),
+               "bounce texel passes");
+        }
+        if (p.has_volume) {
+            // the probes the cache holds, then the ones baked here (every launch starts from the same grid)
+            ck(cudaMemcpyAsync(p.probes.p, p.probes_init.p, size_t(p.n_probes) * 64, cudaMemcpyDeviceToDevice, st),
+               "probes");
+            if (p.n_todo) {
+                WarpPass vw{};
+                vw.pass = LB_PASS_VOLUME;
+                vw.S = &S;
+                vw.P = &pvol;
+                vw.tex = p.probe_items.as<float4>();
+                vw.n_host = p.n_todo;
+                vw.light = p.light.as<float4>();
+                vw.n_light = p.aw * p.ah;
+                vw.out = p.probes.as<float4>();
+                vw.slot = p.probe_slot.as<uint32_t>();
+                vw.counters = cnt + 8;
+                vw.sms = p.g->sms;
+                vw.blocks = p.blocks_volume;
+                ck(lb_launch_pass_warp(vw, st), "volume pass");
+            }
+            ck(lb_volume_fill(p.probes.as<float4>(), p.probes_b.as<float4>(), p.pk_a.as<uint8_t>(), p.pk_b.as<uint8_t>(),
+                              p.vsize[0], p.vsize[1], p.vsize[2], 8, st),
+               "volume fill");
+            const lb::VolumeSettings &v = *h.volume;
+            ck(lb_fallback(a, p.probes.as<float4>(), make_float3(v.min[0], v.min[1], v.min[2]), v.step, p.vsize[0],
+                           p.vsize[1], p.vsize[2], st),
+               "fallback");
+        }
+        CompositeArgs c{};
+        c.owner = p.owner.as<uint32_t>();
+        c.known = p.known.as<uint8_t>();
+        c.state = p.state.as<uint8_t>();
+        c.field = p.field.as<float>();
+        c.ao = p.ao.as<float>();
+        c.ind = p.ind.as<float4>();
+        c.aw = p.aw;
+        c.ah = p.ah;
+        c.iw = p.iw;
+        c.ih = p.ih;
+        c.ds = p.ds;
+        c.direct_out = p.direct_atlas.as<float2>();
+        c.validity = p.validity.as<uint8_t>();
+        c.indirect = p.indirect.as<float4>();
+        c.has = p.has.as<uint8_t>();
+        ck(lb_composite(c, p.indirect_b.as<float4>(), p.has_b.as<uint8_t>(), st), "composite");
+    } catch (...) {
+        cudaGraph_t g;
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    ck(cudaStreamEndCapture(st, &p.graph), "end capture");
+    ck(cudaGraphInstantiate(&p.exec, p.graph, 0), "graph instantiate");
+    size_t n_nodes = 0;
+    ck(cudaGraphGetNodes(p.graph, nullptr, &n_nodes), "graph nodes");
+    std::vector<cudaGraphNode_t> nodes(n_nodes);
+    ck(cudaGraphGetNodes(p.graph, nodes.data(), &n_nodes), "graph nodes");
+    p.kernel_nodes = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) p.kernel_nodes++;
+    }
+}
+
+template <class T> std::vector<T> down(lb_plan &p, const DBuf &d, size_t n, size_t off = 0) {
+    std::vector<T> v(n);
+    if (n) {
+        ck(cudaMemcpyAsync(v.data(), (const char *)d.p + off * sizeof(T), n * sizeof(T), cudaMemcpyDeviceToHost,
+                           p.g->stream),
+           "download");
+        p.g->d2h += n * sizeof(T);
+    }
+    return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+lb_plan *lb_plan_create(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_options *opts) {
+    if (!g || !scene) {
+        lb_set_error("lb_plan_create: bad arguments");
+        return nullptr;
+    }
+    try {
+        ck(cudaSetDevice(g->device), "cudaSetDevice");
+        auto p = std::make_unique<lb_plan>();
+        p->g = g;
+        p->scene = lb::Scene::read(scene, len);
+        if (opts && opts->cache_dir) p->opt.cache = opts->cache_dir;
+        if (opts && opts->log) {
+            auto fn = opts->log;
+            void *ctx = opts->log_ctx;
+            p->opt.log = [fn, ctx](const std::string &s) { fn(ctx, s.c_str()); };
+        }
+        build(*p);
+        capture(*p);
+        if (p->opt.log)
+            p->opt.log(std::to_string(p->dirty.size()) + " of " + std::to_string(p->P.layout.tiles.size()) +
+                       " tiles to bake on the device, " + std::to_string(p->n_cov) + " texels, " +
+                       std::to_string(p->n_todo) + " probes");
+        return p.release();
+    } catch (const std::exception &e) {
+        lb_set_error(e.what());
+    }
+    return nullptr;
+}
+
+int lb_plan_launch(lb_plan *p) {
+    if (!p) return LB_EINVAL;
+    cudaError_t e = cudaGraphLaunch(p->exec, p->g->stream);
+    if (e != cudaSuccess) return lb_cuda_fail(e, "lb_plan_launch");
+    return LB_OK;
+}
+
+int lb_plan_rays(lb_plan *p, uint64_t rays[3]) {
+    if (!p || !rays) return LB_EINVAL;
+    unsigned long long c[12];
+    cudaError_t e = cudaMemcpyAsync(c, p->counters.p, sizeof c, cudaMemcpyDeviceToHost, p->g->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(p->g->stream);
+    if (e != cudaSuccess) return lb_cuda_fail(e, "lb_plan_rays");
+    rays[0] = c[0];
+    rays[1] = c[4];
+    rays[2] = c[8];
+    return LB_OK;
+}
+
+int lb_plan_kernels(const lb_plan *p) { return p ? p->kernel_nodes : 0; }
+
+void lb_plan_free(lb_plan *p) {
+    if (p) {
+        cudaStreamSynchronize(p->g->stream);
+        delete p;
+    }
+}
+
+}  // extern "C"
+
+const lb::Scene &lb_plan_scene(const lb_plan &p) { return p.scene; }
+
+// The results of the last launch, as a bake (downloads, the cache writes).
+lb::Bake lb_plan_collect(lb_plan &p) {
+    const lb::SceneHeader &h = p.scene.header;
+    auto t0 = std::chrono::steady_clock::now();
+    lb::Bake out;
+    size_t A = size_t(p.aw) * p.ah;
+    std::vector<float> dir = down<float>(p, p.direct_atlas, A * 2);
+    std::vector<uint8_t> val = down<uint8_t>(p, p.validity, A);
+    std::vector<float> ind = down<float>(p, p.indirect, size_t(p.iw) * p.ih * 4);
+    std::vector<float> probes;
+    if (p.has_volume) probes = down<float>(p, p.probes, size_t(p.n_probes) * 16);
+    uint64_t rays[3];
+    if (lb_plan_rays(&p, rays) != LB_OK) throw std::runtime_error(lb_last_error());
+    out.direct.resize(A);
+    std::memcpy(out.direct.data(), dir.data(), A * 8);
+    out.validity = std::move(val);
+    out.indirect.resize(size_t(p.iw) * p.ih);
+    for (size_t i = 0; i < out.indirect.size(); i++) out.indirect[i] = {ind[i * 4], ind[i * 4 + 1], ind[i * 4 + 2]};
+    out.iw = p.iw;
+    out.ih = p.ih;
+    if (p.has_volume) {
+        lb::Volume v;
+        v.origin = h.volume->min;
+        v.step = h.volume->step;
+        v.size = p.vsize;
+        v.probes.resize(p.n_probes);
+        std::memcpy(v.probes.data(), probes.data(), probes.size() * 4);
+        v.chunks = p.n_chunks;
+        v.chunks_baked = p.chunk_keys.size();
+        out.volume = std::move(v);
+    }
+    lb::Cache cache(p.opt.cache);
+    if (!p.opt.cache.empty()) {
+        // the dirty tiles' light for the cache (bake.rs:360-362), and the probe chunks (volume.rs:81-84)
+        std::vector<uint8_t> kn = down<uint8_t>(p, p.known, p.n_dirty_texels), stt = down<uint8_t>(p, p.state, p.n_dirty_texels);
+        std::vector<float> fd = down<float>(p, p.field, p.n_dirty_texels), ao = down<float>(p, p.ao, p.n_dirty_texels);
+        std::vector<float> dl = down<float>(p, p.dl, size_t(p.n_dirty_texels) * 4),
+                           id = down<float>(p, p.ind, size_t(p.n_dirty_texels) * 4);
+        ck(cudaStreamSynchronize(p.g->stream), "download");
+        for (size_t k = 0; k < p.dirty.size(); k++) {
+            const DTile &t = p.tiles_all[k];
+            size_t n = size_t(t.w) * t.h;
+            lb::TileLight l;
+            l.known.assign(kn.begin() + t.off, kn.begin() + t.off + n);
+            l.state.assign(stt.begin() + t.off, stt.begin() + t.off + n);
+            l.field.assign(fd.begin() + t.off, fd.begin() + t.off + n);
+            l.ao.assign(ao.begin() + t.off, ao.begin() + t.off + n);
+            l.direct.resize(n);
+            l.indirect.resize(n);
+            for (size_t i = 0; i < n; i++) {
+                size_t d = (t.off + i) * 4;
+                l.direct[i] = {dl[d], dl[d + 1], dl[d + 2]};
+                l.indirect[i] = {id[d], id[d + 1], id[d + 2]};
+            }
+            cache.put("tile", p.hashes[p.dirty[k]], l.pack());
+        }
+        if (p.has_volume)
+            for (auto &kv : p.chunk_keys) {
+                std::vector<uint8_t> bytes(kv.second.size() * 64);
+                for (size_t i = 0; i < kv.second.size(); i++)
+                    std::memcpy(bytes.data() + i * 64, &probes[size_t(kv.second[i]) * 16], 64);
+                cache.put("probes", kv.first, bytes);
+            }
+    }
+    out.layout = p.P.layout;
+    lb::Stats &s = out.stats;
+    s.tiles = p.P.layout.tiles.size();
+    s.tiles_baked = p.dirty.size();
+    s.texels_baked = p.n_cov;
+    s.chunks = p.n_chunks;
+    s.chunks_baked = p.chunk_keys.size();
+    s.rays_direct = rays[0];
+    s.rays_gather = rays[1];
+    s.rays_volume = rays[2];
+    s.t_layout = p.t_prepare;
+    s.t_composite = since(t0);
+    return out;
+}

@@ -1,4 +1,5 @@
 // The C ABI's host side: prepared scenes, the bake entry point and the file writers.
+#include <chrono>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -8,6 +9,7 @@
 #include "bake.h"
 #include "blake3.h"
 #include "encode.h"
+#include "handles.h"
 #include "raster.h"
 
 struct lb_prepared {
@@ -15,10 +17,6 @@ struct lb_prepared {
     lb::Prepared prep;
 };
 
-struct lb_bake {
-    lb::Scene scene;
-    lb::Bake bake;
-};
 
 namespace {
 
@@ -205,6 +203,29 @@ lb_bake *lb_bake_run_with(const lb_tracer *t, const uint8_t *scene, size_t len, 
 }
 
 void lb_bake_free(lb_bake *b) { delete b; }
+
+lb_bake *lb_plan_result(lb_plan *p) {
+    return guard(
+        [&]() -> lb_bake * {
+            if (!p) throw std::runtime_error("lb_plan_result: no plan");
+            auto b = std::make_unique<lb_bake>();
+            b->scene = lb_plan_scene(*p);
+            b->bake = lb_plan_collect(*p);
+            return b.release();
+        },
+        nullptr);
+}
+
+lb_bake *lb_bake_device(lb_gpu *gpu, const uint8_t *scene, size_t len, const lb_bake_options *opts) {
+    auto t0 = std::chrono::steady_clock::now();
+    lb_plan *p = lb_plan_create(gpu, scene, len, opts);
+    if (!p) return nullptr;
+    lb_bake *b = nullptr;
+    if (lb_plan_launch(p) == LB_OK) b = lb_plan_result(p);
+    lb_plan_free(p);
+    if (b) b->bake.stats.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return b;
+}
 
 int lb_bake_get_info(const lb_bake *b, lb_bake_info *o) {
     if (!b || !o) return LB_EINVAL;

@@ -15,3 +15,28 @@ struct Scene;
 cudaError_t lb_launch_pass_bvh2(int pass, const lbd::Scene &S, const lb_params &P, const float4 *items, uint32_t n,
                                 uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
                                 unsigned long long *counters, bool full_count, cudaStream_t stream);
+
+// A warp-per-item pass (passes_warp.cu). Items are tex[idx[k]] (or tex[k] without idx), k < *n_dev
+// (or n_host); the gather pass may take positions from `pos` (indexed like tex records).
+struct WarpPass {
+    int pass;
+    const lbd::Scene *S;
+    const lb_params *P;
+    const float4 *tex;        // 4 float4 a texel record
+    const uint32_t *idx;      // optional
+    const float4 *pos;        // optional (gather)
+    const uint32_t *n_dev;    // optional (direct, gather)
+    uint32_t n_host;
+    uint32_t base;
+    const float4 *light;
+    uint32_t n_light;
+    float4 *out;
+    const uint32_t *slot;     // optional (volume): where probe k's records go
+    unsigned long long *counters;
+    bool full_count;
+    int sms;
+    int blocks;               // 0: as many as fit on the device at once
+};
+cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream);
+// The persistent grid's size for a pass: SMs x resident blocks of 256 threads.
+int lb_warp_pass_blocks(const WarpPass &w);

@@ -1,0 +1,62 @@
+// The device bake's per-texel state and the launchers of its texel passes (post.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+// A tile in the device's texel arrays: its rectangle in the atlas and its first texel.
+struct DTile {
+    uint32_t x, y, w, h;
+    uint32_t off;
+};
+
+// Arrays over the dirty tiles' texels (n_texels, the tiles in `tiles`, concatenated), and the atlas.
+struct PostArgs {
+    const DTile *tiles;
+    int n_tiles;
+    uint32_t n_texels;
+    const float4 *tex;          // 4 float4 a texel (raster.rs Texel)
+    const uint32_t *cov_k;      // a covered texel's index in the direct pass's list
+    const float4 *direct_out;   // the direct pass's records
+    uint32_t *chart;            // covered: its chart; else 0xffffffff
+    uint8_t *valid, *state, *known, *known_tmp, *gathered;
+    uint32_t *hard, *gk;
+    float *soft, *ao_raw, *ao, *field;
+    float4 *dl, *ind, *posg;
+    float4 *light;              // the atlas the gathers read
+    uint32_t aw;
+    const float *w1;            // smooth weights, radius 1
+    float inside_share, ao_strength, ao_contrast, ao_floor, sdf_radius;
+    uint32_t g, ds;
+    float3 sun, irr;
+};
+
+struct PostScratch {
+    uint8_t *known_a, *known_b;
+    float *f1, *f2;
+    float4 *v4, *e0, *e1;
+};
+
+struct CompositeArgs {
+    const uint32_t *owner;      // per atlas texel: its texel in the device arrays (all tiles), or none
+    const uint8_t *known, *state;
+    const float *field, *ao;
+    const float4 *ind;
+    uint32_t aw, ah, iw, ih, ds;
+    float2 *direct_out;
+    uint8_t *validity;
+    float4 *indirect;
+    uint8_t *has;
+};
+
+cudaError_t lb_post_direct(const PostArgs &a, int rings, PostScratch &s, cudaStream_t st);
+size_t lb_select_temp_bytes(uint32_t n);
+cudaError_t lb_select_gathered(const PostArgs &a, void *temp, size_t temp_bytes, uint32_t *idx, uint32_t *count,
+                               cudaStream_t st);
+cudaError_t lb_post_bounce(const PostArgs &a, const float4 *res, int r, const float *w, int rings, PostScratch &s,
+                           cudaStream_t st);
+cudaError_t lb_volume_fill(float4 *probes, float4 *scratch, uint8_t *ka, uint8_t *kb, uint32_t nx, uint32_t ny,
+                           uint32_t nz, int rings, cudaStream_t st);
+cudaError_t lb_fallback(const PostArgs &a, const float4 *probes, float3 origin, float step, uint32_t nx, uint32_t ny,
+                        uint32_t nz, cudaStream_t st);
+cudaError_t lb_composite(const CompositeArgs &c, float4 *scratch, uint8_t *has_b, cudaStream_t st);

@@ -19,6 +19,7 @@ struct lb_gpu {
     char name[256] = {0};
     cudaStream_t stream = nullptr;
     bool counting = false;
+    int kernel = 0;  // lb_run's kernels: 0 a thread an item, 1 a warp an item
     unsigned long long *counters = nullptr;       // device: rays, nodes, tris, mats
     unsigned long long *host_counters = nullptr;  // pinned copy, written by the stream
     lb_counters last = {};

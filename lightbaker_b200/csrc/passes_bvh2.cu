@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(128) direct_kernel(Scene S, lb_params P, const
                 float cx = ((__uint2float_rn(s % g) + 0.5f) / fg - 0.5f) * span;
                 float cy = ((__uint2float_rn(s / g) + 0.5f) / fg - 0.5f) * span;
                 float3 o = add(add(add(at, scl(dx, cx)), scl(dy, cy)), lift);
-                if (trace<COUNT>(S, o, sun, FAR, true, key + s, seed, c).tri == NONE) hard |= 1u << s;
+                if (trace<COUNT>(S, o, sun, FAR, true, key + s, seed, c).tri == NONE) hard |= 1u << (s & 31u);  // WGSL shifts modulo the bit width
                 uint32_t k = (s + turn) % gg;
                 float3 d = sun_disc(P, sf, k, gg);
                 if (trace<COUNT>(S, o, d, FAR, true, key + s + 1000u, seed, c).tri == NONE) soft += 1.0f;

@@ -1,0 +1,386 @@
+// The three ray passes with a warp on each item (crates/lightbaker/src/gpu/trace.wgsl:170-324), for
+// the device-resident bake. The shader runs an item's rays one after another in one thread; here the 32
+// lanes of a warp trace 32 of the item's rays at once: the 16 rays of an inside test, the 16 hard and 16
+// soft sun rays of a 4 x 4 grid, 32 occlusion or gather rays at a time. Rays of one item start at the
+// same point (or within one texel) and their walks visit the same nodes, so a warp's loads coalesce
+// and its lanes stay together far longer than with 32 items' rays. Sums the shader builds ray by ray
+// (occlusion, bounced light, the L1 coefficients) are built in the same ray order here too (a lane
+// adds its neighbours' terms in turn), so the records are bit-identical to the shader's.
+//
+// Persistent: a grid of (SMs x resident warps) walks the items with a stride. The item count may live
+// in device memory (read at launch), so a pass can follow a device-side compaction in a CUDA graph.
+#include <cuda_runtime.h>
+
+#include "lb_device.cuh"
+#include "lb_kernels.h"
+
+namespace lbd {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// Adds the lanes' terms (those whose flag is set) to `sum` in lane order: the order a sequential loop
+// over the rays would add them.
+__device__ __forceinline__ float ordered_add(float sum, float term, bool on) {
+    unsigned mask = __ballot_sync(FULL, on);
+    for (int l = 0; l < 32; l++) {
+        float v = __shfl_sync(FULL, term, l);
+        if (mask & (1u << l)) sum += v;
+    }
+    return sum;
+}
+__device__ __forceinline__ float3 ordered_add3(float3 sum, float3 term, bool on) {
+    unsigned mask = __ballot_sync(FULL, on);
+    for (int l = 0; l < 32; l++) {
+        float x = __shfl_sync(FULL, term.x, l), y = __shfl_sync(FULL, term.y, l), z = __shfl_sync(FULL, term.z, l);
+        if (mask & (1u << l)) sum = add(sum, mk(x, y, z));
+    }
+    return sum;
+}
+
+// An item: its record (pos, normal, dx, dy), the position optionally taken from a second array
+// (the texel's sample point moved by the direct pass, bake.rs:227-238).
+struct Item {
+    float4 pos, nrm, dx, dy;
+};
+__device__ __forceinline__ Item load_item(const float4 *tex, const uint32_t *idx, const float4 *pos_override,
+                                          uint32_t k) {
+    uint32_t t = idx ? __ldg(&idx[k]) : k;
+    Item it;
+    it.pos = pos_override ? __ldg(&pos_override[t]) : __ldg(&tex[4 * t]);
+    it.nrm = __ldg(&tex[4 * t + 1]);
+    it.dx = __ldg(&tex[4 * t + 2]);
+    it.dy = __ldg(&tex[4 * t + 3]);
+    return it;
+}
+
+// trace.wgsl:159-168 with lanes 0..15 each tracing one of the 16 rays; true on every lane when more than
+// insideShare of them meet back faces. The count of back faces is exact, as the shader's float sum of ones.
+template <bool COUNT>
+__device__ __forceinline__ bool inside_warp(const Scene &S, const lb_params &P, uint32_t seed, float3 o, float3 n,
+                                            uint32_t key, int lane, Count &c) {
+    bool back = false;
+    if (lane < 16) {
+        Frame f = frame(n);
+        uint32_t r = uint32_t(lane);
+        float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
+        Hit h = trace<COUNT>(S, o, d, P.ground[3], false, key + r + 7000u, seed, c);
+        back = h.tri != NONE && h.back;
+    }
+    float nb = __uint2float_rn(__popc(__ballot_sync(FULL, back)));
+    return nb / 16.0f > __uint_as_float(P.atlas[3]);
+}
+
+template <bool COUNT>
+__device__ __forceinline__ void flush_counts(Count &c, unsigned long long *counters) {
+    for (int o = 16; o > 0; o >>= 1) {
+        c.rays += __shfl_down_sync(FULL, c.rays, o);
+        if (COUNT) {
+            c.nodes += __shfl_down_sync(FULL, c.nodes, o);
+            c.tris += __shfl_down_sync(FULL, c.tris, o);
+            c.mats += __shfl_down_sync(FULL, c.mats, o);
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&counters[0], (unsigned long long)c.rays);
+        if (COUNT) {
+            atomicAdd(&counters[1], (unsigned long long)c.nodes);
+            atomicAdd(&counters[2], (unsigned long long)c.tris);
+            atomicAdd(&counters[3], (unsigned long long)c.mats);
+        }
+    }
+}
+
+// trace.wgsl:170-243
+template <bool COUNT>
+__global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
+                                                   const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
+                                                   unsigned long long *counters) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t n = n_dev ? *n_dev : n_host;
+    const uint32_t seed = __float_as_uint(P.reach[3]);
+    Count c;
+    c.zero();
+    for (uint32_t k = warp; k < n; k += warps) {
+        Item it = load_item(tex, idx, nullptr, k);
+        float3 nrm = xyz(it.nrm), pos = xyz(it.pos), dx = xyz(it.dx), dy = xyz(it.dy);
+        uint32_t key = (base + k) * 7919u;
+        uint32_t g = P.counts[0];
+        float3 sun = xyz(P.sun_dir);
+        float3 lift = scl(nrm, P.reach[2]);
+        float3 at = pos;
+        uint32_t pick = 0u;
+        float span = 1.0f;
+        if (inside_warp<COUNT>(S, P, seed, add(at, lift), nrm, key, lane, c)) {
+            for (uint32_t q = 1u; q < 9u; q++) {
+                float2 cc = offset(q);
+                float3 p = add(add(pos, scl(dx, cc.x)), scl(dy, cc.y));
+                if (!inside_warp<COUNT>(S, P, seed, add(p, lift), nrm, key + q * 31u, lane, c)) {
+                    at = p;
+                    pick = q;
+                    span = 0.4f;
+                    break;
+                }
+            }
+            if (pick == 0u) {
+                float3 p = add(pos, scl(nrm, PUSH));
+                if (!inside_warp<COUNT>(S, P, seed, add(p, lift), nrm, key + 331u, lane, c)) {
+                    at = p;
+                    pick = 9u;
+                    span = 0.4f;
+                }
+            }
+        }
+        float soft = 0.0f;
+        uint32_t hard = 0u;
+        if (dot3(sun, nrm) > 0.0f) {
+            Frame sf = frame(sun);
+            uint32_t gg = g * g;
+            float fg = __uint2float_rn(g), fgg = __uint2float_rn(gg);
+            uint32_t turn = uint32_t(rnd(key, 17u, seed) * fgg);
+            uint32_t nsoft = 0;
+            // a pair of rays a cell: lanes 0..15 the hard ray of cell s0 + lane, lanes 16..31 the soft one
+            for (uint32_t s0 = 0; s0 < gg; s0 += 16) {
+                uint32_t s = s0 + uint32_t(lane & 15);
+                bool escaped = false;
+                if (s < gg) {
+                    float cx = ((__uint2float_rn(s % g) + 0.5f) / fg - 0.5f) * span;
+                    float cy = ((__uint2float_rn(s / g) + 0.5f) / fg - 0.5f) * span;
+                    float3 o = add(add(add(at, scl(dx, cx)), scl(dy, cy)), lift);
+                    if (lane < 16) {
+                        escaped = trace<COUNT>(S, o, sun, FAR, true, key + s, seed, c).tri == NONE;
+                    } else {
+                        float3 d = sun_disc(P, sf, (s + turn) % gg, gg);
+                        escaped = trace<COUNT>(S, o, d, FAR, true, key + s + 1000u, seed, c).tri == NONE;
+                    }
+                }
+                unsigned m = __ballot_sync(FULL, escaped);
+                hard |= (m & 0xffffu) << (s0 & 31u);  // the shader shifts modulo 32
+                nsoft += __popc(m >> 16);
+            }
+            soft = __uint2float_rn(nsoft) / fgg;
+        }
+        Frame f = frame(nrm);
+        float3 o = add(at, lift);
+        uint32_t rays = P.counts[1];
+        float frays = __uint2float_rn(rays);
+        float s1 = rnd(key, 3u, seed), s2 = rnd(key, 5u, seed);
+        float occ = 0.0f;
+        uint32_t nback = 0;
+        for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
+            uint32_t r = r0 + uint32_t(lane);
+            bool hit = false, bk = false;
+            float term = 0.0f;
+            if (r < rays) {
+                float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
+                Hit h = trace<COUNT>(S, o, d, P.reach[0], false, key + r + 2000u, seed, c);
+                if (h.tri != NONE) {
+                    hit = true;
+                    float kk = h.t / P.reach[0];
+                    term = 1.0f - kk * kk;
+                    bk = h.back && h.t < P.ground[3];
+                }
+            }
+            occ = ordered_add(occ, term, hit);
+            nback += __popc(__ballot_sync(FULL, bk));
+        }
+        if (lane == 0)
+            out[k] = make_float4(soft, __uint_as_float(hard | (pick << 24u)), occ / frays, __uint2float_rn(nback) / frays);
+    }
+    flush_counts<COUNT>(c, counters);
+}
+
+// trace.wgsl:245-270
+template <bool COUNT>
+__global__ void __launch_bounds__(256) gather_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
+                                                   const float4 *pos_override, const uint32_t *n_dev, uint32_t n_host,
+                                                   uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
+                                                   unsigned long long *counters) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t n = n_dev ? *n_dev : n_host;
+    const uint32_t seed = __float_as_uint(P.reach[3]);
+    Count c;
+    c.zero();
+    for (uint32_t k = warp; k < n; k += warps) {
+        Item it = load_item(tex, idx, pos_override, k);
+        float3 nrm = xyz(it.nrm), pos = xyz(it.pos), dx = xyz(it.dx), dy = xyz(it.dy);
+        Frame f = frame(nrm);
+        uint32_t key = (base + k) * 7919u;
+        uint32_t rays = P.counts[2];
+        float frays = __uint2float_rn(rays);
+        float s1 = rnd(key, 11u, seed), s2 = rnd(key, 13u, seed);
+        float3 sum = mk(0.f, 0.f, 0.f);
+        uint32_t nback = 0;
+        for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
+            uint32_t r = r0 + uint32_t(lane);
+            bool on = false, bk = false;
+            float3 term = mk(0.f, 0.f, 0.f);
+            if (r < rays) {
+                float jx = rnd(key + r, 19u, seed) - 0.5f, jy = rnd(key + r, 23u, seed) - 0.5f;
+                float3 o = add(add(add(pos, scl(dx, jx)), scl(dy, jy)), scl(nrm, P.reach[2]));
+                float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
+                Hit h = trace<COUNT>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c);
+                if (h.tri == NONE) {
+                    term = sky(P, d);
+                    on = true;
+                } else if (h.back) {
+                    bk = true;
+                } else {
+                    term = bounced(S, P, light, n_light, o, d, h);
+                    on = true;
+                }
+            }
+            sum = ordered_add3(sum, term, on);
+            nback += __popc(__ballot_sync(FULL, bk));
+        }
+        if (lane == 0) {
+            float3 e = scl(sum, PI);
+            out[k] = make_float4(e.x / frays, e.y / frays, e.z / frays, __uint2float_rn(nback) / frays);
+        }
+    }
+    flush_counts<COUNT>(c, counters);
+}
+
+// trace.wgsl:272-324. `slot` (optional) scatters probe k's four records to 4 * slot[k].
+template <bool COUNT>
+__global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const float4 *tex, uint32_t n, const float4 *light,
+                                                   uint32_t n_light, float4 *out, const uint32_t *slot,
+                                                   unsigned long long *counters) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t seed = __float_as_uint(P.reach[3]);
+    Count c;
+    c.zero();
+    for (uint32_t k = warp; k < n; k += warps) {
+        float3 o = xyz(__ldg(&tex[4 * k]));
+        uint32_t key = __float_as_uint(__ldg(&tex[4 * k + 1]).w) * 7919u + 77u;
+        uint32_t rays = P.counts[2];
+        float frays = __uint2float_rn(rays);
+        float s1 = rnd(key, 29u, seed), s2 = rnd(key, 31u, seed);
+        float3 l0 = mk(0.f, 0.f, 0.f), l1x = l0, l1y = l0, l1z = l0;
+        uint32_t nback = 0;
+        for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
+            uint32_t r = r0 + uint32_t(lane);
+            bool on = r < rays, bk = false;
+            float3 t0 = mk(0.f, 0.f, 0.f), tx = t0, ty = t0, tz = t0;
+            if (on) {
+                float u = fract((__uint2float_rn(r) + 0.5f) / frays + s1);
+                float v = fract(radical(r) + s2);
+                float z = 1.0f - 2.0f * u;
+                float rr = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+                float a = v * 2.0f * PI;
+                float sa, ca;
+                sincos32(a, &sa, &ca);
+                float3 d = mk(rr * ca, z, rr * sa);
+                Hit h = trace<COUNT>(S, o, d, P.reach[1], false, key + r, seed, c);
+                float3 l = sky(P, d);
+                if (h.tri != NONE) {
+                    bk = h.back;
+                    l = h.back ? mk(0.f, 0.f, 0.f) : bounced(S, P, light, n_light, o, d, h);
+                }
+                t0 = scl(l, 0.282095f);
+                float3 lw = scl(l, 0.488603f);
+                tx = scl(lw, d.x);
+                ty = scl(lw, d.y);
+                tz = scl(lw, d.z);
+            }
+            l0 = ordered_add3(l0, t0, on);
+            l1x = ordered_add3(l1x, tx, on);
+            l1y = ordered_add3(l1y, ty, on);
+            l1z = ordered_add3(l1z, tz, on);
+            nback += __popc(__ballot_sync(FULL, bk));
+        }
+        float w = 4.0f * PI / frays;
+        uint32_t g = P.counts[0], gg = g * g;
+        Frame sf = frame(xyz(P.sun_dir));
+        uint32_t nsun = 0;
+        for (uint32_t s0 = 0; s0 < gg; s0 += 32) {
+            uint32_t s = s0 + uint32_t(lane);
+            bool esc = false;
+            if (s < gg) {
+                float3 d = sun_disc(P, sf, s, gg);
+                esc = trace<COUNT>(S, o, d, FAR, true, key + s + 9000u, seed, c).tri == NONE;
+            }
+            nsun += __popc(__ballot_sync(FULL, esc));
+        }
+        if (lane < 4) {
+            float3 a0 = scl(l0, w), ax = scl(l1x, w), ay = scl(l1y, w), az = scl(l1z, w);
+            float4 rec;
+            if (lane == 0) rec = make_float4(a0.x, a0.y, a0.z, __uint2float_rn(nsun) / __uint2float_rn(gg));
+            else if (lane == 1) rec = make_float4(ax.x, ax.y, ax.z, __uint2float_rn(nback) / frays);
+            else if (lane == 2) rec = make_float4(ay.x, ay.y, ay.z, 0.0f);
+            else rec = make_float4(az.x, az.y, az.z, 0.0f);
+            uint32_t dst = slot ? __ldg(&slot[k]) : k;
+            out[4 * dst + lane] = rec;
+        }
+    }
+    flush_counts<COUNT>(c, counters);
+}
+
+}  // namespace lbd
+
+int lb_warp_pass_blocks(const WarpPass &w) {
+    const int T = 256;
+    int per_sm = 0;
+    cudaError_t e;
+    bool count = w.full_count;
+    switch (w.pass) {
+    case LB_PASS_DIRECT:
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, count ? lbd::direct_warp<true> : lbd::direct_warp<false>, T, 0);
+        break;
+    case LB_PASS_GATHER:
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, count ? lbd::gather_warp<true> : lbd::gather_warp<false>, T, 0);
+        break;
+    default:
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, count ? lbd::volume_warp<true> : lbd::volume_warp<false>, T, 0);
+        break;
+    }
+    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    return w.sms * per_sm;
+}
+
+cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream) {
+    const int T = 256;
+    bool count = w.full_count;
+    int blocks = w.blocks > 0 ? w.blocks : lb_warp_pass_blocks(w);
+    if (w.n_dev == nullptr) {
+        // no more warps than items
+        uint32_t need = (w.n_host + (T / 32) - 1) / (T / 32);
+        if (need == 0) return cudaSuccess;
+        if ((uint32_t)blocks > need) blocks = (int)need;
+    }
+    switch (w.pass) {
+    case LB_PASS_DIRECT:
+        if (count)
+            lbd::direct_warp<true><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base, w.out,
+                                                             w.counters);
+        else
+            lbd::direct_warp<false><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base,
+                                                              w.out, w.counters);
+        break;
+    case LB_PASS_GATHER:
+        if (count)
+            lbd::gather_warp<true><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host, w.base,
+                                                             w.light, w.n_light, w.out, w.counters);
+        else
+            lbd::gather_warp<false><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host,
+                                                              w.base, w.light, w.n_light, w.out, w.counters);
+        break;
+    default:
+        if (count)
+            lbd::volume_warp<true><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light, w.out,
+                                                             w.slot, w.counters);
+        else
+            lbd::volume_warp<false><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light, w.out,
+                                                              w.slot, w.counters);
+        break;
+    }
+    return cudaGetLastError();
+}

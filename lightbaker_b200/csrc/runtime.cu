@@ -242,6 +242,12 @@ int lb_get_transfer(lb_gpu *g, uint64_t *h2d, uint64_t *d2h, int reset) {
     return LB_OK;
 }
 
+int lb_set_pass_kernel(lb_gpu *g, int kind) {
+    if (!g || kind < 0 || kind > 1) return LB_EINVAL;
+    g->kernel = kind;
+    return LB_OK;
+}
+
 int lb_set_counting(lb_gpu *g, int on) {
     if (!g) return LB_EINVAL;
     g->counting = on != 0;
@@ -264,8 +270,26 @@ int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const fl
     lbd::Scene S{(const float4 *)s->nodes, (const float4 *)s->tris, (const float4 *)s->mats, (const float4 *)s->charts,
                  s->n_nodes, s->n_tris, s->n_mats, s->n_charts};
     LB_CUDA(cudaMemsetAsync(g->counters, 0, 4 * sizeof(unsigned long long), g->stream), "counters");
-    LB_CUDA(lb_launch_pass_bvh2(pass, S, P, items, n, base, light, n_light, out, g->counters, g->counting, g->stream),
-            "pass launch");
+    if (g->kernel == 1) {
+        WarpPass w{};
+        w.pass = pass;
+        w.S = &S;
+        w.P = &P;
+        w.tex = items;
+        w.n_host = n;
+        w.base = base;
+        w.light = light;
+        w.n_light = n_light;
+        w.out = out;
+        w.counters = g->counters;
+        w.full_count = g->counting;
+        w.sms = g->sms;
+        LB_CUDA(lb_launch_pass_warp(w, g->stream), "pass launch");
+    } else {
+        LB_CUDA(lb_launch_pass_bvh2(pass, S, P, items, n, base, light, n_light, out, g->counters, g->counting,
+                                    g->stream),
+                "pass launch");
+    }
     LB_CUDA(cudaMemcpyAsync(g->host_counters, g->counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                             g->stream),
             "counters");

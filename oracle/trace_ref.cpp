@@ -317,7 +317,7 @@ void direct_item(const Ctx &C, const lb_texel &tx, uint32_t index, float *out) {
             float cx = ((float(s % g) + 0.5f) / float(g) - 0.5f) * span;
             float cy = ((float(s / g) + 0.5f) / float(g) - 0.5f) * span;
             V3<float> o = ((at + dx * cx) + dy * cy) + lift;
-            if (trace<float>(C, o, sun, FAR, true, key + s).tri == NONE) hard |= 1u << s;
+            if (trace<float>(C, o, sun, FAR, true, key + s).tri == NONE) hard |= 1u << (s & 31u);  // WGSL: the shift is taken modulo 32
             uint32_t k = (s + uint32_t(rnd(key, 17u, C.seed) * float(gg))) % gg;
             V3<float> d = sun_disc(C, sf, k, gg);
             if (trace<float>(C, o, d, FAR, true, key + s + 1000u).tri == NONE) soft += 1.0f;

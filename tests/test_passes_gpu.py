@@ -33,8 +33,9 @@ def _compare(gpu_out, cpu_out, what):
                           f"gpu {gpu_out[bad[:3]]} oracle {cpu_out[bad[:3]]}"
 
 
+@pytest.mark.parametrize("kernel", [0, 1], ids=["thread_per_item", "warp_per_item"])
 @pytest.mark.parametrize("name,limit", [("reference_test", 20000), ("small_map", 20000), ("map_100m", 3000)])
-def test_passes_bit_exact(gpu, oracle_mod, name, limit):
+def test_passes_bit_exact(gpu, oracle_mod, name, limit, kernel):
     scene = scenes.WORKLOADS[name]()
     P = lb.prepare(scene)
     buffers = gpu.scene(P.nodes, P.tris, P.materials, P.charts)
@@ -44,6 +45,7 @@ def test_passes_bit_exact(gpu, oracle_mod, name, limit):
     # a spread sample across the map, in list order (keys follow the index)
     idx = np.sort(rng.choice(len(items), size=min(limit, len(items)), replace=False))
     items = items[idx]
+    gpu.set_pass_kernel(kernel)
     gpu.set_counting(True)
     g = gpu.run(lb.Pass.DIRECT, buffers, P.params, items)
     gc = gpu.counters()
@@ -70,6 +72,7 @@ def test_passes_bit_exact(gpu, oracle_mod, name, limit):
     c, _ = oracle_mod.run(2, sc, P.params, probes, light)
     _compare(g, c, f"{name} volume")
     gpu.set_counting(False)
+    gpu.set_pass_kernel(0)
 
 
 def test_empty_and_edge_cases(gpu, oracle_mod):
