@@ -195,6 +195,40 @@ def reference_arm(args):
         "e2e": {"value": value, "unit": "Grays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def kernel_only(args):
+    """One pass kind alone over a slice of the workload's items, for a profiler: no flush, no bake."""
+    import torch
+    import lightbaker_b200 as lb
+    scene, P, direct, gather, probes, light = load_workload(args.workload, 0)
+    items = (direct if args.kernel_only == "direct" else gather)[: args.items]
+    gpu = lb.Gpu.new(0)
+    gpu.set_pass_kernel(1)
+    buffers = gpu.scene(P.nodes, P.tris, P.materials, P.charts)
+    dev = torch.device("cuda", 0)
+    d_items = torch.from_numpy(items.view(np.uint8).reshape(-1)).to(dev)
+    d_light = torch.from_numpy(light.view(np.uint8).reshape(-1)).to(dev)
+    out = torch.empty(len(items) * 16, dtype=torch.uint8, device=dev)
+    pass_ = lb.Pass.DIRECT if args.kernel_only == "direct" else lb.Pass.GATHER
+    stream = torch.cuda.ExternalStream(gpu.stream, device=dev)
+    times = []
+    for i in range(args.warmup + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        gpu.run_async(pass_, buffers, P.params, d_items.data_ptr(), len(items), 0, d_light.data_ptr(), len(light),
+                      out.data_ptr())
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        gpu.sync()
+        if i >= args.warmup:
+            times.append(e0.elapsed_time(e1))
+    rays = gpu.counters()["rays"]
+    print(json.dumps({"kernel": f"{args.kernel_only}_warp", "workload": args.workload, "items": int(len(items)),
+                      "rays": int(rays), "ms": statistics.median(times), "grays": rays / statistics.median(times) / 1e6}))
+    buffers.close()
+    gpu.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -205,9 +239,15 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--kernel-only", choices=["direct", "gather"], default=None,
+                    help="run one warp-per-item pass over --items texels of the workload, warmup + steps times "
+                         "(for profiler captures; prints its own line)")
+    ap.add_argument("--items", type=int, default=262144)
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.kernel_only:
+        return kernel_only(args)
     world, rank, local = dist_env()
 
     import torch
@@ -232,7 +272,8 @@ def main():
         return t.item()
 
     # ---- the device-resident bake: graph replays, inputs resident ----
-    plan = lb.Plan(scene, gpu)
+    plan = lb.Plan(scene, gpu, autotune=True)
+    tuning = (lb._native.lib().lb_plan_tuning(plan._h) or b"").decode()
     plan.launch()
     gpu.sync()
     rays3 = plan.rays()
@@ -311,7 +352,7 @@ def main():
         with torch.cuda.stream(stream):
             e0.record(stream)
         t0 = time.perf_counter()
-        b = lb.bake_device(scene, gpu)
+        b = lb.bake_device(scene, gpu, autotune=True)
         with torch.cuda.stream(stream):
             e1.record(stream)
         gpu.sync()
@@ -370,6 +411,7 @@ def main():
                        "rays_per_step": int(rays_step), "rays_direct_gather_volume": [int(r) for r in rays3],
                        "l2": "flushed before every step (256 MB write)",
                        "path": "device-resident bake, one CUDA graph, warp-per-item BVH2 passes",
+                       "autotune": tuning,
                        "parallelism": f"independent maps x{world}"},
             "bake_seconds": e2e_t / 1e3,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,

@@ -125,9 +125,30 @@ int lb_run_async(lb_gpu *gpu, lb_scene *scene, int pass, const lb_params *params
 /* Which kernels lb_run and lb_run_async use: 0 (default) one thread an item, as the shader is
  * dispatched; 1 one warp an item (the device-resident bake's kernels). Results are identical. */
 int lb_set_pass_kernel(lb_gpu *gpu, int kind);
+/* The warp kernels' ray order within an item: a warp's 32 rays of a round share the top `group` bits of
+ * the ray index (and the bottom bits that remain): large values give the shader's order (bands of
+ * elevation), 0 wedges of azimuth. Results are identical; speed is not (lb_autotune picks). */
+int lb_set_ray_order(lb_gpu *gpu, int direct, int gather);
 /* Bytes this handle copied host to device and device to host since the last reset. */
 int lb_get_transfer(lb_gpu *gpu, uint64_t *h2d, uint64_t *d2h, int reset);
 
+
+/* ---- the texel filters on the device (crates/lightbaker/src/filter.rs) ----
+ * One tile of w x h texels, row by row; every array is in device memory; `channels` (1..4) floats a
+ * texel, interleaved; chart: a texel's chart (0xffffffff: none); normal: 3 floats a texel. Enqueued on
+ * the handle's stream (lb_gpu_sync waits). Results equal the reference's host functions. */
+/* smooth (filter.rs:20-53): Gaussian mean (sigma = 0.75 r) of the valid texels on the same surface
+ * (same chart, normals within n.n >= 0.9); radius 0..8. */
+int lb_smooth(lb_gpu *gpu, uint32_t w, uint32_t h, const uint32_t *chart, const float *normal,
+              const float *values, int channels, const uint8_t *valid, int radius, float *out);
+/* fill (filter.rs:58-94): `rings` rings of filling texels without light from their neighbours, in place
+ * (values and valid). Uses scratch the handle keeps (a ping-pong copy of the tile). */
+int lb_fill(lb_gpu *gpu, uint32_t w, uint32_t h, const uint32_t *chart, float *values, int channels,
+            uint8_t *valid, int rings);
+/* sun_field (filter.rs:106-141): the sun's distance field from each texel's grid_side^2 hard bits
+ * (grid side 1..5), 0.5 at a shadow's edge, 0 and 1 at `radius` texels; -1 where not covered. */
+int lb_sun_field(lb_gpu *gpu, uint32_t w, uint32_t h, const uint32_t *chart, const float *normal,
+                 const uint32_t *hard, const uint8_t *covered, uint32_t grid_side, float radius, float *out);
 
 /* ---- the host pipeline (crates/lightbaker/src/bake.rs, lib.rs) ---- */
 
@@ -168,6 +189,7 @@ typedef struct lb_bake_options {
     const char *cache_dir;                      /* NULL: no cache (bake.rs:30-34) */
     void (*log)(void *ctx, const char *line);   /* NULL: quiet */
     void *log_ctx;
+    int autotune;                               /* device bake: time the passes' shapes on a sample first */
 } lb_bake_options;
 
 typedef struct lb_bake lb_bake;
@@ -218,6 +240,8 @@ int lb_plan_rays(lb_plan *plan, uint64_t rays[3]);
 lb_bake *lb_plan_result(lb_plan *plan);
 /* Kernel launches in one launch of the plan's graph. */
 int lb_plan_kernels(const lb_plan *plan);
+/* What the autotuner chose for the plan ("" when it did not run). */
+const char *lb_plan_tuning(const lb_plan *plan);
 void lb_plan_free(lb_plan *plan);
 
 /* Scene::write (scene.rs:164-181) from a JSON header and positions: for tools and tests that make

@@ -139,6 +139,10 @@ class Gpu:
         """0: one thread an item (as the shader); 1: one warp an item. Same results."""
         N.check(N.lib().lb_set_pass_kernel(self._h, int(kind)), "lb_set_pass_kernel")
 
+    def set_ray_order(self, direct: int, gather: int) -> None:
+        """The warp kernels' ray order (see include/lightbaker.h lb_set_ray_order). Same results."""
+        N.check(N.lib().lb_set_ray_order(self._h, int(direct), int(gather)), "lb_set_ray_order")
+
     def set_counting(self, on: bool) -> None:
         N.check(N.lib().lb_set_counting(self._h, int(on)), "lb_set_counting")
 
@@ -287,9 +291,10 @@ class Bake:
             pass
 
 
-def _options(cache, log):
+def _options(cache, log, autotune=False):
     opts = N.BakeOptions()
     opts.cache_dir = str(cache).encode() if cache else None
+    opts.autotune = int(bool(autotune))
     keep = None
     if log is not None:
         keep = N.LOG_CB(lambda ctx, line: log(line.decode("utf-8", "replace")))
@@ -307,9 +312,10 @@ def bake(scene: bytes, gpu: Gpu, cache=None, log=None) -> Bake:
     return Bake(h)
 
 
-def bake_device(scene: bytes, gpu: Gpu, cache=None, log=None) -> Bake:
-    """The device-resident bake: every dirty tile rebaked in one CUDA graph (same results as bake())."""
-    opts, keep = _options(cache, log)
+def bake_device(scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False) -> Bake:
+    """The device-resident bake: every dirty tile rebaked in one CUDA graph (same results as bake()).
+    autotune: time the passes' ray order and grid on a sample of the texels first (lb_bake_options)."""
+    opts, keep = _options(cache, log, autotune)
     h = N.lib().lb_bake_device(gpu.handle, scene, len(scene), C.byref(opts))
     del keep
     if not h:
@@ -321,8 +327,8 @@ class Plan:
     """A device bake in steps: the host work and the graph once (`Plan(scene, gpu)`), then `launch()`
     (the graph enqueued on gpu.stream; repeatable), `rays()`, `result()`."""
 
-    def __init__(self, scene: bytes, gpu: Gpu, cache=None, log=None):
-        self._opts, self._keep = _options(cache, log)
+    def __init__(self, scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False):
+        self._opts, self._keep = _options(cache, log, autotune)
         self._h = N.lib().lb_plan_create(gpu.handle, scene, len(scene), C.byref(self._opts))
         if not self._h:
             raise LightbakerError(N.last_error())

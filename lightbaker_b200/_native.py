@@ -69,7 +69,7 @@ class Tracer(C.Structure):
 
 
 class BakeOptions(C.Structure):
-    _fields_ = [("cache_dir", C.c_char_p), ("log", LOG_CB), ("log_ctx", C.c_void_p)]
+    _fields_ = [("cache_dir", C.c_char_p), ("log", LOG_CB), ("log_ctx", C.c_void_p), ("autotune", C.c_int)]
 
 
 # every exported entry point: name -> (restype, argtypes)
@@ -84,12 +84,18 @@ SIGNATURES = {
                          C.c_size_t, C.c_void_p]),
     "lb_set_counting": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_set_pass_kernel": (C.c_int, [C.c_void_p, C.c_int]),
+    "lb_set_ray_order": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "lb_get_counters": (C.c_int, [C.c_void_p, C.POINTER(Counters)]),
     "lb_gpu_stream": (C.c_void_p, [C.c_void_p]),
     "lb_gpu_sync": (C.c_int, [C.c_void_p]),
     "lb_run_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(Params), C.c_void_p, C.c_size_t,
                                C.c_uint32, C.c_void_p, C.c_size_t, C.c_void_p]),
     "lb_get_transfer": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_int]),
+    "lb_smooth": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                            C.c_void_p, C.c_int, C.c_void_p]),
+    "lb_fill": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "lb_sun_field": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_uint32, C.c_float, C.c_void_p]),
     "lb_prepare": (C.c_void_p, [C.c_char_p, C.c_size_t]),
     "lb_prepared_free": (None, [C.c_void_p]),
     "lb_prepared_get_info": (C.c_int, [C.c_void_p, C.POINTER(PreparedInfo)]),
@@ -108,6 +114,7 @@ SIGNATURES = {
     "lb_plan_result": (C.c_void_p, [C.c_void_p]),
     "lb_plan_free": (None, [C.c_void_p]),
     "lb_plan_kernels": (C.c_int, [C.c_void_p]),
+    "lb_plan_tuning": (C.c_char_p, [C.c_void_p]),
     "lb_bake_get_info": (C.c_int, [C.c_void_p, C.POINTER(BakeInfo)]),
     "lb_bake_get_direct": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lb_bake_get_indirect": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -12,7 +12,9 @@
 // shader's arithmetic in its order, the texel passes the host's.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
+#include <string>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -99,6 +101,9 @@ struct lb_plan {
     uint32_t aw = 0, ah = 0, iw = 0, ih = 0, ds = 1;
     int blocks_direct = 0, blocks_gather = 0, blocks_volume = 0;
     int kernel_nodes = 0;
+    bool autotune = false;
+    int group_direct = 8, group_gather = 8;  // ray order for the warp passes
+    std::string tuned;  // what the autotuner picked
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     double t_prepare = 0;
@@ -328,6 +333,84 @@ void build(lb_plan &p) {
     p.t_prepare = since(t0);
 }
 
+// The autotuner: times the warp passes on a sample of this plan's covered texels (every k-th, up to
+// 16384) for each ray order and persistent grid size, and keeps the fastest for the graph. Results do
+// not depend on either choice.
+void autotune(lb_plan &p) {
+    if (p.n_cov == 0) return;
+    cudaStream_t st = p.g->stream;
+    lbd::Scene S{(const float4 *)p.dscene->nodes, (const float4 *)p.dscene->tris, (const float4 *)p.dscene->mats,
+                 (const float4 *)p.dscene->charts, p.dscene->n_nodes, p.dscene->n_tris, p.dscene->n_mats,
+                 p.dscene->n_charts};
+    uint32_t want = std::min<uint32_t>(p.n_cov, 16384), stride = std::max<uint32_t>(1, p.n_cov / want);
+    std::vector<uint32_t> sample;
+    {
+        std::vector<uint32_t> all(p.n_cov);
+        ck(cudaMemcpy(all.data(), p.cov_idx.p, size_t(p.n_cov) * 4, cudaMemcpyDeviceToHost), "autotune");
+        for (uint32_t k = 0; k < p.n_cov && sample.size() < want; k += stride) sample.push_back(all[k]);
+    }
+    DBuf sidx, sout;
+    sidx.alloc(sample.size() * 4);
+    sout.alloc(sample.size() * 16);
+    ck(cudaMemcpy(sidx.p, sample.data(), sample.size() * 4, cudaMemcpyHostToDevice), "autotune");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int orders[] = {8, 3, 2, 1, 0};
+    std::string report;
+    for (int pass : {LB_PASS_DIRECT, LB_PASS_GATHER}) {
+        int full = pass == LB_PASS_DIRECT ? p.blocks_direct : p.blocks_gather;
+        int per_sm = std::max(1, full / std::max(1, p.g->sms));
+        float best = 1e30f;
+        int best_order = 8, best_blocks = full;
+        for (int order : orders)
+            for (int bps = per_sm; bps >= 1; bps = bps > 1 ? std::max(1, bps / 2) : 0) {
+                WarpPass w{};
+                w.pass = pass;
+                w.S = &S;
+                w.P = &p.P.params;
+                w.tex = p.tex.as<float4>();
+                w.idx = sidx.as<uint32_t>();
+                w.n_host = uint32_t(sample.size());
+                w.light = p.light.as<float4>();
+                w.n_light = p.aw * p.ah;
+                w.out = sout.as<float4>();
+                w.counters = p.counters.as<unsigned long long>();
+                w.sms = p.g->sms;
+                w.blocks = bps * p.g->sms;
+                w.group = order;
+                float t = 0;
+                for (int rep = 0; rep < 2; rep++) {
+                    ck(cudaEventRecord(e0, st), "autotune");
+                    ck(lb_launch_pass_warp(w, st), "autotune");
+                    ck(cudaEventRecord(e1, st), "autotune");
+                    ck(cudaEventSynchronize(e1), "autotune");
+                    if (rep) cudaEventElapsedTime(&t, e0, e1);
+                }
+                if (t < best) {
+                    best = t;
+                    best_order = order;
+                    best_blocks = bps * p.g->sms;
+                }
+                if (bps == 1) break;
+            }
+        if (pass == LB_PASS_DIRECT) {
+            p.group_direct = best_order;
+            p.blocks_direct = best_blocks;
+        } else {
+            p.group_gather = best_order;
+            p.blocks_gather = best_blocks;
+        }
+        report += std::string(pass == LB_PASS_DIRECT ? "direct" : "gather") + ": order " + std::to_string(best_order) +
+                  ", " + std::to_string(best_blocks / std::max(1, p.g->sms)) + " blocks/SM (" + std::to_string(best) +
+                  " ms on " + std::to_string(sample.size()) + " texels); ";
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    p.tuned = report;
+    if (p.opt.log) p.opt.log("autotune: " + report);
+}
+
 // The graph: everything from the direct pass to the atlas.
 void capture(lb_plan &p) {
     const lb::SceneHeader &h = p.scene.header;
@@ -393,6 +476,7 @@ void capture(lb_plan &p) {
             w.out = p.direct_out.as<float4>();
             w.counters = cnt;
             w.blocks = p.blocks_direct;
+            w.group = p.group_direct;
             ck(lb_launch_pass_warp(w, st), "direct pass");
         }
         ck(lb_post_direct(a, int(h.lightmap.padding) + 4, s, st), "direct texel passes");
@@ -414,6 +498,7 @@ void capture(lb_plan &p) {
             gw.counters = cnt + 4;
             gw.sms = p.g->sms;
             gw.blocks = p.blocks_gather;
+            gw.group = p.group_gather;
             ck(lb_launch_pass_warp(gw, st), "gather pass");
             ck(lb_post_bounce(a, p.gather_out.as<float4>(), int(b.gi_filter * p.ds), p.wr.as<float>(),
                               int(h.lightmap.padding + 2 * p.ds + 2), s, st),
@@ -514,7 +599,11 @@ lb_plan *lb_plan_create(lb_gpu *g, const uint8_t *scene, size_t len, const lb_ba
             void *ctx = opts->log_ctx;
             p->opt.log = [fn, ctx](const std::string &s) { fn(ctx, s.c_str()); };
         }
+        p->autotune = opts && opts->autotune;
+        p->group_direct = g->group_direct;
+        p->group_gather = g->group_gather;
         build(*p);
+        if (p->autotune) autotune(*p);
         capture(*p);
         if (p->opt.log)
             p->opt.log(std::to_string(p->dirty.size()) + " of " + std::to_string(p->P.layout.tiles.size()) +
@@ -547,6 +636,8 @@ int lb_plan_rays(lb_plan *p, uint64_t rays[3]) {
 }
 
 int lb_plan_kernels(const lb_plan *p) { return p ? p->kernel_nodes : 0; }
+
+const char *lb_plan_tuning(const lb_plan *p) { return p ? p->tuned.c_str() : ""; }
 
 void lb_plan_free(lb_plan *p) {
     if (p) {

@@ -1,0 +1,221 @@
+// The reference's texel filters as device operations on one tile (crates/lightbaker/src/filter.rs:
+// smooth :20-53, fill :58-94, sun_field :106-141): arrays in device memory, w x h texels row by row,
+// `channels` floats a texel interleaved, enqueued on the handle's stream. Sums run in the reference's
+// order; the Gaussian weights are computed on the host as the reference computes them, so results
+// equal the host's (and the oracle's) bit for bit.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "lb_device.cuh"
+#include "lb_runtime.h"
+
+namespace lbd {
+
+constexpr int MAX_R = 8;  // smoothing radius a launch's weight table holds
+struct Weights {
+    float w[(2 * MAX_R + 1) * (2 * MAX_R + 1)];
+};
+
+__device__ __forceinline__ bool same_surface(const uint32_t *chart, const float *normal, uint32_t i, uint32_t j) {
+    if (chart[i] != chart[j]) return false;
+    const float *a = normal + 3 * size_t(i), *b = normal + 3 * size_t(j);
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] >= 0.9f;
+}
+
+template <int N>
+__global__ void k_tile_smooth(uint32_t w, uint32_t h, const uint32_t *chart, const float *normal, const float *v,
+                              const uint8_t *valid, int r, Weights W, float *out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w * h) return;
+    int x = int(i % w), y = int(i / w);
+    float sum[N], wsum = 0.0f;
+    for (int c = 0; c < N; c++) sum[c] = 0.0f;
+    if (!valid[i] || r == 0) {
+        for (int c = 0; c < N; c++) out[size_t(i) * N + c] = v[size_t(i) * N + c];
+        return;
+    }
+    for (int yy = y > r ? y - r : 0; yy < min(y + r + 1, int(h)); yy++)
+        for (int xx = x > r ? x - r : 0; xx < min(x + r + 1, int(w)); xx++) {
+            uint32_t j = uint32_t(yy) * w + uint32_t(xx);
+            if (!valid[j] || !same_surface(chart, normal, i, j)) continue;
+            float k = W.w[(yy - y + r) * (2 * r + 1) + (xx - x + r)];
+            for (int c = 0; c < N; c++) sum[c] += v[size_t(j) * N + c] * k;
+            wsum += k;
+        }
+    for (int c = 0; c < N; c++) out[size_t(i) * N + c] = sum[c] / wsum;
+}
+
+// one ring: reads (was, src), writes (now, dst)
+template <int N>
+__global__ void k_tile_fill(uint32_t w, uint32_t h, const uint32_t *chart, const uint8_t *was, const float *src,
+                            uint8_t *now, float *dst) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w * h) return;
+    float o[N];
+    for (int c = 0; c < N; c++) o[c] = src[size_t(i) * N + c];
+    uint8_t k = was[i];
+    if (!k) {
+        int x = int(i % w), y = int(i / w);
+        uint32_t ci = chart[i];
+        float own[N], any[N];
+        for (int c = 0; c < N; c++) own[c] = any[c] = 0.0f;
+        int no = 0, na = 0;
+        for (int yy = y > 0 ? y - 1 : 0; yy < min(y + 2, int(h)); yy++)
+            for (int xx = x > 0 ? x - 1 : 0; xx < min(x + 2, int(w)); xx++) {
+                uint32_t j = uint32_t(yy) * w + uint32_t(xx);
+                if (!was[j]) continue;
+                if (ci != NONE && chart[j] == ci) {
+                    for (int c = 0; c < N; c++) own[c] += src[size_t(j) * N + c];
+                    no++;
+                } else {
+                    for (int c = 0; c < N; c++) any[c] += src[size_t(j) * N + c];
+                    na++;
+                }
+            }
+        if (no > 0) {
+            for (int c = 0; c < N; c++) o[c] = own[c] / float(no);
+            k = 1;
+        } else if (na > 0 && ci == NONE) {
+            for (int c = 0; c < N; c++) o[c] = any[c] / float(na);
+            k = 1;
+        }
+    }
+    now[i] = k;
+    for (int c = 0; c < N; c++) dst[size_t(i) * N + c] = o[c];
+}
+
+__global__ void k_tile_sun_field(uint32_t w, uint32_t h, const uint32_t *chart, const float *normal,
+                                 const uint32_t *hard, const uint8_t *covered, int g, float radius, float *out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w * h) return;
+    float res = -1.0f;
+    if (covered[i]) {
+        int x = int(i % w), y = int(i / w);
+        int gg = g * g, reach = int(ceilf(radius)) + 1;
+        bool lit = __popc(hard[i]) * 2 >= gg;
+        float best = radius, fg = float(g), half = 0.5f / fg;
+        for (int yy = y > reach ? y - reach : 0; yy < min(y + reach + 1, int(h)); yy++)
+            for (int xx = x > reach ? x - reach : 0; xx < min(x + reach + 1, int(w)); xx++) {
+                uint32_t j = uint32_t(yy) * w + uint32_t(xx);
+                if (!covered[j] || !same_surface(chart, normal, i, j)) continue;
+                uint32_t other = lit ? ~hard[j] : hard[j];
+                if (gg < 32) other &= (1u << gg) - 1u;
+                while (other) {
+                    int c = __ffs(other) - 1;
+                    other &= other - 1;
+                    float px = float(xx) + (float(c % g) + 0.5f) / fg - (float(x) + 0.5f);
+                    float py = float(yy) + (float(c / g) + 0.5f) / fg - (float(y) + 0.5f);
+                    best = fminf(best, sqrtf(px * px + py * py) - half);
+                }
+            }
+        float d = fminf(fmaxf(best, 0.0f), radius);
+        res = 0.5f + 0.5f * (lit ? d : -d) / radius;
+    }
+    out[i] = res;
+}
+
+template <int N>
+cudaError_t fill_rings(uint32_t w, uint32_t h, const uint32_t *chart, float *v, uint8_t *valid, int rings, float *sv,
+                       uint8_t *sk, cudaStream_t st) {
+    uint32_t n = w * h;
+    dim3 grid((n + 255) / 256);
+    float *vw = v, *vn = sv;
+    uint8_t *kw = valid, *kn = sk;
+    for (int r = 0; r < rings; r++) {
+        k_tile_fill<N><<<grid, 256, 0, st>>>(w, h, chart, kw, vw, kn, vn);
+        float *t = vw;
+        vw = vn;
+        vn = t;
+        uint8_t *u = kw;
+        kw = kn;
+        kn = u;
+    }
+    if (vw != v) {
+        cudaError_t e = cudaMemcpyAsync(v, vw, size_t(n) * N * 4, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(valid, kw, n, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace lbd
+
+// Runs `rings` fill rings with the given scratch (n * channels floats, n bytes): shared by lb_fill and its
+// fixed-scratch variant.
+cudaError_t lb_fill_with_scratch(uint32_t w, uint32_t h, const uint32_t *chart, float *values, int channels,
+                                 uint8_t *valid, int rings, float *sv, uint8_t *sk, cudaStream_t st) {
+    switch (channels) {
+    case 1: return lbd::fill_rings<1>(w, h, chart, values, valid, rings, sv, sk, st);
+    case 2: return lbd::fill_rings<2>(w, h, chart, values, valid, rings, sv, sk, st);
+    case 3: return lbd::fill_rings<3>(w, h, chart, values, valid, rings, sv, sk, st);
+    case 4: return lbd::fill_rings<4>(w, h, chart, values, valid, rings, sv, sk, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+extern "C" {
+
+int lb_smooth(lb_gpu *g, uint32_t w, uint32_t h, const uint32_t *chart, const float *normal, const float *values,
+              int channels, const uint8_t *valid, int radius, float *out) {
+    if (!g || !chart || !normal || !values || !valid || !out || channels < 1 || channels > 4 || radius < 0 ||
+        radius > lbd::MAX_R || w == 0 || h == 0 || uint64_t(w) * h > 0xffffffffu) {
+        lb_set_error("lb_smooth: bad arguments (channels 1..4, radius 0..8)");
+        return LB_EINVAL;
+    }
+    lbd::Weights W;
+    std::memset(&W, 0, sizeof W);
+    if (radius > 0) {
+        float q = float(radius) * 0.75f;
+        float sigma2 = 2.0f * (q * q);
+        for (int dy = -radius; dy <= radius; dy++)
+            for (int dx = -radius; dx <= radius; dx++) {
+                float fx = float(dx), fy = float(dy);
+                W.w[(dy + radius) * (2 * radius + 1) + (dx + radius)] = std::exp(-(fx * fx + fy * fy) / sigma2);
+            }
+    }
+    uint32_t n = w * h;
+    dim3 grid((n + 255) / 256);
+    switch (channels) {
+    case 1: lbd::k_tile_smooth<1><<<grid, 256, 0, g->stream>>>(w, h, chart, normal, values, valid, radius, W, out); break;
+    case 2: lbd::k_tile_smooth<2><<<grid, 256, 0, g->stream>>>(w, h, chart, normal, values, valid, radius, W, out); break;
+    case 3: lbd::k_tile_smooth<3><<<grid, 256, 0, g->stream>>>(w, h, chart, normal, values, valid, radius, W, out); break;
+    default: lbd::k_tile_smooth<4><<<grid, 256, 0, g->stream>>>(w, h, chart, normal, values, valid, radius, W, out); break;
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LB_OK : lb_cuda_fail(e, "lb_smooth");
+}
+
+int lb_fill(lb_gpu *g, uint32_t w, uint32_t h, const uint32_t *chart, float *values, int channels, uint8_t *valid,
+            int rings) {
+    if (!g || !chart || !values || !valid || channels < 1 || channels > 4 || rings < 0 || w == 0 || h == 0 ||
+        uint64_t(w) * h > 0xffffffffu) {
+        lb_set_error("lb_fill: bad arguments (channels 1..4)");
+        return LB_EINVAL;
+    }
+    size_t n = size_t(w) * h;
+    // ping-pong scratch, kept by the handle
+    int rc = lb_buffer_reserve(g->scratch, n * channels * 4 + n + 256);
+    if (rc != LB_OK) return rc;
+    float *sv = (float *)g->scratch.ptr;
+    uint8_t *sk = (uint8_t *)g->scratch.ptr + ((n * channels * 4 + 255) & ~size_t(255));
+    cudaError_t e = lb_fill_with_scratch(w, h, chart, values, channels, valid, rings, sv, sk, g->stream);
+    return e == cudaSuccess ? LB_OK : lb_cuda_fail(e, "lb_fill");
+}
+
+int lb_sun_field(lb_gpu *g, uint32_t w, uint32_t h, const uint32_t *chart, const float *normal, const uint32_t *hard,
+                 const uint8_t *covered, uint32_t grid_side, float radius, float *out) {
+    if (!g || !chart || !normal || !hard || !covered || !out || grid_side < 1 || grid_side > 5 || !(radius > 0.0f) ||
+        w == 0 || h == 0 || uint64_t(w) * h > 0xffffffffu) {
+        lb_set_error("lb_sun_field: bad arguments (grid side 1..5, radius > 0)");
+        return LB_EINVAL;
+    }
+    uint32_t n = w * h;
+    lbd::k_tile_sun_field<<<(n + 255) / 256, 256, 0, g->stream>>>(w, h, chart, normal, hard, covered, int(grid_side),
+                                                                  radius, out);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LB_OK : lb_cuda_fail(e, "lb_sun_field");
+}
+
+}  // extern "C"

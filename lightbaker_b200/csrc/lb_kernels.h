@@ -36,6 +36,7 @@ struct WarpPass {
     bool full_count;
     int sms;
     int blocks;               // 0: as many as fit on the device at once
+    int group;                // ray order within an item (passes_warp.cu): top index bits a round shares
 };
 cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream);
 // The persistent grid's size for a pass: SMs x resident blocks of 256 threads.

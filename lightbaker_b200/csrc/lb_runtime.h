@@ -20,11 +20,12 @@ struct lb_gpu {
     cudaStream_t stream = nullptr;
     bool counting = false;
     int kernel = 0;  // lb_run's kernels: 0 a thread an item, 1 a warp an item
+    int group_direct = 8, group_gather = 8;  // the warp kernels' ray order (passes_warp.cu); 8: the shader's
     unsigned long long *counters = nullptr;       // device: rays, nodes, tris, mats
     unsigned long long *host_counters = nullptr;  // pinned copy, written by the stream
     lb_counters last = {};
     uint64_t h2d = 0, d2h = 0;  // bytes copied by this handle
-    lb_buffer items, out, light;
+    lb_buffer items, out, light, scratch;
 };
 
 // The scene's buffers (gpu/mod.rs:65-71).

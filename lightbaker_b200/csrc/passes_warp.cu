@@ -20,8 +20,11 @@ constexpr unsigned FULL = 0xffffffffu;
 
 // Adds the lanes' terms (those whose flag is set) to `sum` in lane order: the order a sequential loop
 // over the rays would add them.
+// (The loops stay rolled: fully unrolled twice in one kernel they make ptxas 12.9 fail register
+// allocation on sm_100a.)
 __device__ __forceinline__ float ordered_add(float sum, float term, bool on) {
     unsigned mask = __ballot_sync(FULL, on);
+#pragma unroll 1
     for (int l = 0; l < 32; l++) {
         float v = __shfl_sync(FULL, term, l);
         if (mask & (1u << l)) sum += v;
@@ -30,12 +33,43 @@ __device__ __forceinline__ float ordered_add(float sum, float term, bool on) {
 }
 __device__ __forceinline__ float3 ordered_add3(float3 sum, float3 term, bool on) {
     unsigned mask = __ballot_sync(FULL, on);
+#pragma unroll 1
     for (int l = 0; l < 32; l++) {
         float x = __shfl_sync(FULL, term.x, l), y = __shfl_sync(FULL, term.y, l), z = __shfl_sync(FULL, term.z, l);
         if (mask & (1u << l)) sum = add(sum, mk(x, y, z));
     }
     return sum;
 }
+
+// Ray order within an item. For a power-of-two ray count N = 2^L (32 <= N <= CAP), the warp's 32 rays
+// of a round are those whose index shares its top `a` bits and its bottom `b` bits (a + b = L - 5):
+// the Hammersley points (r / N, bitrev(r) / N) are a (0, m, 2)-net, so such a set fills one box of the
+// unit square: a = L - 5 a band of elevations (the shader's order), a = 0 a wedge of azimuths, between
+// them a patch of both. Rays of a patch head the same way and walk the same nodes. Each ray's term goes
+// to shared memory at its index and the item's sum is then built in index order, as the shader's.
+constexpr int WARPS = 8;     // warps a block (256 threads)
+constexpr int AO_CAP = 512;  // largest grouped occlusion ray count
+constexpr int GI_CAP = 256;  // largest grouped gather ray count
+
+// The round-invariant parts of the index: the lane's bits, and how a round's number splits.
+struct RayOrder {
+    uint32_t lane_bits, b, top, lo_mask;
+    bool grouped;
+    __device__ __forceinline__ RayOrder(uint32_t n, uint32_t cap, int a, int lane) {
+        int L = (n >= 32 && n <= cap && (n & (n - 1)) == 0) ? __ffs(n) - 1 : -1;
+        grouped = L >= 0;
+        if (!grouped) L = 5;
+        a = max(0, min(a, L - 5));
+        b = uint32_t(L - 5 - a);
+        top = uint32_t(L - a);
+        lo_mask = (1u << b) - 1u;
+        lane_bits = grouped ? uint32_t(lane) << b : uint32_t(lane);
+    }
+    __device__ __forceinline__ uint32_t ray(uint32_t round) const {
+        uint32_t r = grouped ? (((round >> b) << top) | lane_bits | (round & lo_mask)) : round * 32u + lane_bits;
+        return r;
+    }
+};
 
 // An item: its record (pos, normal, dx, dy), the position optionally taken from a second array
 // (the texel's sample point moved by the direct pass, bake.rs:227-238).
@@ -94,7 +128,9 @@ __device__ __forceinline__ void flush_counts(Count &c, unsigned long long *count
 template <bool COUNT>
 __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
-                                                   unsigned long long *counters) {
+                                                   unsigned long long *counters, int group) {
+    __shared__ float s_term[WARPS][AO_CAP];
+    __shared__ uint8_t s_hit[WARPS][AO_CAP];
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -168,8 +204,10 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
         float s1 = rnd(key, 3u, seed), s2 = rnd(key, 5u, seed);
         float occ = 0.0f;
         uint32_t nback = 0;
+        const RayOrder ord(rays, AO_CAP, group, lane);
+        const int w = threadIdx.x >> 5;
         for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
-            uint32_t r = r0 + uint32_t(lane);
+            uint32_t r = ord.ray(r0 >> 5);
             bool hit = false, bk = false;
             float term = 0.0f;
             if (r < rays) {
@@ -182,8 +220,18 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
                     bk = h.back && h.t < P.ground[3];
                 }
             }
-            occ = ordered_add(occ, term, hit);
+            if (ord.grouped) {
+                s_term[w][r] = term;
+                s_hit[w][r] = hit;
+            } else {
+                occ = ordered_add(occ, term, hit);
+            }
             nback += __popc(__ballot_sync(FULL, bk));
+        }
+        if (ord.grouped) {
+            __syncwarp();
+            for (uint32_t r0 = 0; r0 < rays; r0 += 32) occ = ordered_add(occ, s_term[w][r0 + lane], s_hit[w][r0 + lane]);
+            __syncwarp();
         }
         if (lane == 0)
             out[k] = make_float4(soft, __uint_as_float(hard | (pick << 24u)), occ / frays, __uint2float_rn(nback) / frays);
@@ -196,7 +244,9 @@ template <bool COUNT>
 __global__ void __launch_bounds__(256) gather_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const float4 *pos_override, const uint32_t *n_dev, uint32_t n_host,
                                                    uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
-                                                   unsigned long long *counters) {
+                                                   unsigned long long *counters, int group) {
+    __shared__ float3 s_term[WARPS][GI_CAP];
+    __shared__ uint8_t s_on[WARPS][GI_CAP];
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -214,8 +264,10 @@ __global__ void __launch_bounds__(256) gather_warp(Scene S, lb_params P, const f
         float s1 = rnd(key, 11u, seed), s2 = rnd(key, 13u, seed);
         float3 sum = mk(0.f, 0.f, 0.f);
         uint32_t nback = 0;
+        const RayOrder ord(rays, GI_CAP, group, lane);
+        const int w = threadIdx.x >> 5;
         for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
-            uint32_t r = r0 + uint32_t(lane);
+            uint32_t r = ord.ray(r0 >> 5);
             bool on = false, bk = false;
             float3 term = mk(0.f, 0.f, 0.f);
             if (r < rays) {
@@ -233,8 +285,18 @@ __global__ void __launch_bounds__(256) gather_warp(Scene S, lb_params P, const f
                     on = true;
                 }
             }
-            sum = ordered_add3(sum, term, on);
+            if (ord.grouped) {
+                s_term[w][r] = term;
+                s_on[w][r] = on;
+            } else {
+                sum = ordered_add3(sum, term, on);
+            }
             nback += __popc(__ballot_sync(FULL, bk));
+        }
+        if (ord.grouped) {
+            __syncwarp();
+            for (uint32_t r0 = 0; r0 < rays; r0 += 32) sum = ordered_add3(sum, s_term[w][r0 + lane], s_on[w][r0 + lane]);
+            __syncwarp();
         }
         if (lane == 0) {
             float3 e = scl(sum, PI);
@@ -360,18 +422,18 @@ cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream) {
     case LB_PASS_DIRECT:
         if (count)
             lbd::direct_warp<true><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base, w.out,
-                                                             w.counters);
+                                                             w.counters, w.group);
         else
             lbd::direct_warp<false><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base,
-                                                              w.out, w.counters);
+                                                              w.out, w.counters, w.group);
         break;
     case LB_PASS_GATHER:
         if (count)
             lbd::gather_warp<true><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host, w.base,
-                                                             w.light, w.n_light, w.out, w.counters);
+                                                             w.light, w.n_light, w.out, w.counters, w.group);
         else
             lbd::gather_warp<false><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host,
-                                                              w.base, w.light, w.n_light, w.out, w.counters);
+                                                              w.base, w.light, w.n_light, w.out, w.counters, w.group);
         break;
     default:
         if (count)

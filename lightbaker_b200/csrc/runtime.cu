@@ -109,6 +109,7 @@ void lb_gpu_close(lb_gpu *g) {
     lb_buffer_free(g->items);
     lb_buffer_free(g->out);
     lb_buffer_free(g->light);
+    lb_buffer_free(g->scratch);
     if (g->counters) cudaFree(g->counters);
     if (g->host_counters) cudaFreeHost(g->host_counters);
     cudaStreamDestroy(g->stream);
@@ -248,6 +249,13 @@ int lb_set_pass_kernel(lb_gpu *g, int kind) {
     return LB_OK;
 }
 
+int lb_set_ray_order(lb_gpu *g, int direct, int gather) {
+    if (!g || direct < 0 || gather < 0) return LB_EINVAL;
+    g->group_direct = direct;
+    g->group_gather = gather;
+    return LB_OK;
+}
+
 int lb_set_counting(lb_gpu *g, int on) {
     if (!g) return LB_EINVAL;
     g->counting = on != 0;
@@ -284,6 +292,7 @@ int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const fl
         w.counters = g->counters;
         w.full_count = g->counting;
         w.sms = g->sms;
+        w.group = pass == LB_PASS_GATHER ? g->group_gather : g->group_direct;
         LB_CUDA(lb_launch_pass_warp(w, g->stream), "pass launch");
     } else {
         LB_CUDA(lb_launch_pass_bvh2(pass, S, P, items, n, base, light, n_light, out, g->counters, g->counting,

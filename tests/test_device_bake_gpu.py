@@ -36,6 +36,14 @@ def test_device_bake_equals_drop_in(gpu, name):
     assert dev.stats.tiles_baked == plain.stats.tiles_baked
 
 
+def test_autotuned_device_bake_equals_drop_in(gpu):
+    s = scenes.small_map()
+    logs = []
+    dev = lb.bake_device(s, gpu, autotune=True, log=logs.append)
+    assert any(l.startswith("autotune:") for l in logs), logs
+    same(dev, lb.bake(s, gpu))
+
+
 def test_plan_replays_identically(gpu):
     s = scenes.small_map()
     p = lb.Plan(s, gpu)

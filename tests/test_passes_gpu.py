@@ -33,9 +33,10 @@ def _compare(gpu_out, cpu_out, what):
                           f"gpu {gpu_out[bad[:3]]} oracle {cpu_out[bad[:3]]}"
 
 
-@pytest.mark.parametrize("kernel", [0, 1], ids=["thread_per_item", "warp_per_item"])
+@pytest.mark.parametrize("kernel,order", [(0, 8), (1, 8), (1, 0), (1, 1)],
+                         ids=["thread_per_item", "warp_shader_order", "warp_azimuth_wedges", "warp_patches"])
 @pytest.mark.parametrize("name,limit", [("reference_test", 20000), ("small_map", 20000), ("map_100m", 3000)])
-def test_passes_bit_exact(gpu, oracle_mod, name, limit, kernel):
+def test_passes_bit_exact(gpu, oracle_mod, name, limit, kernel, order):
     scene = scenes.WORKLOADS[name]()
     P = lb.prepare(scene)
     buffers = gpu.scene(P.nodes, P.tris, P.materials, P.charts)
@@ -46,6 +47,7 @@ def test_passes_bit_exact(gpu, oracle_mod, name, limit, kernel):
     idx = np.sort(rng.choice(len(items), size=min(limit, len(items)), replace=False))
     items = items[idx]
     gpu.set_pass_kernel(kernel)
+    gpu.set_ray_order(order, order)
     gpu.set_counting(True)
     g = gpu.run(lb.Pass.DIRECT, buffers, P.params, items)
     gc = gpu.counters()
@@ -73,6 +75,7 @@ def test_passes_bit_exact(gpu, oracle_mod, name, limit, kernel):
     _compare(g, c, f"{name} volume")
     gpu.set_counting(False)
     gpu.set_pass_kernel(0)
+    gpu.set_ray_order(8, 8)
 
 
 def test_empty_and_edge_cases(gpu, oracle_mod):
