@@ -129,6 +129,9 @@ int lb_set_pass_kernel(lb_gpu *gpu, int kind);
  * the ray index (and the bottom bits that remain): large values give the shader's order (bands of
  * elevation), 0 wedges of azimuth. Results are identical; speed is not (lb_autotune picks). */
 int lb_set_ray_order(lb_gpu *gpu, int direct, int gather);
+/* The BVH the warp kernels walk: 2, the reference's (as uploaded); 8, the 8-wide BVH lb_scene_upload
+ * collapses from it (80-byte nodes, 8-bit child boxes). Same hits, faces and records. */
+int lb_set_bvh(lb_gpu *gpu, int width);
 /* Bytes this handle copied host to device and device to host since the last reset. */
 int lb_get_transfer(lb_gpu *gpu, uint64_t *h2d, uint64_t *d2h, int reset);
 
@@ -248,6 +251,10 @@ void lb_plan_free(lb_plan *plan);
  * scenes. header_json is the header as the file holds it. */
 int lb_scene_encode(const char *header_json, const float *const *positions, const size_t *n_floats,
                     size_t n_meshes, uint8_t **out, size_t *len);
+/* Collapses a BVH2 into the 8-wide BVH the device walks and checks it (every triangle in exactly one
+ * leaf, every box inside its parent's slot): LB_OK, its node count and depth; for tests and tools. */
+int lb_bvh8_check(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris, uint64_t *n_nodes8,
+                  uint64_t *depth);
 /* blake3 of a byte string (the hash the cache is keyed by), 32 bytes. */
 void lb_blake3(const uint8_t *data, size_t len, uint8_t out[32]);
 /* encode.rs: RGB9E5 and BC4 blocks, for format tests. */

@@ -85,6 +85,7 @@ SIGNATURES = {
     "lb_set_counting": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_set_pass_kernel": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_set_ray_order": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "lb_set_bvh": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_get_counters": (C.c_int, [C.c_void_p, C.POINTER(Counters)]),
     "lb_gpu_stream": (C.c_void_p, [C.c_void_p]),
     "lb_gpu_sync": (C.c_int, [C.c_void_p]),
@@ -126,6 +127,8 @@ SIGNATURES = {
     "lb_free": (None, [C.c_void_p]),
     "lb_scene_encode": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t), C.c_size_t,
                                   C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t)]),
+    "lb_bvh8_check": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64),
+                                C.POINTER(C.c_uint64)]),
     "lb_blake3": (None, [C.c_char_p, C.c_size_t, C.c_void_p]),
     "lb_rgb9e5": (C.c_uint32, [C.POINTER(C.c_float)]),
     "lb_rgb9e5_decode": (None, [C.c_uint32, C.POINTER(C.c_float)]),

@@ -103,6 +103,7 @@ struct lb_plan {
     int kernel_nodes = 0;
     bool autotune = false;
     int group_direct = 8, group_gather = 8;  // ray order for the warp passes
+    int bvh_direct = 2, bvh_gather = 2, bvh_volume = 2;  // BVH width for the warp passes
     std::string tuned;  // what the autotuner picked
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -339,9 +340,7 @@ void build(lb_plan &p) {
 void autotune(lb_plan &p) {
     if (p.n_cov == 0) return;
     cudaStream_t st = p.g->stream;
-    lbd::Scene S{(const float4 *)p.dscene->nodes, (const float4 *)p.dscene->tris, (const float4 *)p.dscene->mats,
-                 (const float4 *)p.dscene->charts, p.dscene->n_nodes, p.dscene->n_tris, p.dscene->n_mats,
-                 p.dscene->n_charts};
+    lbd::Scene S = lb_scene_view(p.dscene);
     uint32_t want = std::min<uint32_t>(p.n_cov, 16384), stride = std::max<uint32_t>(1, p.n_cov / want);
     std::vector<uint32_t> sample;
     {
@@ -416,9 +415,7 @@ void capture(lb_plan &p) {
     const lb::SceneHeader &h = p.scene.header;
     const lb::BakeSettings &b = h.bake;
     cudaStream_t st = p.g->stream;
-    lbd::Scene S{(const float4 *)p.dscene->nodes, (const float4 *)p.dscene->tris, (const float4 *)p.dscene->mats,
-                 (const float4 *)p.dscene->charts, p.dscene->n_nodes, p.dscene->n_tris, p.dscene->n_mats,
-                 p.dscene->n_charts};
+    lbd::Scene S = lb_scene_view(p.dscene);
     const lb_params &params = p.P.params;
     lb_params pvol = params;
     if (h.volume) pvol.counts[2] = h.volume->rays;
@@ -477,6 +474,7 @@ void capture(lb_plan &p) {
             w.counters = cnt;
             w.blocks = p.blocks_direct;
             w.group = p.group_direct;
+            w.bvh = p.bvh_direct;
             ck(lb_launch_pass_warp(w, st), "direct pass");
         }
         ck(lb_post_direct(a, int(h.lightmap.padding) + 4, s, st), "direct texel passes");
@@ -499,6 +497,7 @@ void capture(lb_plan &p) {
             gw.sms = p.g->sms;
             gw.blocks = p.blocks_gather;
             gw.group = p.group_gather;
+            gw.bvh = p.bvh_gather;
             ck(lb_launch_pass_warp(gw, st), "gather pass");
             ck(lb_post_bounce(a, p.gather_out.as<float4>(), int(b.gi_filter * p.ds), p.wr.as<float>(),
                               int(h.lightmap.padding + 2 * p.ds + 2), s, st),
@@ -522,6 +521,7 @@ void capture(lb_plan &p) {
                 vw.counters = cnt + 8;
                 vw.sms = p.g->sms;
                 vw.blocks = p.blocks_volume;
+                vw.bvh = p.bvh_volume;
                 ck(lb_launch_pass_warp(vw, st), "volume pass");
             }
             ck(lb_volume_fill(p.probes.as<float4>(), p.probes_b.as<float4>(), p.pk_a.as<uint8_t>(), p.pk_b.as<uint8_t>(),
@@ -602,6 +602,7 @@ lb_plan *lb_plan_create(lb_gpu *g, const uint8_t *scene, size_t len, const lb_ba
         p->autotune = opts && opts->autotune;
         p->group_direct = g->group_direct;
         p->group_gather = g->group_gather;
+        p->bvh_direct = p->bvh_gather = p->bvh_volume = g->bvh;
         build(*p);
         if (p->autotune) autotune(*p);
         capture(*p);

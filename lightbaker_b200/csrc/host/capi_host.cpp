@@ -8,6 +8,7 @@
 #include "../lb_runtime.h"
 #include "bake.h"
 #include "blake3.h"
+#include "bvh8.h"
 #include "encode.h"
 #include "handles.h"
 #include "raster.h"
@@ -348,6 +349,24 @@ int lb_scene_encode(const char *header_json, const float *const *positions, cons
             return LB_OK;
         },
         LB_EIO);
+}
+
+int lb_bvh8_check(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris, uint64_t *n_nodes8,
+                  uint64_t *depth) {
+    if (!nodes || !n_nodes || (n_tris && !tris)) return LB_EINVAL;
+    return guard(
+        [&]() -> int {
+            lb::Bvh8 b = lb::Bvh8::collapse(nodes, n_nodes, tris, n_tris);
+            size_t d = 0;
+            // the reference's empty scene has one dummy triangle no leaf holds
+            bool empty = nodes[0].count == 0 && n_nodes == 1;
+            std::string err = lb::bvh8_check(b, empty ? 0 : n_tris, d);
+            if (n_nodes8) *n_nodes8 = b.n_nodes();
+            if (depth) *depth = d;
+            if (!err.empty()) throw std::runtime_error("bvh8: " + err);
+            return LB_OK;
+        },
+        LB_EINVAL);
 }
 
 void lb_blake3(const uint8_t *data, size_t len, uint8_t out[32]) { lb::blake3_hash(data, len, out); }

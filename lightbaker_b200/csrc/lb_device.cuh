@@ -23,7 +23,12 @@ struct Scene {
     const float4 *mats;
     const float4 *charts;
     uint32_t n_nodes, n_tris, n_mats, n_charts;
+    // the 8-wide BVH (host/bvh8.h): 5 uint4 a node, its triangle copy (e2.w: the reference index)
+    const uint4 *nodes8 = nullptr;
+    const float4 *tris8 = nullptr;
 };
+
+constexpr int STACK8 = 96;  // node groups the 8-wide walk can hold (depth x 7 at most)
 
 // Work counters a thread keeps when counting is on (lb_counters).
 struct Count {
@@ -207,6 +212,138 @@ __device__ __forceinline__ Hit trace(const Scene &S, float3 o, float3 d, float t
         nhi = __ldg(&S.nodes[2 * n + 1]);
     }
     return hit;
+}
+
+// The same query over the 8-wide BVH: the nearest accepted hit within tmax (any: the first accepted),
+// the same triangle test in the same arithmetic, so every hit, its t and its face are the BVH2 walk's.
+// A node's eight child boxes are tested at once; its leaf slots' triangles first, then its hit inner
+// children nearest first (the rest pushed far to near with their entry distance, and skipped when
+// popped beyond the nearest hit so far).
+template <bool COUNT>
+__device__ __forceinline__ Hit trace8(const Scene &S, float3 o, float3 d, float tmax, bool any, uint32_t ray,
+                                      uint32_t seed, Count &c) {
+    Hit hit{tmax, NONE, false};
+    c.rays++;
+    float3 dd = mk(fabsf(d.x) < 1e-12f ? 1e-12f : d.x, fabsf(d.y) < 1e-12f ? 1e-12f : d.y,
+                   fabsf(d.z) < 1e-12f ? 1e-12f : d.z);
+    float3 inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+    uint32_t st_node[STACK8];
+    float st_t[STACK8];
+    int sp = 0;
+    uint32_t n = 0;
+    for (;;) {
+        const uint4 *nd = S.nodes8 + 5 * size_t(n);
+        uint4 a0 = __ldg(nd), a1 = __ldg(nd + 1), a2 = __ldg(nd + 2), a3 = __ldg(nd + 3), a4 = __ldg(nd + 4);
+        if (COUNT) c.nodes++;
+        float px = __uint_as_float(a0.x), py = __uint_as_float(a0.y), pz = __uint_as_float(a0.z);
+        float sx = __uint_as_float((a0.w & 0xffu) << 23), sy = __uint_as_float(((a0.w >> 8) & 0xffu) << 23),
+              sz = __uint_as_float(((a0.w >> 16) & 0xffu) << 23);
+        uint32_t imask = a0.w >> 24;
+        float tc[8];
+        uint32_t leafmask = 0, innermask = 0;
+#pragma unroll
+        for (int s = 0; s < 8; s++) {
+            uint32_t sh = uint32_t(s & 3) * 8u;
+            uint32_t meta = ((s < 4 ? a1.z : a1.w) >> sh) & 0xffu;
+            bool inner = (imask >> s) & 1u;
+            if (!inner && meta == 0xffu) {
+                tc[s] = FAR;
+                continue;
+            }
+            float4 mn = make_float4(px + __uint2float_rn(((s < 4 ? a2.x : a2.y) >> sh) & 0xffu) * sx,
+                                    py + __uint2float_rn(((s < 4 ? a2.z : a2.w) >> sh) & 0xffu) * sy,
+                                    pz + __uint2float_rn(((s < 4 ? a3.x : a3.y) >> sh) & 0xffu) * sz, 0.0f);
+            float4 mx = make_float4(px + __uint2float_rn(((s < 4 ? a3.z : a3.w) >> sh) & 0xffu) * sx,
+                                    py + __uint2float_rn(((s < 4 ? a4.x : a4.y) >> sh) & 0xffu) * sy,
+                                    pz + __uint2float_rn(((s < 4 ? a4.z : a4.w) >> sh) & 0xffu) * sz, 0.0f);
+            float t = box(o, inv, mn, mx, hit.t);
+            tc[s] = t;
+            if (t < FAR) {
+                if (inner) innermask |= 1u << s;
+                else leafmask |= 1u << s;
+            }
+        }
+        while (leafmask) {
+            int s = __ffs(leafmask) - 1;
+            leafmask &= leafmask - 1;
+            uint32_t meta = ((s < 4 ? a1.z : a1.w) >> (uint32_t(s & 3) * 8u)) & 0xffu;
+            uint32_t first = a1.y + (meta & 31u), cnt = ((meta >> 5) & 3u) + 1u;
+            for (uint32_t k = 0; k < cnt; k++) {
+                if (COUNT) c.tris++;
+                const float4 *tp = S.tris8 + 3 * size_t(first + k);
+                float4 v0 = __ldg(tp), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+                float3 p = cross3(d, xyz(e2));
+                float det = dot3(xyz(e1), p);
+                if (fabsf(det) < 1e-12f) continue;
+                float id = 1.0f / det;
+                float3 s3 = sub(o, xyz(v0));
+                float u = dot3(s3, p) * id;
+                if (u < 0.0f || u > 1.0f) continue;
+                float3 q = cross3(s3, xyz(e1));
+                float v = dot3(d, q) * id;
+                if (v < 0.0f || u + v > 1.0f) continue;
+                float t = dot3(xyz(e2), q) * id;
+                uint32_t orig = __float_as_uint(e2.w);
+                if (t > 1e-4f && t < hit.t && stops<COUNT>(S, orig, v0.w, ray, seed, c)) {
+                    hit = Hit{t, orig, det < 0.0f};
+                    if (any) return hit;
+                }
+            }
+        }
+        // inner children still nearer than the nearest hit: the nearest next, the rest on the stack
+        uint32_t next = NONE;
+        float tnext = FAR;
+        uint32_t live = 0;
+        for (uint32_t m = innermask; m; m &= m - 1) {
+            int s = __ffs(m) - 1;
+            if (tc[s] < hit.t) live |= 1u << s;
+        }
+        if (live) {
+            // push far to near, keep the nearest
+            while (live) {
+                int far_s = -1;
+                float tf = -1.0f;
+                for (uint32_t m = live; m; m &= m - 1) {
+                    int s = __ffs(m) - 1;
+                    if (tc[s] >= tf) {
+                        tf = tc[s];
+                        far_s = s;
+                    }
+                }
+                live &= ~(1u << far_s);
+                uint32_t child = a1.x + __popc(imask & ((1u << far_s) - 1u));
+                if (live == 0) {
+                    next = child;
+                    tnext = tf;
+                } else if (sp < STACK8) {
+                    st_node[sp] = child;
+                    st_t[sp] = tf;
+                    sp++;
+                }
+            }
+        }
+        if (next == NONE) {
+            while (sp > 0) {
+                sp--;
+                if (st_t[sp] < hit.t) {
+                    next = st_node[sp];
+                    break;
+                }
+            }
+            if (next == NONE) break;
+        }
+        (void)tnext;
+        n = next;
+    }
+    return hit;
+}
+
+// The walk a pass uses: BVH 2 the reference's tree, 8 the 8-wide one.
+template <int BVH, bool COUNT>
+__device__ __forceinline__ Hit walk(const Scene &S, float3 o, float3 d, float tmax, bool any, uint32_t ray,
+                                    uint32_t seed, Count &c) {
+    if (BVH == 8) return trace8<COUNT>(S, o, d, tmax, any, ray, seed, c);
+    return trace<COUNT>(S, o, d, tmax, any, ray, seed, c);
 }
 
 // trace.wgsl:133-148

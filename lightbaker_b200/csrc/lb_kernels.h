@@ -37,6 +37,7 @@ struct WarpPass {
     int sms;
     int blocks;               // 0: as many as fit on the device at once
     int group;                // ray order within an item (passes_warp.cu): top index bits a round shares
+    int bvh;                  // 2: the reference's BVH2; 8: the 8-wide BVH (S->nodes8)
 };
 cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream);
 // The persistent grid's size for a pass: SMs x resident blocks of 256 threads.

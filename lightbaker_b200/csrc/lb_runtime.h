@@ -20,7 +20,8 @@ struct lb_gpu {
     cudaStream_t stream = nullptr;
     bool counting = false;
     int kernel = 0;  // lb_run's kernels: 0 a thread an item, 1 a warp an item
-    int group_direct = 8, group_gather = 8;  // the warp kernels' ray order (passes_warp.cu); 8: the shader's
+    int group_direct = 8, group_gather = 8;
+    int bvh = 2;  // the warp kernels' BVH: 2 the reference's, 8 the 8-wide one  // the warp kernels' ray order (passes_warp.cu); 8: the shader's
     unsigned long long *counters = nullptr;       // device: rays, nodes, tris, mats
     unsigned long long *host_counters = nullptr;  // pinned copy, written by the stream
     lb_counters last = {};
@@ -33,9 +34,16 @@ struct lb_scene {
     lb_gpu *gpu = nullptr;
     void *nodes = nullptr, *tris = nullptr, *mats = nullptr, *charts = nullptr;
     uint32_t n_nodes = 0, n_tris = 0, n_mats = 0, n_charts = 0;
+    void *nodes8 = nullptr, *tris8 = nullptr;  // the 8-wide BVH collapsed from the BVH2 (host/bvh8.h)
+    uint32_t n_nodes8 = 0, n_tris8 = 0;
 };
 
 void lb_set_error(const std::string &msg);
+// the device view of an uploaded scene (both BVHs)
+namespace lbd {
+struct Scene;
+}
+lbd::Scene lb_scene_view(const lb_scene *s);
 int lb_cuda_fail(cudaError_t e, const char *what);
 int lb_buffer_reserve(lb_buffer &b, size_t bytes);
 void lb_buffer_free(lb_buffer &b);

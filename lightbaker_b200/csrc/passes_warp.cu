@@ -89,7 +89,7 @@ __device__ __forceinline__ Item load_item(const float4 *tex, const uint32_t *idx
 
 // trace.wgsl:159-168 with lanes 0..15 each tracing one of the 16 rays; true on every lane when more than
 // insideShare of them meet back faces. The count of back faces is exact, as the shader's float sum of ones.
-template <bool COUNT>
+template <int BVH, bool COUNT>
 __device__ __forceinline__ bool inside_warp(const Scene &S, const lb_params &P, uint32_t seed, float3 o, float3 n,
                                             uint32_t key, int lane, Count &c) {
     bool back = false;
@@ -97,7 +97,7 @@ __device__ __forceinline__ bool inside_warp(const Scene &S, const lb_params &P, 
         Frame f = frame(n);
         uint32_t r = uint32_t(lane);
         float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
-        Hit h = trace<COUNT>(S, o, d, P.ground[3], false, key + r + 7000u, seed, c);
+        Hit h = walk<BVH, COUNT>(S, o, d, P.ground[3], false, key + r + 7000u, seed, c);
         back = h.tri != NONE && h.back;
     }
     float nb = __uint2float_rn(__popc(__ballot_sync(FULL, back)));
@@ -125,7 +125,7 @@ __device__ __forceinline__ void flush_counts(Count &c, unsigned long long *count
 }
 
 // trace.wgsl:170-243
-template <bool COUNT>
+template <int BVH, bool COUNT>
 __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
                                                    unsigned long long *counters, int group) {
@@ -148,11 +148,11 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
         float3 at = pos;
         uint32_t pick = 0u;
         float span = 1.0f;
-        if (inside_warp<COUNT>(S, P, seed, add(at, lift), nrm, key, lane, c)) {
+        if (inside_warp<BVH, COUNT>(S, P, seed, add(at, lift), nrm, key, lane, c)) {
             for (uint32_t q = 1u; q < 9u; q++) {
                 float2 cc = offset(q);
                 float3 p = add(add(pos, scl(dx, cc.x)), scl(dy, cc.y));
-                if (!inside_warp<COUNT>(S, P, seed, add(p, lift), nrm, key + q * 31u, lane, c)) {
+                if (!inside_warp<BVH, COUNT>(S, P, seed, add(p, lift), nrm, key + q * 31u, lane, c)) {
                     at = p;
                     pick = q;
                     span = 0.4f;
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
             }
             if (pick == 0u) {
                 float3 p = add(pos, scl(nrm, PUSH));
-                if (!inside_warp<COUNT>(S, P, seed, add(p, lift), nrm, key + 331u, lane, c)) {
+                if (!inside_warp<BVH, COUNT>(S, P, seed, add(p, lift), nrm, key + 331u, lane, c)) {
                     at = p;
                     pick = 9u;
                     span = 0.4f;
@@ -185,10 +185,10 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
                     float cy = ((__uint2float_rn(s / g) + 0.5f) / fg - 0.5f) * span;
                     float3 o = add(add(add(at, scl(dx, cx)), scl(dy, cy)), lift);
                     if (lane < 16) {
-                        escaped = trace<COUNT>(S, o, sun, FAR, true, key + s, seed, c).tri == NONE;
+                        escaped = walk<BVH, COUNT>(S, o, sun, FAR, true, key + s, seed, c).tri == NONE;
                     } else {
                         float3 d = sun_disc(P, sf, (s + turn) % gg, gg);
-                        escaped = trace<COUNT>(S, o, d, FAR, true, key + s + 1000u, seed, c).tri == NONE;
+                        escaped = walk<BVH, COUNT>(S, o, d, FAR, true, key + s + 1000u, seed, c).tri == NONE;
                     }
                 }
                 unsigned m = __ballot_sync(FULL, escaped);
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
             float term = 0.0f;
             if (r < rays) {
                 float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
-                Hit h = trace<COUNT>(S, o, d, P.reach[0], false, key + r + 2000u, seed, c);
+                Hit h = walk<BVH, COUNT>(S, o, d, P.reach[0], false, key + r + 2000u, seed, c);
                 if (h.tri != NONE) {
                     hit = true;
                     float kk = h.t / P.reach[0];
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
 }
 
 // trace.wgsl:245-270
-template <bool COUNT>
+template <int BVH, bool COUNT>
 __global__ void __launch_bounds__(256) gather_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const float4 *pos_override, const uint32_t *n_dev, uint32_t n_host,
                                                    uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(256) gather_warp(Scene S, lb_params P, const f
                 float jx = rnd(key + r, 19u, seed) - 0.5f, jy = rnd(key + r, 23u, seed) - 0.5f;
                 float3 o = add(add(add(pos, scl(dx, jx)), scl(dy, jy)), scl(nrm, P.reach[2]));
                 float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
-                Hit h = trace<COUNT>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c);
+                Hit h = walk<BVH, COUNT>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c);
                 if (h.tri == NONE) {
                     term = sky(P, d);
                     on = true;
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(256) gather_warp(Scene S, lb_params P, const f
 }
 
 // trace.wgsl:272-324. `slot` (optional) scatters probe k's four records to 4 * slot[k].
-template <bool COUNT>
+template <int BVH, bool COUNT>
 __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const float4 *tex, uint32_t n, const float4 *light,
                                                    uint32_t n_light, float4 *out, const uint32_t *slot,
                                                    unsigned long long *counters) {
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const f
                 float sa, ca;
                 sincos32(a, &sa, &ca);
                 float3 d = mk(rr * ca, z, rr * sa);
-                Hit h = trace<COUNT>(S, o, d, P.reach[1], false, key + r, seed, c);
+                Hit h = walk<BVH, COUNT>(S, o, d, P.reach[1], false, key + r, seed, c);
                 float3 l = sky(P, d);
                 if (h.tri != NONE) {
                     bk = h.back;
@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const f
             bool esc = false;
             if (s < gg) {
                 float3 d = sun_disc(P, sf, s, gg);
-                esc = trace<COUNT>(S, o, d, FAR, true, key + s + 9000u, seed, c).tri == NONE;
+                esc = walk<BVH, COUNT>(S, o, d, FAR, true, key + s + 9000u, seed, c).tri == NONE;
             }
             nsun += __popc(__ballot_sync(FULL, esc));
         }
@@ -385,32 +385,45 @@ __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const f
 
 }  // namespace lbd
 
-int lb_warp_pass_blocks(const WarpPass &w) {
+template <int BVH, bool COUNT> int blocks_for(int pass) {
     const int T = 256;
     int per_sm = 0;
     cudaError_t e;
-    bool count = w.full_count;
+    switch (pass) {
+    case LB_PASS_DIRECT: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::direct_warp<BVH, COUNT>, T, 0); break;
+    case LB_PASS_GATHER: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::gather_warp<BVH, COUNT>, T, 0); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::volume_warp<BVH, COUNT>, T, 0); break;
+    }
+    return (e != cudaSuccess || per_sm < 1) ? 1 : per_sm;
+}
+
+template <int BVH, bool COUNT> void launch(const WarpPass &w, int blocks, cudaStream_t stream) {
+    const int T = 256;
     switch (w.pass) {
     case LB_PASS_DIRECT:
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, count ? lbd::direct_warp<true> : lbd::direct_warp<false>, T, 0);
+        lbd::direct_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base,
+                                                               w.out, w.counters, w.group);
         break;
     case LB_PASS_GATHER:
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, count ? lbd::gather_warp<true> : lbd::gather_warp<false>, T, 0);
+        lbd::gather_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host,
+                                                               w.base, w.light, w.n_light, w.out, w.counters, w.group);
         break;
     default:
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, count ? lbd::volume_warp<true> : lbd::volume_warp<false>, T, 0);
+        lbd::volume_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light, w.out,
+                                                               w.slot, w.counters);
         break;
     }
-    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+}
+
+int lb_warp_pass_blocks(const WarpPass &w) {
+    int per_sm = w.bvh == 8 ? (w.full_count ? blocks_for<8, true>(w.pass) : blocks_for<8, false>(w.pass))
+                            : (w.full_count ? blocks_for<2, true>(w.pass) : blocks_for<2, false>(w.pass));
     return w.sms * per_sm;
 }
 
 cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream) {
     const int T = 256;
-    bool count = w.full_count;
+    if (w.bvh == 8 && (w.S->nodes8 == nullptr || w.S->tris8 == nullptr)) return cudaErrorInvalidValue;
     int blocks = w.blocks > 0 ? w.blocks : lb_warp_pass_blocks(w);
     if (w.n_dev == nullptr) {
         // no more warps than items
@@ -418,31 +431,12 @@ cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream) {
         if (need == 0) return cudaSuccess;
         if ((uint32_t)blocks > need) blocks = (int)need;
     }
-    switch (w.pass) {
-    case LB_PASS_DIRECT:
-        if (count)
-            lbd::direct_warp<true><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base, w.out,
-                                                             w.counters, w.group);
-        else
-            lbd::direct_warp<false><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base,
-                                                              w.out, w.counters, w.group);
-        break;
-    case LB_PASS_GATHER:
-        if (count)
-            lbd::gather_warp<true><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host, w.base,
-                                                             w.light, w.n_light, w.out, w.counters, w.group);
-        else
-            lbd::gather_warp<false><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host,
-                                                              w.base, w.light, w.n_light, w.out, w.counters, w.group);
-        break;
-    default:
-        if (count)
-            lbd::volume_warp<true><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light, w.out,
-                                                             w.slot, w.counters);
-        else
-            lbd::volume_warp<false><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light, w.out,
-                                                              w.slot, w.counters);
-        break;
+    if (w.bvh == 8) {
+        if (w.full_count) launch<8, true>(w, blocks, stream);
+        else launch<8, false>(w, blocks, stream);
+    } else {
+        if (w.full_count) launch<2, true>(w, blocks, stream);
+        else launch<2, false>(w, blocks, stream);
     }
     return cudaGetLastError();
 }

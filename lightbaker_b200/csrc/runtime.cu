@@ -12,6 +12,7 @@
 #include <cstring>
 #include <string>
 
+#include "host/bvh8.h"
 #include "lb_device.cuh"
 #include "lb_kernels.h"
 #include "lb_runtime.h"
@@ -157,13 +158,46 @@ lb_scene *lb_scene_upload(lb_gpu *g, const lb_node *nodes, size_t n_nodes, const
     s->n_tris = uint32_t(n_tris);
     s->n_mats = uint32_t(n_materials);
     s->n_charts = uint32_t(n_charts);
+    // the 8-wide BVH over the same triangles
+    try {
+        lb::Bvh8 b8 = lb::Bvh8::collapse(nodes, n_nodes, n_tris ? tris : &zero_tri, n_tris ? n_tris : 1);
+        size_t nb = b8.nodes.size() * 4, tb = b8.tris.size() * sizeof(lb_tri);
+        cudaError_t e = cudaMalloc(&s->nodes8, nb);
+        if (e == cudaSuccess) e = cudaMemcpy(s->nodes8, b8.nodes.data(), nb, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMalloc(&s->tris8, tb);
+        if (e == cudaSuccess) e = cudaMemcpy(s->tris8, b8.tris.data(), tb, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            lb_cuda_fail(e, "lb_scene_upload (8-wide BVH)");
+            lb_scene_free(s);
+            return nullptr;
+        }
+        g->h2d += nb + tb;
+        s->n_nodes8 = uint32_t(b8.n_nodes());
+        s->n_tris8 = uint32_t(b8.tris.size());
+    } catch (const std::exception &ex) {
+        lb_set_error(std::string("lb_scene_upload: ") + ex.what());
+        lb_scene_free(s);
+        return nullptr;
+    }
     return s;
 }
+
+}  // extern "C"
+
+lbd::Scene lb_scene_view(const lb_scene *s) {
+    lbd::Scene S{(const float4 *)s->nodes, (const float4 *)s->tris, (const float4 *)s->mats, (const float4 *)s->charts,
+                 s->n_nodes, s->n_tris, s->n_mats, s->n_charts};
+    S.nodes8 = (const uint4 *)s->nodes8;
+    S.tris8 = (const float4 *)s->tris8;
+    return S;
+}
+
+extern "C" {
 
 void lb_scene_free(lb_scene *s) {
     if (!s) return;
     cudaSetDevice(s->gpu->device);
-    for (void *p : {s->nodes, s->tris, s->mats, s->charts})
+    for (void *p : {s->nodes, s->tris, s->mats, s->charts, s->nodes8, s->tris8})
         if (p) cudaFree(p);
     delete s;
 }
@@ -249,6 +283,12 @@ int lb_set_pass_kernel(lb_gpu *g, int kind) {
     return LB_OK;
 }
 
+int lb_set_bvh(lb_gpu *g, int width) {
+    if (!g || (width != 2 && width != 8)) return LB_EINVAL;
+    g->bvh = width;
+    return LB_OK;
+}
+
 int lb_set_ray_order(lb_gpu *g, int direct, int gather) {
     if (!g || direct < 0 || gather < 0) return LB_EINVAL;
     g->group_direct = direct;
@@ -275,8 +315,7 @@ int lb_get_counters(lb_gpu *g, lb_counters *out) {
 // lb_collect_counters after a sync to move them into g->last.
 int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const float4 *items, uint32_t n, uint32_t base,
                   const float4 *light, uint32_t n_light, float4 *out) {
-    lbd::Scene S{(const float4 *)s->nodes, (const float4 *)s->tris, (const float4 *)s->mats, (const float4 *)s->charts,
-                 s->n_nodes, s->n_tris, s->n_mats, s->n_charts};
+    lbd::Scene S = lb_scene_view(s);
     LB_CUDA(cudaMemsetAsync(g->counters, 0, 4 * sizeof(unsigned long long), g->stream), "counters");
     if (g->kernel == 1) {
         WarpPass w{};
@@ -293,6 +332,7 @@ int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const fl
         w.full_count = g->counting;
         w.sms = g->sms;
         w.group = pass == LB_PASS_GATHER ? g->group_gather : g->group_direct;
+        w.bvh = g->bvh;
         LB_CUDA(lb_launch_pass_warp(w, g->stream), "pass launch");
     } else {
         LB_CUDA(lb_launch_pass_bvh2(pass, S, P, items, n, base, light, n_light, out, g->counters, g->counting,
