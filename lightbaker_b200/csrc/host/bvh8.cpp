@@ -224,54 +224,49 @@ Bvh8 Bvh8::collapse(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, si
 
 namespace lb {
 
-// Structural checks of a collapse (for tests): every triangle once; children in range; each leaf
-// triangle's corners inside its slot's dequantised box; each inner child's slots inside its slot's box.
+// Structural checks of a collapse (for tests): every triangle reached once; children in range; each
+// triangle's corners inside every box on its path from the root (what a correct walk needs; a child's
+// box may reach past its parent's by a quantum, which does not matter).
 std::string bvh8_check(const Bvh8 &b, size_t n_tris, size_t &depth) {
-    auto node = [&](size_t n) { return &b.nodes[n * 20]; };
+    struct Frame {
+        size_t node, depth;
+        float mn[3], mx[3];
+    };
     auto slot_box = [&](const uint32_t *w, int s, float mn[3], float mx[3]) {
         float p[3];
         std::memcpy(p, w, 12);
         const uint8_t *q = (const uint8_t *)&w[8];
         for (int a = 0; a < 3; a++) {
             float scale;
-            uint32_t e = (w[3] >> (8 * a)) & 0xffu;
-            uint32_t bits = e << 23;
+            uint32_t bits = ((w[3] >> (8 * a)) & 0xffu) << 23;
             std::memcpy(&scale, &bits, 4);
             mn[a] = p[a] + float(q[a * 8 + s]) * scale;
             mx[a] = p[a] + float(q[(3 + a) * 8 + s]) * scale;
         }
     };
     std::vector<int> seen(n_tris, 0);
-    std::vector<std::pair<size_t, size_t>> st{{0, 1}};
+    std::vector<Frame> st{{0, 1, {-FLT_MAX, -FLT_MAX, -FLT_MAX}, {FLT_MAX, FLT_MAX, FLT_MAX}}};
     depth = 0;
     size_t visited = 0;
     while (!st.empty()) {
-        auto [n, d] = st.back();
+        Frame f = st.back();
         st.pop_back();
-        depth = std::max(depth, d);
-        if (n >= b.n_nodes()) return "child index out of range";
+        depth = std::max(depth, f.depth);
+        if (f.node >= b.n_nodes()) return "child index out of range";
         if (++visited > b.n_nodes()) return "a node reached twice";
-        const uint32_t *w = node(n);
+        const uint32_t *w = &b.nodes[f.node * 20];
         uint32_t imask = w[3] >> 24, inner_rank = 0;
         const uint8_t *meta = (const uint8_t *)&w[6];
         for (int s = 0; s < 8; s++) {
             float mn[3], mx[3];
             slot_box(w, s, mn, mx);
+            for (int a = 0; a < 3; a++) {
+                mn[a] = std::max(mn[a], f.mn[a]);
+                mx[a] = std::min(mx[a], f.mx[a]);
+            }
             if ((imask >> s) & 1u) {
-                size_t c = w[4] + inner_rank++;
-                if (c >= b.n_nodes()) return "child index out of range";
-                const uint32_t *cw = node(c);
-                uint32_t cim = cw[3] >> 24;
-                const uint8_t *cm = (const uint8_t *)&cw[6];
-                for (int k = 0; k < 8; k++) {
-                    if (!((cim >> k) & 1u) && cm[k] == 0xff) continue;
-                    float a[3], z[3];
-                    slot_box(cw, k, a, z);
-                    for (int x = 0; x < 3; x++)
-                        if (a[x] < mn[x] - 1e-4f * (1 + std::fabs(mn[x])) || z[x] > mx[x] + 1e-4f * (1 + std::fabs(mx[x])))
-                            return "a child's box outside its slot's";
-                }
-                st.emplace_back(c, d + 1);
+                Frame c{w[4] + inner_rank++, f.depth + 1, {mn[0], mn[1], mn[2]}, {mx[0], mx[1], mx[2]}};
+                st.push_back(c);
             } else if (meta[s] != 0xff) {
                 uint32_t first = w[5] + (meta[s] & 31u), cnt = ((meta[s] >> 5) & 3u) + 1u;
                 for (uint32_t k = 0; k < cnt; k++) {
@@ -281,14 +276,12 @@ std::string bvh8_check(const Bvh8 &b, size_t n_tris, size_t &depth) {
                     std::memcpy(&orig, &t.e2[3], 4);
                     if (orig >= n_tris) return "reference index out of range";
                     seen[orig]++;
-                    for (int c3 = 0; c3 < 3; c3++) {
-                        float v[3];
-                        for (int x = 0; x < 3; x++)
-                            v[x] = t.v0[x] + (c3 == 1 ? t.e1[x] : c3 == 2 ? t.e2[x] : 0.0f);
-                        for (int x = 0; x < 3; x++)
-                            if (v[x] < mn[x] - 1e-4f * (1 + std::fabs(mn[x])) || v[x] > mx[x] + 1e-4f * (1 + std::fabs(mx[x])))
-                                return "a triangle outside its slot's box";
-                    }
+                    for (int c3 = 0; c3 < 3; c3++)
+                        for (int x = 0; x < 3; x++) {
+                            float v = t.v0[x] + (c3 == 1 ? t.e1[x] : c3 == 2 ? t.e2[x] : 0.0f);
+                            float tol = 1e-4f * (1.0f + std::fabs(v));
+                            if (v < mn[x] - tol || v > mx[x] + tol) return "a triangle outside a box on its path";
+                        }
                 }
             }
         }
