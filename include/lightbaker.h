@@ -129,6 +129,9 @@ int lb_set_pass_kernel(lb_gpu *gpu, int kind);
  * the ray index (and the bottom bits that remain): large values give the shader's order (bands of
  * elevation), 0 wedges of azimuth. Results are identical; speed is not (lb_autotune picks). */
 int lb_set_ray_order(lb_gpu *gpu, int direct, int gather);
+/* Lane refill in the warp kernels' occlusion and gather rays over the BVH2 (default on): a lane whose
+ * ray has ended starts the item's next one instead of waiting for its round. Same results. */
+int lb_set_refill(lb_gpu *gpu, int on);
 /* The BVH the warp kernels walk: 2, the reference's (as uploaded); 8, the 8-wide BVH lb_scene_upload
  * collapses from it (80-byte nodes, 8-bit child boxes). Same hits, faces and records. */
 int lb_set_bvh(lb_gpu *gpu, int width);

@@ -143,6 +143,10 @@ class Gpu:
         """The warp kernels' ray order (see include/lightbaker.h lb_set_ray_order). Same results."""
         N.check(N.lib().lb_set_ray_order(self._h, int(direct), int(gather)), "lb_set_ray_order")
 
+    def set_refill(self, on: bool) -> None:
+        """Lane refill in the warp kernels (occlusion and gather rays over the BVH2). Same results."""
+        N.check(N.lib().lb_set_refill(self._h, int(on)), "lb_set_refill")
+
     def set_bvh(self, width: int) -> None:
         """The BVH the warp kernels walk: 2 (the reference's) or 8 (8-wide, compressed). Same results."""
         N.check(N.lib().lb_set_bvh(self._h, int(width)), "lb_set_bvh")

@@ -104,6 +104,7 @@ struct lb_plan {
     bool autotune = false;
     int group_direct = 8, group_gather = 8;  // ray order for the warp passes
     int bvh_direct = 2, bvh_gather = 2, bvh_volume = 2;  // BVH width for the warp passes
+    int refill_direct = 1, refill_gather = 1;          // lane refill for the warp passes
     std::string tuned;  // what the autotuner picked
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -355,14 +356,23 @@ void autotune(lb_plan &p) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const int orders[] = {8, 3, 2, 1, 0};
+    const int orders[] = {8, 2, 0};
+    struct Shape {
+        int bvh, refill;
+    };
+    const Shape shapes[] = {{2, 1}, {2, 0}, {8, 0}};
     std::string report;
     for (int pass : {LB_PASS_DIRECT, LB_PASS_GATHER}) {
-        int full = pass == LB_PASS_DIRECT ? p.blocks_direct : p.blocks_gather;
-        int per_sm = std::max(1, full / std::max(1, p.g->sms));
         float best = 1e30f;
-        int best_order = 8, best_blocks = full;
-        for (int order : orders)
+        int best_order = 8, best_blocks = 0, best_bvh = 2, best_refill = 1;
+        for (const Shape &sh : shapes)
+        for (int order : orders) {
+            WarpPass probe{};
+            probe.pass = pass;
+            probe.sms = p.g->sms;
+            probe.bvh = sh.bvh;
+            int full = lb_warp_pass_blocks(probe);
+            int per_sm = std::max(1, full / std::max(1, p.g->sms));
             for (int bps = per_sm; bps >= 1; bps = bps > 1 ? std::max(1, bps / 2) : 0) {
                 WarpPass w{};
                 w.pass = pass;
@@ -378,6 +388,8 @@ void autotune(lb_plan &p) {
                 w.sms = p.g->sms;
                 w.blocks = bps * p.g->sms;
                 w.group = order;
+                w.bvh = sh.bvh;
+                w.refill = sh.refill;
                 float t = 0;
                 for (int rep = 0; rep < 2; rep++) {
                     ck(cudaEventRecord(e0, st), "autotune");
@@ -390,18 +402,26 @@ void autotune(lb_plan &p) {
                     best = t;
                     best_order = order;
                     best_blocks = bps * p.g->sms;
+                    best_bvh = sh.bvh;
+                    best_refill = sh.refill;
                 }
                 if (bps == 1) break;
             }
+        }
         if (pass == LB_PASS_DIRECT) {
             p.group_direct = best_order;
             p.blocks_direct = best_blocks;
+            p.bvh_direct = best_bvh;
+            p.refill_direct = best_refill;
         } else {
             p.group_gather = best_order;
             p.blocks_gather = best_blocks;
+            p.bvh_gather = best_bvh;
+            p.refill_gather = best_refill;
         }
-        report += std::string(pass == LB_PASS_DIRECT ? "direct" : "gather") + ": order " + std::to_string(best_order) +
-                  ", " + std::to_string(best_blocks / std::max(1, p.g->sms)) + " blocks/SM (" + std::to_string(best) +
+        report += std::string(pass == LB_PASS_DIRECT ? "direct" : "gather") + ": bvh " + std::to_string(best_bvh) +
+                  ", refill " + std::to_string(best_refill) + ", order " + std::to_string(best_order) + ", " +
+                  std::to_string(best_blocks / std::max(1, p.g->sms)) + " blocks/SM (" + std::to_string(best) +
                   " ms on " + std::to_string(sample.size()) + " texels); ";
     }
     cudaEventDestroy(e0);
@@ -475,6 +495,7 @@ void capture(lb_plan &p) {
             w.blocks = p.blocks_direct;
             w.group = p.group_direct;
             w.bvh = p.bvh_direct;
+            w.refill = p.refill_direct;
             ck(lb_launch_pass_warp(w, st), "direct pass");
         }
         ck(lb_post_direct(a, int(h.lightmap.padding) + 4, s, st), "direct texel passes");
@@ -498,6 +519,7 @@ void capture(lb_plan &p) {
             gw.blocks = p.blocks_gather;
             gw.group = p.group_gather;
             gw.bvh = p.bvh_gather;
+            gw.refill = p.refill_gather;
             ck(lb_launch_pass_warp(gw, st), "gather pass");
             ck(lb_post_bounce(a, p.gather_out.as<float4>(), int(b.gi_filter * p.ds), p.wr.as<float>(),
                               int(h.lightmap.padding + 2 * p.ds + 2), s, st),
@@ -603,6 +625,7 @@ lb_plan *lb_plan_create(lb_gpu *g, const uint8_t *scene, size_t len, const lb_ba
         p->group_direct = g->group_direct;
         p->group_gather = g->group_gather;
         p->bvh_direct = p->bvh_gather = p->bvh_volume = g->bvh;
+        p->refill_direct = p->refill_gather = g->refill;
         build(*p);
         if (p->autotune) autotune(*p);
         capture(*p);

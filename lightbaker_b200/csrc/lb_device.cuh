@@ -214,6 +214,86 @@ __device__ __forceinline__ Hit trace(const Scene &S, float3 o, float3 d, float t
     return hit;
 }
 
+// trace() as a resumable walk: its state between nodes, so that a lane whose ray has ended can start
+// another while its warp's other lanes go on. step() does what one pass of trace()'s loop does (one
+// node: a leaf's triangles, or an inner node's two children, then a pop when there is nothing to
+// descend to), so a ray visits the same nodes in the same order and ends with the same hit.
+template <bool COUNT>
+struct Walk2 {
+    float3 o, d, inv;
+    uint32_t ray;
+    bool any, done;
+    Hit hit;
+    float4 nlo, nhi;
+    int sp;
+    uint32_t stack[STACK];
+    __device__ __forceinline__ void start(const Scene &S, float3 o_, float3 d_, float tmax, bool any_, uint32_t ray_,
+                                          Count &c) {
+        o = o_;
+        d = d_;
+        any = any_;
+        ray = ray_;
+        hit = Hit{tmax, NONE, false};
+        c.rays++;
+        if (COUNT) c.nodes++;
+        float3 dd = mk(fabsf(d.x) < 1e-12f ? 1e-12f : d.x, fabsf(d.y) < 1e-12f ? 1e-12f : d.y,
+                       fabsf(d.z) < 1e-12f ? 1e-12f : d.z);
+        inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+        sp = 0;
+        nlo = __ldg(&S.nodes[0]);
+        nhi = __ldg(&S.nodes[1]);
+        done = false;
+    }
+    __device__ __forceinline__ void step(const Scene &S, uint32_t seed, Count &c) {
+        uint32_t first = __float_as_uint(nlo.w), count = __float_as_uint(nhi.w);
+        if (count > 0u) {
+            for (uint32_t i = first; i < first + count; i++) {
+                if (COUNT) c.tris++;
+                float4 v0 = __ldg(&S.tris[3 * i]), e1 = __ldg(&S.tris[3 * i + 1]), e2 = __ldg(&S.tris[3 * i + 2]);
+                float3 p = cross3(d, xyz(e2));
+                float det = dot3(xyz(e1), p);
+                if (fabsf(det) < 1e-12f) continue;
+                float id = 1.0f / det;
+                float3 s = sub(o, xyz(v0));
+                float u = dot3(s, p) * id;
+                if (u < 0.0f || u > 1.0f) continue;
+                float3 q = cross3(s, xyz(e1));
+                float v = dot3(d, q) * id;
+                if (v < 0.0f || u + v > 1.0f) continue;
+                float t = dot3(xyz(e2), q) * id;
+                if (t > 1e-4f && t < hit.t && stops<COUNT>(S, i, v0.w, ray, seed, c)) {
+                    hit = Hit{t, i, det < 0.0f};
+                    if (any) {
+                        done = true;
+                        return;
+                    }
+                }
+            }
+        } else if (first + 1u < S.n_nodes) {
+            if (COUNT) c.nodes += 2;
+            float4 alo = __ldg(&S.nodes[2 * first]), ahi = __ldg(&S.nodes[2 * first + 1]);
+            float4 blo = __ldg(&S.nodes[2 * first + 2]), bhi = __ldg(&S.nodes[2 * first + 3]);
+            float ta = box(o, inv, alo, ahi, hit.t);
+            float tb = box(o, inv, blo, bhi, hit.t);
+            bool a_near = ta <= tb;
+            float tn = fminf(ta, tb), tf = fmaxf(ta, tb);
+            if (tn < FAR) {
+                if (tf < FAR && sp < STACK) stack[sp++] = a_near ? first + 1u : first;
+                nlo = a_near ? alo : blo;
+                nhi = a_near ? ahi : bhi;
+                return;
+            }
+        }
+        if (sp == 0) {
+            done = true;
+            return;
+        }
+        uint32_t n = stack[--sp];
+        nlo = __ldg(&S.nodes[2 * n]);
+        nhi = __ldg(&S.nodes[2 * n + 1]);
+    }
+};
+
 // The same query over the 8-wide BVH: the nearest accepted hit within tmax (any: the first accepted),
 // the same triangle test in the same arithmetic, so every hit, its t and its face are the BVH2 walk's.
 // A node's eight child boxes are tested at once; its leaf slots' triangles first, then its hit inner

@@ -69,6 +69,12 @@ struct RayOrder {
         uint32_t r = grouped ? (((round >> b) << top) | lane_bits | (round & lo_mask)) : round * 32u + lane_bits;
         return r;
     }
+    // the ray handed out seq-th (lane refill): the same order, round by round
+    __device__ __forceinline__ uint32_t at(uint32_t seq) const {
+        if (!grouped) return seq;
+        uint32_t round = seq >> 5;
+        return ((round >> b) << top) | ((seq & 31u) << b) | (round & lo_mask);
+    }
 };
 
 // An item: its record (pos, normal, dx, dy), the position optionally taken from a second array
@@ -128,7 +134,7 @@ __device__ __forceinline__ void flush_counts(Count &c, unsigned long long *count
 template <int BVH, bool COUNT>
 __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
-                                                   unsigned long long *counters, int group) {
+                                                   unsigned long long *counters, int group, int refill) {
     __shared__ float s_term[WARPS][AO_CAP];
     __shared__ uint8_t s_hit[WARPS][AO_CAP];
     const int lane = threadIdx.x & 31;
@@ -206,6 +212,52 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
         uint32_t nback = 0;
         const RayOrder ord(rays, AO_CAP, group, lane);
         const int w = threadIdx.x >> 5;
+        if (BVH == 2 && refill && rays <= AO_CAP) {
+            // lane refill: a lane takes the item's next ray as soon as its own has ended
+            Walk2<COUNT> wk;
+            uint32_t seq = uint32_t(lane), next = 32, r = 0, myback = 0;
+            bool have = seq < rays;
+            if (have) {
+                r = ord.at(seq);
+                wk.start(S, o, cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f),
+                         P.reach[0], false, key + r + 2000u, c);
+            }
+            while (__any_sync(FULL, have)) {
+                if (have) wk.step(S, seed, c);
+                bool fin = have && wk.done;
+                if (fin) {
+                    bool hit = wk.hit.tri != NONE;
+                    float term = 0.0f;
+                    if (hit) {
+                        float kk = wk.hit.t / P.reach[0];
+                        term = 1.0f - kk * kk;
+                        if (wk.hit.back && wk.hit.t < P.ground[3]) myback++;
+                    }
+                    s_term[w][r] = term;
+                    s_hit[w][r] = hit;
+                }
+                unsigned fm = __ballot_sync(FULL, fin);
+                if (fin) {
+                    seq = next + __popc(fm & ((1u << lane) - 1u));
+                    have = seq < rays;
+                    if (have) {
+                        r = ord.at(seq);
+                        wk.start(S, o,
+                                 cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f),
+                                 P.reach[0], false, key + r + 2000u, c);
+                    }
+                }
+                next += __popc(fm);
+            }
+            for (int ofs = 16; ofs > 0; ofs >>= 1) myback += __shfl_down_sync(FULL, myback, ofs);
+            nback = __shfl_sync(FULL, myback, 0);
+            __syncwarp();
+            for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
+                uint32_t rr = r0 + uint32_t(lane);
+                occ = ordered_add(occ, rr < rays ? s_term[w][rr] : 0.0f, rr < rays && s_hit[w][rr]);
+            }
+            __syncwarp();
+        } else
         for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
             uint32_t r = ord.ray(r0 >> 5);
             bool hit = false, bk = false;
@@ -228,7 +280,7 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
             }
             nback += __popc(__ballot_sync(FULL, bk));
         }
-        if (ord.grouped) {
+        if (!(BVH == 2 && refill && rays <= AO_CAP) && ord.grouped) {
             __syncwarp();
             for (uint32_t r0 = 0; r0 < rays; r0 += 32) occ = ordered_add(occ, s_term[w][r0 + lane], s_hit[w][r0 + lane]);
             __syncwarp();
@@ -244,7 +296,7 @@ template <int BVH, bool COUNT>
 __global__ void __launch_bounds__(256) gather_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const float4 *pos_override, const uint32_t *n_dev, uint32_t n_host,
                                                    uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
-                                                   unsigned long long *counters, int group) {
+                                                   unsigned long long *counters, int group, int refill) {
     __shared__ float3 s_term[WARPS][GI_CAP];
     __shared__ uint8_t s_on[WARPS][GI_CAP];
     const int lane = threadIdx.x & 31;
@@ -266,6 +318,56 @@ __global__ void __launch_bounds__(256) gather_warp(Scene S, lb_params P, const f
         uint32_t nback = 0;
         const RayOrder ord(rays, GI_CAP, group, lane);
         const int w = threadIdx.x >> 5;
+        const bool refilling = BVH == 2 && refill && rays <= GI_CAP;
+        if (refilling) {
+            // lane refill: a lane takes the item's next ray as soon as its own has ended
+            Walk2<COUNT> wk;
+            uint32_t seq = uint32_t(lane), next = 32, r = 0, myback = 0;
+            bool have = seq < rays;
+            auto begin = [&](uint32_t rr) {
+                float jx = rnd(key + rr, 19u, seed) - 0.5f, jy = rnd(key + rr, 23u, seed) - 0.5f;
+                float3 oo = add(add(add(pos, scl(dx, jx)), scl(dy, jy)), scl(nrm, P.reach[2]));
+                float3 dd = cosine(fract((__uint2float_rn(rr) + 0.5f) / frays + s1), fract(radical(rr) + s2), f);
+                wk.start(S, oo, dd, P.reach[1], false, key + rr + 4000u, c);
+            };
+            if (have) {
+                r = ord.at(seq);
+                begin(r);
+            }
+            while (__any_sync(FULL, have)) {
+                if (have) wk.step(S, seed, c);
+                bool fin = have && wk.done;
+                if (fin) {
+                    float3 term = mk(0.f, 0.f, 0.f);
+                    bool on = true;
+                    if (wk.hit.tri == NONE) term = sky(P, wk.d);
+                    else if (wk.hit.back) {
+                        on = false;
+                        myback++;
+                    } else term = bounced(S, P, light, n_light, wk.o, wk.d, wk.hit);
+                    s_term[w][r] = term;
+                    s_on[w][r] = on;
+                }
+                unsigned fm = __ballot_sync(FULL, fin);
+                if (fin) {
+                    seq = next + __popc(fm & ((1u << lane) - 1u));
+                    have = seq < rays;
+                    if (have) {
+                        r = ord.at(seq);
+                        begin(r);
+                    }
+                }
+                next += __popc(fm);
+            }
+            for (int ofs = 16; ofs > 0; ofs >>= 1) myback += __shfl_down_sync(FULL, myback, ofs);
+            nback = __shfl_sync(FULL, myback, 0);
+            __syncwarp();
+            for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
+                uint32_t rr = r0 + uint32_t(lane);
+                sum = ordered_add3(sum, rr < rays ? s_term[w][rr] : mk(0.f, 0.f, 0.f), rr < rays && s_on[w][rr]);
+            }
+            __syncwarp();
+        } else
         for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
             uint32_t r = ord.ray(r0 >> 5);
             bool on = false, bk = false;
@@ -293,7 +395,7 @@ __global__ void __launch_bounds__(256) gather_warp(Scene S, lb_params P, const f
             }
             nback += __popc(__ballot_sync(FULL, bk));
         }
-        if (ord.grouped) {
+        if (!refilling && ord.grouped) {
             __syncwarp();
             for (uint32_t r0 = 0; r0 < rays; r0 += 32) sum = ordered_add3(sum, s_term[w][r0 + lane], s_on[w][r0 + lane]);
             __syncwarp();
@@ -402,11 +504,12 @@ template <int BVH, bool COUNT> void launch(const WarpPass &w, int blocks, cudaSt
     switch (w.pass) {
     case LB_PASS_DIRECT:
         lbd::direct_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base,
-                                                               w.out, w.counters, w.group);
+                                                               w.out, w.counters, w.group, w.refill);
         break;
     case LB_PASS_GATHER:
         lbd::gather_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host,
-                                                               w.base, w.light, w.n_light, w.out, w.counters, w.group);
+                                                               w.base, w.light, w.n_light, w.out, w.counters, w.group,
+                                                               w.refill);
         break;
     default:
         lbd::volume_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light, w.out,
