@@ -151,6 +151,18 @@ int lb_smooth(lb_gpu *gpu, uint32_t w, uint32_t h, const uint32_t *chart, const 
  * (values and valid). Uses scratch the handle keeps (a ping-pong copy of the tile). */
 int lb_fill(lb_gpu *gpu, uint32_t w, uint32_t h, const uint32_t *chart, float *values, int channels,
             uint8_t *valid, int rings);
+/* lb_fill without allocating anything, for callers that cannot allocate device memory: a host
+ * application that owns all of the GPU's memory through its own allocator (an engine or an editor
+ * hosting the baker as a plugin), or a path where an allocation would synchronise the device while
+ * other work is in flight. No counterpart in the reference. The fill's ping-pong copy lives in a
+ * fixed 4.25 MiB device array that every GPU loading the library holds until exit; tiles of more
+ * than 512 x 512 texels are rejected (LB_ESCRATCH). Arrays are device pointers as for lb_fill;
+ * enqueued on `stream` (a cudaStream_t, NULL: the default stream) on the current device. The first
+ * call on a device looks the array's address up (cudaGetSymbolAddress): make it before any stream
+ * capture. Calls share the array: calls that overlap on the GPU race. Nothing in it needs clearing:
+ * each ring writes every texel of the copy it reads next. */
+int lb_fill_fixed(void *stream, uint32_t w, uint32_t h, const uint32_t *chart, float *values, int channels,
+                  uint8_t *valid, int rings);
 /* sun_field (filter.rs:106-141): the sun's distance field from each texel's grid_side^2 hard bits
  * (grid side 1..5), 0.5 at a shadow's edge, 0 and 1 at `radius` texels; -1 where not covered. */
 int lb_sun_field(lb_gpu *gpu, uint32_t w, uint32_t h, const uint32_t *chart, const float *normal,

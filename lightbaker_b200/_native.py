@@ -96,6 +96,8 @@ SIGNATURES = {
     "lb_smooth": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                             C.c_void_p, C.c_int, C.c_void_p]),
     "lb_fill": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "lb_fill_fixed": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                C.c_int]),
     "lb_sun_field": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                C.c_uint32, C.c_float, C.c_void_p]),
     "lb_prepare": (C.c_void_p, [C.c_char_p, C.c_size_t]),

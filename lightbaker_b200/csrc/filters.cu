@@ -7,6 +7,8 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "lb_device.cuh"
 #include "lb_runtime.h"
@@ -219,3 +221,55 @@ int lb_sun_field(lb_gpu *g, uint32_t w, uint32_t h, const uint32_t *chart, const
 }
 
 }  // extern "C"
+
+// ---- lb_fill_fixed: the fill with its ping-pong copy in a fixed device array, allocating nothing ----
+
+namespace {
+constexpr uint32_t FIXED_TEXELS = 512u * 512u;  // the largest tile lb_fill_fixed takes
+constexpr size_t FIXED_VALUES = size_t(FIXED_TEXELS) * 4 * sizeof(float);
+}  // namespace
+
+// The scratch every lb_fill_fixed call on a device uses: FIXED_TEXELS texels of four channels and their
+// flags (4.25 MiB), held by every GPU that loads the library until the process exits.
+static __device__ __align__(256) unsigned char lb_fill_scratch[FIXED_VALUES + FIXED_TEXELS];
+
+namespace {
+// the array's device address, looked up once per device (host code may not take it by name)
+std::mutex g_fixed_mutex;
+void *g_fixed_ptr[128] = {nullptr};
+}  // namespace
+
+extern "C" int lb_fill_fixed(void *stream, uint32_t w, uint32_t h, const uint32_t *chart, float *values, int channels,
+                             uint8_t *valid, int rings) {
+    if (!chart || !values || !valid || channels < 1 || channels > 4 || rings < 0 || w == 0 || h == 0) {
+        lb_set_error("lb_fill_fixed: bad arguments (channels 1..4)");
+        return LB_EINVAL;
+    }
+    if (uint64_t(w) * h > FIXED_TEXELS) {
+        lb_set_error("lb_fill_fixed: a tile of " + std::to_string(uint64_t(w) * h) + " texels is over the fixed scratch's " +
+                     std::to_string(FIXED_TEXELS) + " (512 x 512); use lb_fill");
+        return LB_ESCRATCH;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return lb_cuda_fail(e, "lb_fill_fixed");
+    if (dev < 0 || dev >= 128) {
+        lb_set_error("lb_fill_fixed: device index out of range");
+        return LB_EINVAL;
+    }
+    void *base;
+    {
+        std::lock_guard<std::mutex> lock(g_fixed_mutex);
+        if (!g_fixed_ptr[dev]) {
+            void *p = nullptr;
+            e = cudaGetSymbolAddress(&p, lb_fill_scratch);
+            if (e != cudaSuccess) return lb_cuda_fail(e, "lb_fill_fixed: cudaGetSymbolAddress");
+            g_fixed_ptr[dev] = p;
+        }
+        base = g_fixed_ptr[dev];
+    }
+    float *sv = (float *)base;
+    uint8_t *sk = (uint8_t *)base + FIXED_VALUES;
+    e = lb_fill_with_scratch(w, h, chart, values, channels, valid, rings, sv, sk, (cudaStream_t)stream);
+    return e == cudaSuccess ? LB_OK : lb_cuda_fail(e, "lb_fill_fixed");
+}
