@@ -129,7 +129,12 @@ int lb_set_pass_kernel(lb_gpu *gpu, int kind);
  * the ray index (and the bottom bits that remain): large values give the shader's order (bands of
  * elevation), 0 wedges of azimuth. Results are identical; speed is not (lb_autotune picks). */
 int lb_set_ray_order(lb_gpu *gpu, int direct, int gather);
-/* Lane refill in the warp kernels' occlusion and gather rays over the BVH2 (default on): a lane whose
+/* Leaf lists for the warp kernels' occlusion rays over the BVH2 (default on): a warp gathers once for
+ * a texel the leaves within the occlusion reach of its sample point, on its front side, nearest first,
+ * and every occlusion ray tests that list instead of walking the tree. Same hits (between triangles
+ * at exactly equal distance the first found in list order). */
+int lb_set_near(lb_gpu *gpu, int on);
+/* Lane refill in the warp kernels' occlusion and gather rays over the BVH2 (default off): a lane whose
  * ray has ended starts the item's next one instead of waiting for its round. Same results. */
 int lb_set_refill(lb_gpu *gpu, int on);
 /* The BVH the warp kernels walk: 2, the reference's (as uploaded); 8, the 8-wide BVH lb_scene_upload

@@ -147,6 +147,10 @@ class Gpu:
         """Lane refill in the warp kernels (occlusion and gather rays over the BVH2). Same results."""
         N.check(N.lib().lb_set_refill(self._h, int(on)), "lb_set_refill")
 
+    def set_near(self, on: bool) -> None:
+        """Leaf lists for the warp kernels' occlusion rays (BVH2). Same results."""
+        N.check(N.lib().lb_set_near(self._h, int(on)), "lb_set_near")
+
     def set_bvh(self, width: int) -> None:
         """The BVH the warp kernels walk: 2 (the reference's) or 8 (8-wide, compressed). Same results."""
         N.check(N.lib().lb_set_bvh(self._h, int(width)), "lb_set_bvh")

@@ -104,7 +104,8 @@ struct lb_plan {
     bool autotune = false;
     int group_direct = 8, group_gather = 8;  // ray order for the warp passes
     int bvh_direct = 2, bvh_gather = 2, bvh_volume = 2;  // BVH width for the warp passes
-    int refill_direct = 1, refill_gather = 1;          // lane refill for the warp passes
+    int refill_direct = 0, refill_gather = 0;          // lane refill for the warp passes
+    int near_direct = 1;                               // leaf lists for the occlusion rays
     std::string tuned;  // what the autotuner picked
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -358,15 +359,16 @@ void autotune(lb_plan &p) {
     cudaEventCreate(&e1);
     const int orders[] = {8, 2, 0};
     struct Shape {
-        int bvh, refill;
+        int bvh, refill, near;
     };
-    const Shape shapes[] = {{2, 1}, {2, 0}, {8, 0}};
+    const Shape shapes[] = {{2, 0, 1}, {2, 0, 0}, {2, 1, 0}, {8, 0, 0}};
     std::string report;
     for (int pass : {LB_PASS_DIRECT, LB_PASS_GATHER}) {
         float best = 1e30f;
-        int best_order = 8, best_blocks = 0, best_bvh = 2, best_refill = 1;
+        int best_order = 8, best_blocks = 0, best_bvh = 2, best_refill = 0, best_near = 0;
         for (const Shape &sh : shapes)
         for (int order : orders) {
+            if (pass == LB_PASS_GATHER && sh.near) continue;
             WarpPass probe{};
             probe.pass = pass;
             probe.sms = p.g->sms;
@@ -390,6 +392,7 @@ void autotune(lb_plan &p) {
                 w.group = order;
                 w.bvh = sh.bvh;
                 w.refill = sh.refill;
+                w.near = sh.near;
                 float t = 0;
                 for (int rep = 0; rep < 2; rep++) {
                     ck(cudaEventRecord(e0, st), "autotune");
@@ -404,6 +407,7 @@ void autotune(lb_plan &p) {
                     best_blocks = bps * p.g->sms;
                     best_bvh = sh.bvh;
                     best_refill = sh.refill;
+                    best_near = sh.near;
                 }
                 if (bps == 1) break;
             }
@@ -413,6 +417,7 @@ void autotune(lb_plan &p) {
             p.blocks_direct = best_blocks;
             p.bvh_direct = best_bvh;
             p.refill_direct = best_refill;
+            p.near_direct = best_near;
         } else {
             p.group_gather = best_order;
             p.blocks_gather = best_blocks;
@@ -420,7 +425,7 @@ void autotune(lb_plan &p) {
             p.refill_gather = best_refill;
         }
         report += std::string(pass == LB_PASS_DIRECT ? "direct" : "gather") + ": bvh " + std::to_string(best_bvh) +
-                  ", refill " + std::to_string(best_refill) + ", order " + std::to_string(best_order) + ", " +
+                  ", refill " + std::to_string(best_refill) + ", near " + std::to_string(best_near) + ", order " + std::to_string(best_order) + ", " +
                   std::to_string(best_blocks / std::max(1, p.g->sms)) + " blocks/SM (" + std::to_string(best) +
                   " ms on " + std::to_string(sample.size()) + " texels); ";
     }
@@ -496,6 +501,7 @@ void capture(lb_plan &p) {
             w.group = p.group_direct;
             w.bvh = p.bvh_direct;
             w.refill = p.refill_direct;
+            w.near = p.near_direct;
             ck(lb_launch_pass_warp(w, st), "direct pass");
         }
         ck(lb_post_direct(a, int(h.lightmap.padding) + 4, s, st), "direct texel passes");
@@ -626,6 +632,7 @@ lb_plan *lb_plan_create(lb_gpu *g, const uint8_t *scene, size_t len, const lb_ba
         p->group_gather = g->group_gather;
         p->bvh_direct = p->bvh_gather = p->bvh_volume = g->bvh;
         p->refill_direct = p->refill_gather = g->refill;
+        p->near_direct = g->near;
         build(*p);
         if (p->autotune) autotune(*p);
         capture(*p);

@@ -294,6 +294,148 @@ struct Walk2 {
     }
 };
 
+// ---- rays that end within a ball: occlusion rays (trace.wgsl:226-241) ----
+// Every triangle a ray of length <= r from o can hit lies in a BVH2 leaf whose box comes within r of o,
+// and, when the rays leave through the hemisphere about n (cosine rays: d.n >= 0), on the n side of o.
+// A warp gathers those leaves once for an item; each of its rays then tests the same short list, a loop
+// its lanes run together, instead of each walking the tree from the root on its own path.
+
+constexpr int BALL_FRONT = 128;   // nodes one level of the ball query holds
+constexpr int BALL_LEAVES = 192;  // leaves an item's list holds (more: the item walks the tree instead)
+
+__device__ __forceinline__ float box_dist2(float3 p, float4 mn, float4 mx) {
+    float dx = fmaxf(fmaxf(mn.x - p.x, 0.0f), p.x - mx.x);
+    float dy = fmaxf(fmaxf(mn.y - p.y, 0.0f), p.y - mx.y);
+    float dz = fmaxf(fmaxf(mn.z - p.z, 0.0f), p.z - mx.z);
+    return dx * dx + dy * dy + dz * dz;
+}
+// the largest (x - o).n over the box's corners
+__device__ __forceinline__ float box_front(float3 o, float3 n, float4 mn, float4 mx) {
+    float x = n.x >= 0.0f ? mx.x : mn.x, y = n.y >= 0.0f ? mx.y : mn.y, z = n.z >= 0.0f ? mx.z : mn.z;
+    return (x - o.x) * n.x + (y - o.y) * n.y + (z - o.z) * n.z;
+}
+
+// Warp-wide: the leaves within reach r of o on the n side (by a margin), into list, nearest first.
+// Returns their count, or -1 when a level or the list would overflow. All lanes return the same value.
+template <bool COUNT>
+__device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float3 n, uint32_t *fa, uint32_t *fb,
+                                        uint32_t *list, int lane, Count &c) {
+    const unsigned FULLM = 0xffffffffu;
+    float rr = r * 1.0001f + 1e-5f, r2 = rr * rr, margin = -(r * 1e-3f + 1e-4f);
+    float4 rlo = __ldg(&S.nodes[0]), rhi = __ldg(&S.nodes[1]);
+    uint32_t rfirst = __float_as_uint(rlo.w), rcount = __float_as_uint(rhi.w);
+    if (rcount > 0u) {
+        if (lane == 0) list[0] = 0;
+        __syncwarp();
+        return 1;
+    }
+    if (rfirst + 1u >= S.n_nodes) return 0;
+    if (lane < 2) fa[lane] = rfirst + uint32_t(lane);
+    __syncwarp();
+    int nf = 2, nl = 0;
+    while (nf > 0) {
+        int nn = 0;
+        for (int base = 0; base < nf; base += 32) {
+            int i = base + lane;
+            bool leaf = false, inner = false;
+            uint32_t node = 0, first = 0;
+            if (i < nf) {
+                node = fa[i];
+                float4 lo = __ldg(&S.nodes[2 * node]), hi = __ldg(&S.nodes[2 * node + 1]);
+                if (COUNT) c.nodes++;
+                if (box_dist2(o, lo, hi) <= r2 && box_front(o, n, lo, hi) >= margin) {
+                    first = __float_as_uint(lo.w);
+                    uint32_t count = __float_as_uint(hi.w);
+                    if (count > 0u) leaf = true;
+                    else if (first + 1u < S.n_nodes) inner = true;
+                }
+            }
+            unsigned lm = __ballot_sync(FULLM, leaf), im = __ballot_sync(FULLM, inner);
+            unsigned below = (1u << lane) - 1u;
+            int lp = nl + __popc(lm & below), ip = nn + 2 * __popc(im & below);
+            if (leaf && lp < BALL_LEAVES) list[lp] = node;
+            if (inner && ip + 1 < BALL_FRONT) {
+                fb[ip] = first;
+                fb[ip + 1] = first + 1u;
+            }
+            nl += __popc(lm);
+            nn += 2 * __popc(im);
+        }
+        __syncwarp();
+        if (nl > BALL_LEAVES || nn > BALL_FRONT) return -1;
+        uint32_t *t = fa;
+        fa = fb;
+        fb = t;
+        nf = nn;
+    }
+    // nearest first: rank by distance (ties by index), then place; keys in fb
+    float *key = (float *)fb;
+    for (int i = lane; i < nl; i += 32) {
+        uint32_t node = list[i];
+        key[i] = box_dist2(o, __ldg(&S.nodes[2 * node]), __ldg(&S.nodes[2 * node + 1]));
+    }
+    __syncwarp();
+    uint32_t mine[BALL_LEAVES / 32];
+    int rank[BALL_LEAVES / 32];
+    for (int q = 0; q < BALL_LEAVES / 32; q++) {
+        int i = q * 32 + lane;
+        rank[q] = -1;
+        if (i < nl) {
+            float ki = key[i];
+            int rk = 0;
+            for (int j = 0; j < nl; j++) {
+                float kj = key[j];
+                rk += (kj < ki || (kj == ki && j < i)) ? 1 : 0;
+            }
+            rank[q] = rk;
+            mine[q] = list[i];
+        }
+    }
+    __syncwarp();
+    for (int q = 0; q < BALL_LEAVES / 32; q++)
+        if (rank[q] >= 0) fa[rank[q]] = mine[q];
+    __syncwarp();
+    for (int i = lane; i < nl; i += 32) list[i] = fa[i];
+    __syncwarp();
+    return nl;
+}
+
+// trace() over a leaf list: the nearest accepted hit within tmax among the listed leaves' triangles,
+// with the walk's box test (culled by the nearest hit so far) and triangle test.
+template <bool COUNT>
+__device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, int nl, float3 o, float3 d, float tmax,
+                                          uint32_t ray, uint32_t seed, Count &c) {
+    Hit hit{tmax, NONE, false};
+    c.rays++;
+    float3 dd = mk(fabsf(d.x) < 1e-12f ? 1e-12f : d.x, fabsf(d.y) < 1e-12f ? 1e-12f : d.y,
+                   fabsf(d.z) < 1e-12f ? 1e-12f : d.z);
+    float3 inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+    for (int k = 0; k < nl; k++) {
+        uint32_t node = list[k];
+        float4 lo = __ldg(&S.nodes[2 * node]), hi = __ldg(&S.nodes[2 * node + 1]);
+        if (COUNT) c.nodes++;
+        if (!(box(o, inv, lo, hi, hit.t) < FAR)) continue;
+        uint32_t first = __float_as_uint(lo.w), count = __float_as_uint(hi.w);
+        for (uint32_t i = first; i < first + count; i++) {
+            if (COUNT) c.tris++;
+            float4 v0 = __ldg(&S.tris[3 * i]), e1 = __ldg(&S.tris[3 * i + 1]), e2 = __ldg(&S.tris[3 * i + 2]);
+            float3 p = cross3(d, xyz(e2));
+            float det = dot3(xyz(e1), p);
+            if (fabsf(det) < 1e-12f) continue;
+            float id = 1.0f / det;
+            float3 s3 = sub(o, xyz(v0));
+            float u = dot3(s3, p) * id;
+            if (u < 0.0f || u > 1.0f) continue;
+            float3 q = cross3(s3, xyz(e1));
+            float v = dot3(d, q) * id;
+            if (v < 0.0f || u + v > 1.0f) continue;
+            float t = dot3(xyz(e2), q) * id;
+            if (t > 1e-4f && t < hit.t && stops<COUNT>(S, i, v0.w, ray, seed, c)) hit = Hit{t, i, det < 0.0f};
+        }
+    }
+    return hit;
+}
+
 // The same query over the 8-wide BVH: the nearest accepted hit within tmax (any: the first accepted),
 // the same triangle test in the same arithmetic, so every hit, its t and its face are the BVH2 walk's.
 // A node's eight child boxes are tested at once; its leaf slots' triangles first, then its hit inner

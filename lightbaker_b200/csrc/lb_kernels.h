@@ -39,6 +39,7 @@ struct WarpPass {
     int group;                // ray order within an item (passes_warp.cu): top index bits a round shares
     int bvh;                  // 2: the reference's BVH2; 8: the 8-wide BVH (S->nodes8)
     int refill;               // BVH2 occlusion and gather rays: a lane starts the item's next ray when its own ends
+    int near;                 // BVH2 occlusion rays: test a leaf list gathered once an item (lb_device.cuh)
 };
 cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream);
 // The persistent grid's size for a pass: SMs x resident blocks of 256 threads.

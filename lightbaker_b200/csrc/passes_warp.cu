@@ -134,9 +134,11 @@ __device__ __forceinline__ void flush_counts(Count &c, unsigned long long *count
 template <int BVH, bool COUNT>
 __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
-                                                   unsigned long long *counters, int group, int refill) {
+                                                   unsigned long long *counters, int group, int refill, int near) {
     __shared__ float s_term[WARPS][AO_CAP];
     __shared__ uint8_t s_hit[WARPS][AO_CAP];
+    __shared__ uint32_t s_front[WARPS][2][BALL_FRONT];
+    __shared__ uint32_t s_list[WARPS][BALL_LEAVES];
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -212,7 +214,37 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
         uint32_t nback = 0;
         const RayOrder ord(rays, AO_CAP, group, lane);
         const int w = threadIdx.x >> 5;
-        if (BVH == 2 && refill && rays <= AO_CAP) {
+        // the leaves within reach of this texel's occlusion rays, once for all of them
+        int nl = -1;
+        if (BVH == 2 && near && rays <= AO_CAP)
+            nl = ball_leaves<COUNT>(S, o, P.reach[0], nrm, s_front[w][0], s_front[w][1], s_list[w], lane, c);
+        if (nl >= 0) {
+            uint32_t myback = 0;
+            for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
+                uint32_t r = ord.ray(r0 >> 5);
+                if (r < rays) {
+                    float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
+                    Hit h = trace_list<COUNT>(S, s_list[w], nl, o, d, P.reach[0], key + r + 2000u, seed, c);
+                    float term = 0.0f;
+                    bool hit = h.tri != NONE;
+                    if (hit) {
+                        float kk = h.t / P.reach[0];
+                        term = 1.0f - kk * kk;
+                        if (h.back && h.t < P.ground[3]) myback++;
+                    }
+                    s_term[w][r] = term;
+                    s_hit[w][r] = hit;
+                }
+            }
+            for (int ofs = 16; ofs > 0; ofs >>= 1) myback += __shfl_down_sync(FULL, myback, ofs);
+            nback = __shfl_sync(FULL, myback, 0);
+            __syncwarp();
+            for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
+                uint32_t rr = r0 + uint32_t(lane);
+                occ = ordered_add(occ, rr < rays ? s_term[w][rr] : 0.0f, rr < rays && s_hit[w][rr]);
+            }
+            __syncwarp();
+        } else if (BVH == 2 && refill && rays <= AO_CAP) {
             // lane refill: a lane takes the item's next ray as soon as its own has ended
             Walk2<COUNT> wk;
             uint32_t seq = uint32_t(lane), next = 32, r = 0, myback = 0;
@@ -280,7 +312,7 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
             }
             nback += __popc(__ballot_sync(FULL, bk));
         }
-        if (!(BVH == 2 && refill && rays <= AO_CAP) && ord.grouped) {
+        if (nl < 0 && !(BVH == 2 && refill && rays <= AO_CAP) && ord.grouped) {
             __syncwarp();
             for (uint32_t r0 = 0; r0 < rays; r0 += 32) occ = ordered_add(occ, s_term[w][r0 + lane], s_hit[w][r0 + lane]);
             __syncwarp();
@@ -504,7 +536,7 @@ template <int BVH, bool COUNT> void launch(const WarpPass &w, int blocks, cudaSt
     switch (w.pass) {
     case LB_PASS_DIRECT:
         lbd::direct_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base,
-                                                               w.out, w.counters, w.group, w.refill);
+                                                               w.out, w.counters, w.group, w.refill, w.near);
         break;
     case LB_PASS_GATHER:
         lbd::gather_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host,

@@ -283,6 +283,12 @@ int lb_set_pass_kernel(lb_gpu *g, int kind) {
     return LB_OK;
 }
 
+int lb_set_near(lb_gpu *g, int on) {
+    if (!g) return LB_EINVAL;
+    g->near = on != 0;
+    return LB_OK;
+}
+
 int lb_set_refill(lb_gpu *g, int on) {
     if (!g) return LB_EINVAL;
     g->refill = on != 0;
@@ -340,6 +346,7 @@ int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const fl
         w.group = pass == LB_PASS_GATHER ? g->group_gather : g->group_direct;
         w.bvh = g->bvh;
         w.refill = g->refill;
+        w.near = g->near;
         LB_CUDA(lb_launch_pass_warp(w, g->stream), "pass launch");
     } else {
         LB_CUDA(lb_launch_pass_bvh2(pass, S, P, items, n, base, light, n_light, out, g->counters, g->counting,

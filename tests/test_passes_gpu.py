@@ -33,12 +33,14 @@ def _compare(gpu_out, cpu_out, what):
                           f"gpu {gpu_out[bad[:3]]} oracle {cpu_out[bad[:3]]}"
 
 
-@pytest.mark.parametrize("kernel,order,bvh,refill", [(0, 8, 2, 0), (1, 8, 2, 0), (1, 0, 2, 0), (1, 1, 2, 1),
-                                                     (1, 8, 2, 1), (1, 8, 8, 0), (1, 0, 8, 0)],
+@pytest.mark.parametrize("kernel,order,bvh,refill,near",
+                         [(0, 8, 2, 0, 0), (1, 8, 2, 0, 0), (1, 0, 2, 0, 0), (1, 1, 2, 1, 0), (1, 8, 2, 1, 0),
+                          (1, 8, 8, 0, 0), (1, 0, 8, 0, 0), (1, 8, 2, 0, 1), (1, 0, 2, 0, 1)],
                          ids=["thread_per_item", "warp_shader_order", "warp_azimuth_wedges", "warp_patches_refill",
-                              "warp_refill", "warp_bvh8", "warp_bvh8_wedges"])
+                              "warp_refill", "warp_bvh8", "warp_bvh8_wedges", "warp_leaf_lists",
+                              "warp_leaf_lists_wedges"])
 @pytest.mark.parametrize("name,limit", [("reference_test", 20000), ("small_map", 20000), ("map_100m", 3000)])
-def test_passes_bit_exact(gpu, oracle_mod, name, limit, kernel, order, bvh, refill):
+def test_passes_bit_exact(gpu, oracle_mod, name, limit, kernel, order, bvh, refill, near):
     scene = scenes.WORKLOADS[name]()
     P = lb.prepare(scene)
     buffers = gpu.scene(P.nodes, P.tris, P.materials, P.charts)
@@ -52,13 +54,14 @@ def test_passes_bit_exact(gpu, oracle_mod, name, limit, kernel, order, bvh, refi
     gpu.set_ray_order(order, order)
     gpu.set_bvh(bvh)
     gpu.set_refill(refill)
+    gpu.set_near(near)
     gpu.set_counting(True)
     g = gpu.run(lb.Pass.DIRECT, buffers, P.params, items)
     gc = gpu.counters()
     c, cc = oracle_mod.run(0, sc, P.params, items)
     _compare(g, c, f"{name} direct")
     # the BVH2 walks fetch, test and read exactly what the oracle does; the 8-wide walk its own amounts
-    for k in ("rays", "nodes", "tris", "mats") if bvh == 2 else ("rays",):
+    for k in ("rays", "nodes", "tris", "mats") if bvh == 2 and not near else ("rays",):
         assert gc[k] == cc[k], f"direct {k}: gpu {gc[k]} oracle {cc[k]}"
     assert cc["overflows"] == 0
     light = _light_for(P, rng)
@@ -82,7 +85,8 @@ def test_passes_bit_exact(gpu, oracle_mod, name, limit, kernel, order, bvh, refi
     gpu.set_pass_kernel(0)
     gpu.set_ray_order(8, 8)
     gpu.set_bvh(2)
-    gpu.set_refill(1)
+    gpu.set_refill(0)
+    gpu.set_near(1)
 
 
 def test_empty_and_edge_cases(gpu, oracle_mod):
