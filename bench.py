@@ -203,6 +203,11 @@ def kernel_only(args):
     items = (direct if args.kernel_only == "direct" else gather)[: args.items]
     gpu = lb.Gpu.new(0)
     gpu.set_pass_kernel(1)
+    bvh, refill, near, order = (int(x) for x in args.walk.split(","))
+    gpu.set_bvh(bvh)
+    gpu.set_refill(refill)
+    gpu.set_near(near)
+    gpu.set_ray_order(order, order)
     buffers = gpu.scene(P.nodes, P.tris, P.materials, P.charts)
     dev = torch.device("cuda", 0)
     d_items = torch.from_numpy(items.view(np.uint8).reshape(-1)).to(dev)
@@ -223,7 +228,7 @@ def kernel_only(args):
         if i >= args.warmup:
             times.append(e0.elapsed_time(e1))
     rays = gpu.counters()["rays"]
-    print(json.dumps({"kernel": f"{args.kernel_only}_warp", "workload": args.workload, "items": int(len(items)),
+    print(json.dumps({"kernel": f"{args.kernel_only}_warp", "walk": args.walk, "workload": args.workload, "items": int(len(items)),
                       "rays": int(rays), "ms": statistics.median(times), "grays": rays / statistics.median(times) / 1e6}))
     buffers.close()
     gpu.close()
@@ -243,6 +248,7 @@ def main():
                     help="run one warp-per-item pass over --items texels of the workload, warmup + steps times "
                          "(for profiler captures; prints its own line)")
     ap.add_argument("--items", type=int, default=262144)
+    ap.add_argument("--walk", default="2,0,1,8", help="kernel-only: bvh,refill,near,order")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

@@ -300,8 +300,9 @@ struct Walk2 {
 // A warp gathers those leaves once for an item; each of its rays then tests the same short list, a loop
 // its lanes run together, instead of each walking the tree from the root on its own path.
 
-constexpr int BALL_FRONT = 128;   // nodes one level of the ball query holds
 constexpr int BALL_LEAVES = 192;  // leaves an item's list holds (more: the item walks the tree instead)
+// nodes one level of the ball query holds; also the sort's scratch, so at least BALL_LEAVES
+constexpr int BALL_FRONT = BALL_LEAVES;
 
 __device__ __forceinline__ float box_dist2(float3 p, float4 mn, float4 mx) {
     float dx = fmaxf(fmaxf(mn.x - p.x, 0.0f), p.x - mx.x);
