@@ -31,92 +31,52 @@
 #include "lb_kernels.h"
 #include "lb_post.h"
 #include "lb_runtime.h"
+#include "plan.h"
 
-namespace {
+using lbplan::ck;
+using lbplan::DBuf;
+using lbplan::gauss_weights;
+using lbplan::since;
 
-void ck(cudaError_t e, const char *what) {
-    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+PostArgs lb_plan_post_args(lb_plan &p) {
+    const lb::SceneHeader &h = p.scene.header;
+    const lb::BakeSettings &b = h.bake;
+    PostArgs a{};
+    a.tiles = p.tiles_d.as<DTile>();
+    a.n_tiles = int(p.dirty.size());
+    a.n_texels = p.n_dirty_texels;
+    a.tex = p.tex.as<float4>();
+    a.cov_k = p.cov_k.as<uint32_t>();
+    a.direct_out = p.direct_out.as<float4>();
+    a.chart = p.chart.as<uint32_t>();
+    a.valid = p.valid.as<uint8_t>();
+    a.state = p.state.as<uint8_t>();
+    a.known = p.known.as<uint8_t>();
+    a.known_tmp = p.known_tmp.as<uint8_t>();
+    a.gathered = p.gathered.as<uint8_t>();
+    a.hard = p.hard.as<uint32_t>();
+    a.gk = p.gk.as<uint32_t>();
+    a.soft = p.soft.as<float>();
+    a.ao_raw = p.ao_raw.as<float>();
+    a.ao = p.ao.as<float>();
+    a.field = p.field.as<float>();
+    a.dl = p.dl.as<float4>();
+    a.ind = p.ind.as<float4>();
+    a.posg = p.posg.as<float4>();
+    a.light = p.light.as<float4>();
+    a.aw = p.aw;
+    a.w1 = p.w1.as<float>();
+    a.inside_share = b.inside_share;
+    a.ao_strength = b.ao_strength;
+    a.ao_contrast = b.ao_contrast;
+    a.ao_floor = b.ao_floor;
+    a.sdf_radius = b.sdf_radius;
+    a.g = p.P.g;
+    a.ds = p.ds;
+    a.sun = make_float3(p.P.sun.x, p.P.sun.y, p.P.sun.z);
+    a.irr = make_float3(h.sun.irradiance[0], h.sun.irradiance[1], h.sun.irradiance[2]);
+    return a;
 }
-
-// A device allocation freed with the plan.
-struct DBuf {
-    void *p = nullptr;
-    size_t bytes = 0;
-    void alloc(size_t n) {
-        bytes = n ? n : 16;
-        ck(cudaMalloc(&p, bytes), "cudaMalloc");
-    }
-    ~DBuf() {
-        if (p) cudaFree(p);
-    }
-    template <class T> T *as() const { return (T *)p; }
-};
-
-std::vector<float> gauss_weights(int r) {
-    // filter.rs:28-41: exp(-(dx^2 + dy^2) / sigma2), sigma2 = 2 (0.75 r)^2, as the host computes it
-    std::vector<float> w(size_t(2 * r + 1) * (2 * r + 1), 0.0f);
-    if (r == 0) return w;
-    float q = float(r) * 0.75f;
-    float sigma2 = 2.0f * (q * q);
-    for (int dy = -r; dy <= r; dy++)
-        for (int dx = -r; dx <= r; dx++) {
-            float fx = float(dx), fy = float(dy);
-            w[size_t(dy + r) * (2 * r + 1) + (dx + r)] = std::exp(-(fx * fx + fy * fy) / sigma2);
-        }
-    return w;
-}
-
-double since(std::chrono::steady_clock::time_point t) {
-    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
-}
-
-}  // namespace
-
-struct lb_plan {
-    lb_gpu *g = nullptr;
-    lb::Scene scene;
-    lb::Prepared P;
-    lb::Options opt;
-    lb_scene *dscene = nullptr;
-    std::vector<size_t> dirty, order;          // order: dirty tiles, then cached ones
-    std::vector<lb::Hash> hashes;
-    std::vector<std::optional<lb::TileLight>> lights;
-    std::vector<DTile> tiles_all;              // in `order`
-    uint32_t n_dirty_texels = 0, n_all = 0, n_cov = 0;
-    std::vector<uint32_t> cov_counts;          // covered texels per dirty tile
-    // volume
-    bool has_volume = false;
-    std::array<uint32_t, 3> vsize{};
-    uint32_t n_probes = 0, n_todo = 0;
-    std::map<lb::TileKey, std::vector<uint32_t>> chunks;
-    std::vector<std::pair<lb::Hash, std::vector<uint32_t>>> chunk_keys;
-    size_t n_chunks = 0;
-    // device arrays
-    DBuf tiles_d, tex, cov_idx, cov_k, direct_out, chart, valid, state, known, known_tmp, gathered, hard, gk, soft,
-        ao_raw, ao, field, dl, ind, posg, light, w1, wr, gath_idx, gath_count, gather_out, select_temp;
-    DBuf s_ka, s_kb, s_f1, s_f2, s_v4, s_e0, s_e1;
-    DBuf probes, probes_init, probes_b, probe_items, probe_slot, pk_a, pk_b;
-    DBuf owner, direct_atlas, validity, indirect, indirect_b, has, has_b, counters;
-    size_t select_bytes = 0;
-    uint32_t aw = 0, ah = 0, iw = 0, ih = 0, ds = 1;
-    int blocks_direct = 0, blocks_gather = 0, blocks_volume = 0;
-    int kernel_nodes = 0;
-    bool autotune = false;
-    int group_direct = 8, group_gather = 8;  // ray order for the warp passes
-    int bvh_direct = 2, bvh_gather = 2, bvh_volume = 2;  // BVH width for the warp passes
-    int refill_direct = 0, refill_gather = 0;          // lane refill for the warp passes
-    int near_direct = 1;                               // leaf lists for the occlusion rays
-    std::string tuned;  // what the autotuner picked
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    double t_prepare = 0;
-    lb::Stats stats;
-    ~lb_plan() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        if (dscene) lb_scene_free(dscene);
-    }
-};
 
 namespace {
 
@@ -444,40 +404,7 @@ void capture(lb_plan &p) {
     const lb_params &params = p.P.params;
     lb_params pvol = params;
     if (h.volume) pvol.counts[2] = h.volume->rays;
-    PostArgs a{};
-    a.tiles = p.tiles_d.as<DTile>();
-    a.n_tiles = int(p.dirty.size());
-    a.n_texels = p.n_dirty_texels;
-    a.tex = p.tex.as<float4>();
-    a.cov_k = p.cov_k.as<uint32_t>();
-    a.direct_out = p.direct_out.as<float4>();
-    a.chart = p.chart.as<uint32_t>();
-    a.valid = p.valid.as<uint8_t>();
-    a.state = p.state.as<uint8_t>();
-    a.known = p.known.as<uint8_t>();
-    a.known_tmp = p.known_tmp.as<uint8_t>();
-    a.gathered = p.gathered.as<uint8_t>();
-    a.hard = p.hard.as<uint32_t>();
-    a.gk = p.gk.as<uint32_t>();
-    a.soft = p.soft.as<float>();
-    a.ao_raw = p.ao_raw.as<float>();
-    a.ao = p.ao.as<float>();
-    a.field = p.field.as<float>();
-    a.dl = p.dl.as<float4>();
-    a.ind = p.ind.as<float4>();
-    a.posg = p.posg.as<float4>();
-    a.light = p.light.as<float4>();
-    a.aw = p.aw;
-    a.w1 = p.w1.as<float>();
-    a.inside_share = b.inside_share;
-    a.ao_strength = b.ao_strength;
-    a.ao_contrast = b.ao_contrast;
-    a.ao_floor = b.ao_floor;
-    a.sdf_radius = b.sdf_radius;
-    a.g = p.P.g;
-    a.ds = p.ds;
-    a.sun = make_float3(p.P.sun.x, p.P.sun.y, p.P.sun.z);
-    a.irr = make_float3(h.sun.irradiance[0], h.sun.irradiance[1], h.sun.irradiance[2]);
+    PostArgs a = lb_plan_post_args(p);
     PostScratch s{p.s_ka.as<uint8_t>(), p.s_kb.as<uint8_t>(), p.s_f1.as<float>(), p.s_f2.as<float>(),
                   p.s_v4.as<float4>(), p.s_e0.as<float4>(), p.s_e1.as<float4>()};
     unsigned long long *cnt = p.counters.as<unsigned long long>();

@@ -1,0 +1,111 @@
+// The device-resident bake's state (bake_device.cu) and the transport built on it (transport.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <map>
+#include <optional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "host/bake.h"
+#include "host/deps.h"
+#include "lb_post.h"
+#include "lb_runtime.h"
+
+namespace lbplan {
+
+inline void ck(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// A device allocation freed with its owner.
+struct DBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    void alloc(size_t n) {
+        if (p) cudaFree(p);
+        bytes = n ? n : 16;
+        ck(cudaMalloc(&p, bytes), "cudaMalloc");
+    }
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+    template <class T> T *as() const { return (T *)p; }
+};
+
+// filter.rs:28-41: exp(-(dx^2 + dy^2) / sigma2), sigma2 = 2 (0.75 r)^2, as the host computes it
+inline std::vector<float> gauss_weights(int r) {
+    std::vector<float> w(size_t(2 * r + 1) * (2 * r + 1), 0.0f);
+    if (r == 0) return w;
+    float q = float(r) * 0.75f;
+    float sigma2 = 2.0f * (q * q);
+    for (int dy = -r; dy <= r; dy++)
+        for (int dx = -r; dx <= r; dx++) {
+            float fx = float(dx), fy = float(dy);
+            w[size_t(dy + r) * (2 * r + 1) + (dx + r)] = std::exp(-(fx * fx + fy * fy) / sigma2);
+        }
+    return w;
+}
+
+inline double since(std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+}
+
+}  // namespace lbplan
+
+struct lb_plan {
+    lb_gpu *g = nullptr;
+    lb::Scene scene;
+    lb::Prepared P;
+    lb::Options opt;
+    lb_scene *dscene = nullptr;
+    std::vector<size_t> dirty, order;          // order: dirty tiles, then cached ones
+    std::vector<lb::Hash> hashes;
+    std::vector<std::optional<lb::TileLight>> lights;
+    std::vector<DTile> tiles_all;              // in `order`
+    uint32_t n_dirty_texels = 0, n_all = 0, n_cov = 0;
+    std::vector<uint32_t> cov_counts;          // covered texels per dirty tile
+    // volume
+    bool has_volume = false;
+    std::array<uint32_t, 3> vsize{};
+    uint32_t n_probes = 0, n_todo = 0;
+    std::map<lb::TileKey, std::vector<uint32_t>> chunks;
+    std::vector<std::pair<lb::Hash, std::vector<uint32_t>>> chunk_keys;
+    size_t n_chunks = 0;
+    // device arrays
+    lbplan::DBuf tiles_d, tex, cov_idx, cov_k, direct_out, chart, valid, state, known, known_tmp, gathered, hard, gk, soft,
+        ao_raw, ao, field, dl, ind, posg, light, w1, wr, gath_idx, gath_count, gather_out, select_temp;
+    lbplan::DBuf s_ka, s_kb, s_f1, s_f2, s_v4, s_e0, s_e1;
+    lbplan::DBuf probes, probes_init, probes_b, probe_items, probe_slot, pk_a, pk_b;
+    lbplan::DBuf owner, direct_atlas, validity, indirect, indirect_b, has, has_b, counters;
+    size_t select_bytes = 0;
+    uint32_t aw = 0, ah = 0, iw = 0, ih = 0, ds = 1;
+    int blocks_direct = 0, blocks_gather = 0, blocks_volume = 0;
+    int kernel_nodes = 0;
+    bool autotune = false;
+    int group_direct = 8, group_gather = 8;  // ray order for the warp passes
+    int bvh_direct = 2, bvh_gather = 2, bvh_volume = 2;  // BVH width for the warp passes
+    int refill_direct = 0, refill_gather = 0;          // lane refill for the warp passes
+    int near_direct = 1;                               // leaf lists for the occlusion rays
+    std::string tuned;  // what the autotuner picked
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double t_prepare = 0;
+    lb::Stats stats;
+    ~lb_plan() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (dscene) lb_scene_free(dscene);
+    }
+};
+
+
+// The plan's arguments for the texel passes over its dirty tiles.
+PostArgs lb_plan_post_args(lb_plan &p);

@@ -61,6 +61,13 @@ size_t or_item_rays(int pass, const lb_params *params, const lb_texel *item, siz
                     uint32_t pick, float *o, float *d, float *tmax, int *any, uint32_t *key,
                     int *kind, size_t cap);
 
+/* Every gather ray's outcome for items[0..n) (4 words a ray, [item][ray]): kind (0 sky, 1 back face,
+ * 2 surface), material, atlas texel of the hit (0xffffffff: none), bits of the direction's y. */
+int or_gather_records(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+                      const float *materials, size_t n_materials, const float *charts, size_t n_charts,
+                      const lb_params *params, const lb_texel *items, size_t n, size_t n_light,
+                      uint32_t *records, int threads);
+
 /* The shader's own helpers, for unit tests: pcg (trace.wgsl:41-45), rand (:46), radical (:49),
  * the sine and cosine both sides use. */
 uint32_t or_pcg(uint32_t v);

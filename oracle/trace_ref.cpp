@@ -622,6 +622,58 @@ size_t or_item_rays(int pass, const lb_params *P, const lb_texel *item, size_t i
     return k;
 }
 
+// The outcome of every gather ray of every item (trace.wgsl:245-270): kind (0 sky, 1 back face, 2 a
+// surface), for the sky the ray's direction y, for a surface its material and the atlas texel its chart
+// maps the hit to (0xffffffff: none, the fallback). Records are [item][ray], 4 words each:
+// kind, material, atlas index, bits of d.y.
+int or_gather_records(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris, const float *materials,
+                      size_t n_materials, const float *charts, size_t n_charts, const lb_params *P,
+                      const lb_texel *items, size_t n, size_t n_light, uint32_t *rec, int threads) {
+    Ctx base = make_ctx(nodes, n_nodes, tris, n_tris, materials, n_materials, charts, n_charts, P, nullptr, 0);
+    uint32_t rays = P->counts[2];
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (long long k = 0; k < (long long)n; k++) {
+        const Ctx &C = base;
+        const lb_texel &tx = items[k];
+        V3<float> nrm = f3(tx.normal), pos = f3(tx.pos), dx = f3(tx.dx), dy = f3(tx.dy);
+        Frame f = frame(nrm);
+        uint32_t key = uint32_t(k) * 7919u;
+        float s1 = rnd(key, 11u, C.seed), s2 = rnd(key, 13u, C.seed);
+        for (uint32_t r = 0; r < rays; r++) {
+            float jx = rnd(key + r, 19u, C.seed) - 0.5f, jy = rnd(key + r, 23u, C.seed) - 0.5f;
+            V3<float> o = ((pos + dx * jx) + dy * jy) + nrm * C.P->reach[2];
+            V3<float> d = cosine(fract((float(r) + 0.5f) / float(rays) + s1), fract(radical(r) + s2), f);
+            Hit<float> h = trace<float>(C, o, d, C.P->reach[1], false, key + r + 4000u);
+            uint32_t *w = rec + (size_t(k) * rays + r) * 4;
+            w[0] = 0;
+            w[1] = 0;
+            w[2] = NONE;
+            w[3] = fbits(d.y);
+            if (h.tri == NONE) continue;
+            if (h.back) {
+                w[0] = 1;
+                continue;
+            }
+            w[0] = 2;
+            const lb_tri &tr = C.tris[h.tri];
+            w[1] = fbits(tr.v0[3]);
+            uint32_t c = fbits(tr.e1[3]);
+            if (c != NONE && c < C.n_charts) {
+                V3<float> p = o + d * h.t;
+                const float *r0 = C.charts + size_t(c) * 8, *r1 = r0 + 4;
+                float x = r0[0] * p.x + r0[1] * p.y + r0[2] * p.z + r0[3] * 1.0f;
+                float y = r1[0] * p.x + r1[1] * p.y + r1[2] * p.z + r1[3] * 1.0f;
+                int aw = int(C.P->atlas[0]), ah = int(C.P->atlas[1]);
+                int ix = std::min(std::max(int(std::floor(x)), 0), aw - 1);
+                int iy = std::min(std::max(int(std::floor(y)), 0), ah - 1);
+                size_t li = size_t(uint32_t(iy)) * C.P->atlas[0] + uint32_t(ix);
+                if (li < n_light) w[2] = uint32_t(li);
+            }
+        }
+    }
+    return LB_OK;
+}
+
 uint32_t or_pcg(uint32_t v) { return pcg(v); }
 float or_rand(uint32_t a, uint32_t b, uint32_t seed_bits) { return rnd(a, b, seed_bits); }
 float or_radical(uint32_t i) { return radical(i); }
