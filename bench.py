@@ -244,6 +244,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--kernel-only", choices=["direct", "gather"], default=None,
                     help="run one warp-per-item pass over --items texels of the workload, warmup + steps times "
                          "(for profiler captures; prints its own line)")
@@ -387,6 +388,74 @@ def main():
                               "volume": st.t_volume}}
         pb.close()
 
+    # ---- the bounce transport and its adjoint: gradients of the indirect atlas wrt albedos, sky, sun ----
+    adjoint = None
+    if not args.no_adjoint:
+        def timed(fn, reps):
+            out_ms = []
+            for i in range(reps + 1):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with torch.cuda.stream(stream):
+                    flush.fill_(1)
+                    e0.record(stream)
+                fn()
+                with torch.cuda.stream(stream):
+                    e1.record(stream)
+                gpu.sync()
+                if i > 0:
+                    out_ms.append(e0.elapsed_time(e1))
+            return statistics.median(out_ms)
+
+        t0 = time.perf_counter()
+        tr = lb.Transport(scene, gpu)
+        create_s = time.perf_counter() - t0
+        th = torch.from_numpy(tr.theta0()).to(dev)
+        out_t = torch.empty((tr.ih, tr.iw, 4), dtype=torch.float32, device=dev)
+        g_in = torch.rand((tr.ih, tr.iw, 4), dtype=torch.float32, device=dev)
+        g_th = torch.empty(tr.n_params, dtype=torch.float32, device=dev)
+        torch.cuda.synchronize()
+        reps = max(3, args.steps)
+        fwd_ms = timed(lambda: tr.forward_async(th.data_ptr(), out_t.data_ptr()), reps)
+        bwd_ms = timed(lambda: tr.backward_async(g_in.data_ptr(), g_th.data_ptr()), reps)
+        shape = tr.shape
+        # the L2 loss against a target baked at theta0 + N(0, 0.05), its gradient at theta0, and central
+        # differences (h = 1e-3) of the loss on a few parameters: albedos, the sky's colours, the sun
+        rng = np.random.default_rng(100 + rank)
+        theta0 = tr.theta0()
+        target = tr.forward(theta0 + rng.normal(0.0, 0.05, theta0.shape).astype(np.float32)).astype(np.float64)
+
+        def loss(t):
+            return float(((tr.forward(t).astype(np.float64) - target) ** 2).sum())
+        y0 = tr.forward(theta0)
+        grad = tr.backward(2.0 * (y0.astype(np.float64) - target))
+        M = tr.n_materials
+        h = 1e-3
+        checks = []
+        for j in sorted({0, 1, 2, 3 * (M // 2) + 1, 3 * (M - 1) + 2, 3 * M, 3 * M + 4, 3 * M + 8, 3 * M + 9}):
+            tp, tm = theta0.copy(), theta0.copy()
+            tp[j] += h
+            tm[j] -= h
+            fd = (loss(tp) - loss(tm)) / (2 * h)
+            checks.append({"param": j, "adjoint": float(grad[j]), "central_difference": fd,
+                           "rel_err": abs(fd - grad[j]) / max(abs(grad[j]), 1e-30)})
+        tr.close()
+        one = lb.Transport(scene, gpu, max_checkpoints=1)
+        one.forward_async(th.data_ptr(), out_t.data_ptr())
+        bwd1_ms = timed(lambda: one.backward_async(g_in.data_ptr(), g_th.data_ptr()), reps)
+        one_bytes = one.shape.checkpoint_bytes
+        one.close()
+        adjoint = {"forward_ms": max_over_ranks(fwd_ms), "backward_ms": max_over_ranks(bwd_ms),
+                   "backward_over_forward": bwd_ms / fwd_ms, "create_s": create_s,
+                   "backward_ms_one_checkpoint": max_over_ranks(bwd1_ms),
+                   "checkpoint_bytes": {"every_bounce": int(shape.checkpoint_bytes), "one": int(one_bytes)},
+                   "bounces": int(shape.bounces), "params": int(shape.n_params), "records": int(shape.records),
+                   "lit_records": int(shape.lit_records),
+                   "gradient_check": {"loss": "L2 to a target baked at theta0 + N(0, 0.05)", "h": h,
+                                      "max_rel_err": max(c["rel_err"] for c in checks), "params": checks},
+                   "note": "device time of one forward (theta on the device to the indirect atlas) and one "
+                           "backward (atlas gradient to theta's gradient), CUDA graphs, L2 flushed before each"}
+        del th, out_t, g_in, g_th
+
     if rank == 0:
         peaks = {}
         try:
@@ -434,6 +503,7 @@ def main():
                     "d2h_bytes_per_step": d2h // max(1, args.e2e_steps), "bake_seconds": e2e_t / 1e3,
                     "host_prepare_s": e2e_stats.t_layout},
             "plain": plain,
+            "adjoint": adjoint,
             "batched_vs_plain": (value / plain["grays_passes"]) if plain else None,
             "gpu_launches": kernels * args.steps,
             "clocks": clock_info,

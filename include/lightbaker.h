@@ -267,6 +267,47 @@ int lb_plan_kernels(const lb_plan *plan);
 const char *lb_plan_tuning(const lb_plan *plan);
 void lb_plan_free(lb_plan *plan);
 
+/* The bounce transport and its adjoint: the bake's indirect atlas as a function of the scene's light
+ * parameters theta, and the gradient of a loss on that atlas with respect to theta. No reference
+ * counterpart: the reference bakes at the scene's own values only (bake.rs:300-421 is the function
+ * differentiated here).
+ *
+ * theta (3 * n_materials + 10 floats): every material's albedo (rgb, scene.rs:62-75), the sky's zenith,
+ * horizon and ground (rgb each, scene.rs:53-60), and the sun's intensity as a scale on its irradiance
+ * (1 = the scene's own). lb_transport_theta0 gives the scene's own theta; forward at it gives the
+ * device bake's indirect atlas bit for bit. Visibility does not depend on theta: create traces every
+ * gather ray once and records what it met. Texels lit by the volume's fallback (validity 5) keep their
+ * light at the scene's own theta.
+ *
+ * create bakes the scene once on the device (every tile, no cache) and keeps what the transport reads;
+ * max_checkpoints bounds the light atlases the forward keeps for the backward (0: one a bounce); with
+ * fewer than the bounces, backward recomputes the others from the nearest earlier one, and its result
+ * is the same bits. forward / backward take and give host arrays and wait; the _async forms take device
+ * pointers and only enqueue on the gpu handle's stream. backward differentiates the last forward: its
+ * input is d(loss)/d(indirect) (indirect_width x indirect_height float4, w ignored), its output
+ * d(loss)/d(theta). Gradients are deterministic (fixed-order sums, in double for theta). */
+typedef struct lb_transport lb_transport;
+typedef struct lb_transport_shape {
+    uint32_t n_materials, n_params, bounces, checkpoints;
+    uint32_t indirect_width, indirect_height, gathered, rays;
+    uint64_t records, lit_records, unlit_records, checkpoint_bytes;
+} lb_transport_shape;
+lb_transport *lb_transport_create(lb_gpu *gpu, const uint8_t *scene, size_t len, uint32_t max_checkpoints);
+int lb_transport_info(const lb_transport *t, lb_transport_shape *out);
+int lb_transport_theta0(const lb_transport *t, float *theta);
+int lb_transport_forward(lb_transport *t, const float *theta, float *indirect);
+int lb_transport_backward(lb_transport *t, const float *g_indirect, float *g_theta);
+int lb_transport_forward_async(lb_transport *t, const float *d_theta, float *d_indirect);
+int lb_transport_backward_async(lb_transport *t, const float *d_g_indirect, float *d_g_theta);
+/* The indirect atlas of the bake create ran (float4 a texel). */
+int lb_transport_bake_indirect(lb_transport *t, float *indirect);
+/* A copy of one of the transport's fixed arrays, for tests ("records", "gathered_index", "texels", "sample_points",
+ * "chart", "gathered", "known", "known_bounce", "state", "direct_light", "fixed_indirect", "owner",
+ * "light_flags", "tiles", "smooth_weights", "shape"): its size in bytes when out is NULL, else the
+ * bytes copied (0 on error). */
+size_t lb_transport_export(lb_transport *t, const char *name, void *out, size_t cap);
+void lb_transport_free(lb_transport *t);
+
 /* Scene::write (scene.rs:164-181) from a JSON header and positions: for tools and tests that make
  * scenes. header_json is the header as the file holds it. */
 int lb_scene_encode(const char *header_json, const float *const *positions, const size_t *n_floats,

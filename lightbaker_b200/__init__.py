@@ -25,7 +25,8 @@ from . import _native as N
 from ._native import NODE, TEXEL, TRI, LightbakerError, Params
 
 __all__ = ["Pass", "Gpu", "SceneBuffers", "Prepared", "prepare", "bake", "Bake", "encode_scene", "blake3",
-           "rgb9e5", "rgb9e5_decode", "bc4_block", "Params", "NODE", "TRI", "TEXEL", "LightbakerError"]
+           "rgb9e5", "rgb9e5_decode", "bc4_block", "Params", "NODE", "TRI", "TEXEL", "LightbakerError", "Transport",
+           "transport"]
 
 
 class Pass(enum.IntEnum):
@@ -420,3 +421,6 @@ def bc4_block(v) -> bytes:
     out = np.zeros(8, np.uint8)
     N.lib().lb_bc4_block(N.ptr(a), N.ptr(out))
     return out.tobytes()
+
+
+from .transport import Transport, transport  # noqa: E402

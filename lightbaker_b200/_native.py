@@ -57,6 +57,13 @@ class BakeInfo(C.Structure):
                 ("n_triangles", C.c_uint64)]
 
 
+class TransportShape(C.Structure):
+    _fields_ = [("n_materials", C.c_uint32), ("n_params", C.c_uint32), ("bounces", C.c_uint32),
+                ("checkpoints", C.c_uint32), ("indirect_width", C.c_uint32), ("indirect_height", C.c_uint32),
+                ("gathered", C.c_uint32), ("rays", C.c_uint32), ("records", C.c_uint64), ("lit_records", C.c_uint64),
+                ("unlit_records", C.c_uint64), ("checkpoint_bytes", C.c_uint64)]
+
+
 SCENE_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                        C.c_size_t, C.c_void_p, C.c_size_t)
 RUN_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(Params), C.c_void_p, C.c_size_t, C.c_void_p,
@@ -120,6 +127,16 @@ SIGNATURES = {
     "lb_plan_free": (None, [C.c_void_p]),
     "lb_plan_kernels": (C.c_int, [C.c_void_p]),
     "lb_plan_tuning": (C.c_char_p, [C.c_void_p]),
+    "lb_transport_create": (C.c_void_p, [C.c_void_p, C.c_char_p, C.c_size_t, C.c_uint32]),
+    "lb_transport_info": (C.c_int, [C.c_void_p, C.POINTER(TransportShape)]),
+    "lb_transport_theta0": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "lb_transport_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "lb_transport_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "lb_transport_forward_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "lb_transport_backward_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "lb_transport_bake_indirect": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "lb_transport_export": (C.c_size_t, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]),
+    "lb_transport_free": (None, [C.c_void_p]),
     "lb_bake_get_info": (C.c_int, [C.c_void_p, C.POINTER(BakeInfo)]),
     "lb_bake_get_direct": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lb_bake_get_indirect": (C.c_int, [C.c_void_p, C.c_void_p]),

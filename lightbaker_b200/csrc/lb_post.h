@@ -53,6 +53,10 @@ cudaError_t lb_post_direct(const PostArgs &a, int rings, PostScratch &s, cudaStr
 size_t lb_select_temp_bytes(uint32_t n);
 cudaError_t lb_select_gathered(const PostArgs &a, void *temp, size_t temp_bytes, uint32_t *idx, uint32_t *count,
                                cudaStream_t st);
+// The bounce's texel work before the atlas write (bake.rs:309-323): the gather results scattered into their
+// texels, smoothed and filled; *out is whichever of e0, e1 holds the filled light.
+cudaError_t lb_bounce_filters(const PostArgs &a, const float4 *res, int r, const float *w, int rings, uint8_t *ka,
+                              uint8_t *kb, float4 *e0, float4 *e1, float4 **out, cudaStream_t st);
 cudaError_t lb_post_bounce(const PostArgs &a, const float4 *res, int r, const float *w, int rings, PostScratch &s,
                            cudaStream_t st);
 cudaError_t lb_volume_fill(float4 *probes, float4 *scratch, uint8_t *ka, uint8_t *kb, uint32_t nx, uint32_t ny,
@@ -60,3 +64,5 @@ cudaError_t lb_volume_fill(float4 *probes, float4 *scratch, uint8_t *ka, uint8_t
 cudaError_t lb_fallback(const PostArgs &a, const float4 *probes, float3 origin, float step, uint32_t nx, uint32_t ny,
                         uint32_t nz, cudaStream_t st);
 cudaError_t lb_composite(const CompositeArgs &c, float4 *scratch, uint8_t *has_b, cudaStream_t st);
+// the composite's block averages alone, before its dilations
+cudaError_t lb_composite_blocks(const CompositeArgs &c, cudaStream_t st);

@@ -10,25 +10,9 @@
 
 #include "lb_device.cuh"
 #include "lb_post.h"
+#include "lb_texel.cuh"
 
 namespace lbd {
-
-__device__ __forceinline__ int find_tile(const DTile *tiles, int n, uint32_t i) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (tiles[mid].off <= i) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
-// filter.rs:13-18
-__device__ __forceinline__ bool same(const uint32_t *chart, const float4 *tex, uint32_t i, uint32_t j) {
-    if (chart[i] != chart[j]) return false;
-    float4 a = tex[4 * i + 1], b = tex[4 * j + 1];
-    return a.x * b.x + a.y * b.y + a.z * b.z >= 0.9f;
-}
 
 // bake.rs:207-241: each covered texel's direct record unpacked; texels inside solids lose their own
 // light; the AO curve; the sample point moved where the pass sampled off the centre.
@@ -509,22 +493,33 @@ cudaError_t lb_select_gathered(const PostArgs &a, void *temp, size_t temp_bytes,
     return cudaGetLastError();
 }
 
-cudaError_t lb_post_bounce(const PostArgs &a, const float4 *res, int r, const float *w, int rings, PostScratch &s,
-                           cudaStream_t st) {
+cudaError_t lb_bounce_filters(const PostArgs &a, const float4 *res, int r, const float *w, int rings, uint8_t *ka,
+                              uint8_t *kb, float4 *e0, float4 *e1, float4 **out, cudaStream_t st) {
+    *out = e1;
     if (a.n_texels == 0) return cudaSuccess;
     dim3 g = grid_for(a.n_texels);
-    lbd::k_scatter<<<g, 256, 0, st>>>(a, res, s.e0);
-    lbd::k_smooth3<<<g, 256, 0, st>>>(a, s.e0, s.e1, r, w);
-    cudaError_t e = cudaMemcpyAsync(s.known_a, a.gathered, a.n_texels, cudaMemcpyDeviceToDevice, st);
+    lbd::k_scatter<<<g, 256, 0, st>>>(a, res, e0);
+    lbd::k_smooth3<<<g, 256, 0, st>>>(a, e0, e1, r, w);
+    cudaError_t e = cudaMemcpyAsync(ka, a.gathered, a.n_texels, cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return e;
-    uint8_t *kw = s.known_a, *kn = s.known_b;
-    float4 *vw = s.e1, *vn = s.e0;
+    uint8_t *kw = ka, *kn = kb;
+    float4 *vw = e1, *vn = e0;
     for (int q = 0; q < rings; q++) {
         lbd::k_fill3<<<g, 256, 0, st>>>(a, kw, kn, vw, vn);
         std::swap(kw, kn);
         std::swap(vw, vn);
     }
-    lbd::k_bounce_final<<<g, 256, 0, st>>>(a, vw);
+    *out = vw;
+    return cudaGetLastError();
+}
+
+cudaError_t lb_post_bounce(const PostArgs &a, const float4 *res, int r, const float *w, int rings, PostScratch &s,
+                           cudaStream_t st) {
+    if (a.n_texels == 0) return cudaSuccess;
+    float4 *filled = nullptr;
+    cudaError_t e = lb_bounce_filters(a, res, r, w, rings, s.known_a, s.known_b, s.e0, s.e1, &filled, st);
+    if (e != cudaSuccess) return e;
+    lbd::k_bounce_final<<<grid_for(a.n_texels), 256, 0, st>>>(a, filled);
     return cudaGetLastError();
 }
 
@@ -549,6 +544,13 @@ cudaError_t lb_fallback(const PostArgs &a, const float4 *probes, float3 origin, 
                         uint32_t nz, cudaStream_t st) {
     if (a.n_texels == 0) return cudaSuccess;
     lbd::k_fallback<<<grid_for(a.n_texels), 256, 0, st>>>(a, probes, origin, step, nx, ny, nz);
+    return cudaGetLastError();
+}
+
+cudaError_t lb_composite_blocks(const CompositeArgs &c, cudaStream_t st) {
+    uint32_t n = c.iw * c.ih;
+    if (n == 0) return cudaSuccess;
+    lbd::k_composite<<<grid_for(n), 256, 0, st>>>(c);
     return cudaGetLastError();
 }
 

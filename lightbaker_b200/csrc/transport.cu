@@ -1,0 +1,1118 @@
+// The bounce transport of a bake, and its adjoint.
+//
+// The bake's indirect light is a function of the scene's light parameters theta: every material's albedo,
+// the sky's zenith, horizon and ground colours, and the sun's intensity (a scale s on its irradiance).
+// Nothing else in the bake depends on them: visibility, the texel layout, the gather selection and every
+// filter's weights are fixed by the geometry. So the transport records once what each gather ray met
+// (trace.wgsl:245-270; the rays are the same in every bounce, their keys depend on the gathered texel's
+// index and not on the bounce) and runs the bounces of bake.rs:300-329 as
+//
+//   light_0      = write_light(s * dl0)                           bake.rs:268-275 with write_light :434-444
+//   res_b        = eval(records, light_b, theta)                  trace.wgsl:258-269, bounced :133-148
+//   e_b          = fill(smooth(scatter(res_b)))                   bake.rs:309-323
+//   light_{b+1}  = write_light(s * dl0 + e_b)                     bake.rs:324-328
+//   indirect     = dilate(dilate(composite(e_{B-1} | fallback)))  bake.rs:364-421
+//
+// where dl0 is the direct light at the scene's irradiance (linear in it: bake.rs:247-252 and the fills).
+// At theta0 (the scene's own values) every step is the device bake's own kernel on the same inputs, so
+// the result is the bake's indirect atlas bit for bit. Texels that take the volume's fallback
+// (bake.rs:335-359, validity 5) keep their theta0 light: the volume pass is not part of the transport.
+//
+// The adjoint runs the steps transposed, the last bounce first. Every sum runs in a fixed order (no
+// floating-point atomics; theta's sums in double), so a gradient is the same bits call after call and
+// whatever the checkpointing. The forward keeps each bounce's light atlas when the checkpoint budget
+// allows; with fewer checkpoints than bounces the backward recomputes the missing atlases from the
+// nearest earlier checkpoint.
+#include <cub/device/device_radix_sort.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "../../include/lightbaker.h"
+#include "lb_device.cuh"
+#include "lb_post.h"
+#include "lb_texel.cuh"
+#include "plan.h"
+
+using lbplan::ck;
+using lbplan::DBuf;
+
+namespace lbd {
+
+// theta: albedo (3 a material), zenith, horizon, ground (3 each), the sun's scale
+struct Theta {
+    const float *t;
+    uint32_t M;
+    __device__ __forceinline__ float3 albedo(uint32_t m) const { return mk(t[3 * m], t[3 * m + 1], t[3 * m + 2]); }
+    __device__ __forceinline__ float3 zenith() const { return mk(t[3 * M], t[3 * M + 1], t[3 * M + 2]); }
+    __device__ __forceinline__ float3 horizon() const { return mk(t[3 * M + 3], t[3 * M + 4], t[3 * M + 5]); }
+    __device__ __forceinline__ float3 ground() const { return mk(t[3 * M + 6], t[3 * M + 7], t[3 * M + 8]); }
+    __device__ __forceinline__ float sun() const { return t[3 * M + 9]; }
+    // the fallback light, as the host derives it from the sky (bake.rs:150-152)
+    __device__ __forceinline__ float3 fallback() const {
+        float3 z = zenith(), h = horizon();
+        return mk(((z.x + h.x) * 0.5f) * PI, ((z.y + h.y) * 0.5f) * PI, ((z.z + h.z) * 0.5f) * PI);
+    }
+};
+
+constexpr uint32_t KIND_SKY = 0u, KIND_BACK = 1u, KIND_SURFACE = 2u;
+constexpr uint32_t LIT_NONE = 0xffffffffu, UNLIT = 0xfffffffeu;
+
+// A gather ray's outcome: x = kind << 30 | material; y = the direction's y (sky, as bits) or the atlas
+// texel the hit reads (surface; 0xffffffff when it reads none and takes the fallback).
+__device__ __forceinline__ uint2 gather_record(const Scene &S, const lb_params &P, uint32_t n_light, float3 o,
+                                               float3 d, const Hit &h) {
+    if (h.tri == NONE) return make_uint2(KIND_SKY << 30, __float_as_uint(d.y));
+    if (h.back) return make_uint2(KIND_BACK << 30, 0u);
+    float4 v0 = __ldg(&S.tris[3 * h.tri]), e1 = __ldg(&S.tris[3 * h.tri + 1]);
+    uint32_t m = __float_as_uint(v0.w), ch = __float_as_uint(e1.w), li = NONE;
+    // bounced (trace.wgsl:133-148): the chart's atlas texel under the hit point
+    if (ch != NONE && ch < S.n_charts) {
+        float3 p = add(o, scl(d, h.t));
+        float4 r0 = __ldg(&S.charts[2 * ch]), r1 = __ldg(&S.charts[2 * ch + 1]);
+        float x = r0.x * p.x + r0.y * p.y + r0.z * p.z + r0.w * 1.0f;
+        float y = r1.x * p.x + r1.y * p.y + r1.z * p.z + r1.w * 1.0f;
+        int ix = min(max(int(floorf(x)), 0), int(P.atlas[0]) - 1);
+        int iy = min(max(int(floorf(y)), 0), int(P.atlas[1]) - 1);
+        uint32_t l = uint32_t(iy) * P.atlas[0] + uint32_t(ix);
+        if (l < n_light) li = l;
+    }
+    return make_uint2((KIND_SURFACE << 30) | min(m, 0x3fffffffu), li);
+}
+
+// The gather pass's rays (trace.wgsl:245-270) for the gathered texels, each ray's outcome recorded
+// ([item][ray]); a thread a ray.
+__global__ void k_records(Scene S, lb_params P, const float4 *tex, const uint32_t *idx, const float4 *posg,
+                          uint32_t n, uint32_t n_light, uint2 *rec) {
+    uint32_t rays = P.counts[2];
+    uint64_t total = uint64_t(n) * rays;
+    uint32_t seed = __float_as_uint(P.reach[3]);
+    Count c;
+    c.zero();
+    float frays = __uint2float_rn(rays);
+    for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total;
+         g += uint64_t(gridDim.x) * blockDim.x) {
+        uint32_t k = uint32_t(g / rays), r = uint32_t(g % rays);
+        uint32_t t = idx[k];
+        float4 p4 = posg[t], n4 = __ldg(&tex[4 * t + 1]), dx4 = __ldg(&tex[4 * t + 2]), dy4 = __ldg(&tex[4 * t + 3]);
+        float3 nrm = xyz(n4), pos = xyz(p4), dx = xyz(dx4), dy = xyz(dy4);
+        Frame f = frame(nrm);
+        uint32_t key = k * 7919u;
+        float s1 = rnd(key, 11u, seed), s2 = rnd(key, 13u, seed);
+        float jx = rnd(key + r, 19u, seed) - 0.5f, jy = rnd(key + r, 23u, seed) - 0.5f;
+        float3 o = add(add(add(pos, scl(dx, jx)), scl(dy, jy)), scl(nrm, P.reach[2]));
+        float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
+        Hit h = trace<false>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c);
+        rec[g] = gather_record(S, P, n_light, o, d, h);
+    }
+}
+
+// The records against the light and theta: each gathered texel's gather result, its terms summed in ray
+// order as the gather pass sums them (trace.wgsl:258-269); a warp an item.
+__global__ void k_eval(const uint2 *rec, uint32_t n, uint32_t rays, const float4 *light, uint32_t n_light, Theta th,
+                       float4 *out) {
+    const int lane = threadIdx.x & 31;
+    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+    float frays = __uint2float_rn(rays);
+    float3 zen = th.zenith(), hor = th.horizon(), gro = th.ground(), fb = th.fallback();
+    for (uint32_t k = warp; k < n; k += warps) {
+        float3 sum = mk(0.f, 0.f, 0.f);
+        uint32_t nback = 0;
+        for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
+            uint32_t r = r0 + uint32_t(lane);
+            float3 term = mk(0.f, 0.f, 0.f);
+            bool on = false, bk = false;
+            if (r < rays) {
+                uint2 q = rec[size_t(k) * rays + r];
+                uint32_t kind = q.x >> 30;
+                if (kind == KIND_SKY) {
+                    // trace.wgsl:63-66
+                    float y = __uint_as_float(q.y);
+                    term = y < 0.0f ? gro : add(scl(hor, 1.0f - y), scl(zen, y));
+                    on = true;
+                } else if (kind == KIND_BACK) {
+                    bk = true;
+                } else {
+                    uint32_t m = q.x & 0x3fffffffu;
+                    float3 al = m < th.M ? th.albedo(m) : mk(0.f, 0.f, 0.f);
+                    float3 e = fb;
+                    if (q.y < n_light) {
+                        float4 l = light[q.y];
+                        if (l.w > 0.5f) e = mk(l.x, l.y, l.z);
+                    }
+                    term = mulv(mk(al.x / PI, al.y / PI, al.z / PI), e);
+                    on = true;
+                }
+            }
+            unsigned mask = __ballot_sync(0xffffffffu, on);
+#pragma unroll 1
+            for (int l = 0; l < 32; l++) {
+                float x = __shfl_sync(0xffffffffu, term.x, l), y = __shfl_sync(0xffffffffu, term.y, l),
+                      z = __shfl_sync(0xffffffffu, term.z, l);
+                if (mask & (1u << l)) sum = add(sum, mk(x, y, z));
+            }
+            nback += __popc(__ballot_sync(0xffffffffu, bk));
+        }
+        if (lane == 0) {
+            float3 e = scl(sum, PI);
+            out[k] = make_float4(e.x / frays, e.y / frays, e.z / frays, __uint2float_rn(nback) / frays);
+        }
+    }
+}
+
+// write_light (bake.rs:434-444) with the direct light scaled by the sun's theta: the atlas holds a known
+// texel's direct plus (after the first bounce) indirect light
+__global__ void k_write_light(PostArgs a, const uint8_t *kb, const float4 *dl0, Theta th, const float4 *ind,
+                              float4 *light) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_texels) return;
+    const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, i)];
+    uint32_t li = i - t.off, x = li % t.w, y = li / t.w;
+    float s = th.sun();
+    float4 d0 = dl0[i];
+    float4 d = make_float4(s * d0.x, s * d0.y, s * d0.z, 0.f);
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (kb[i] >= 1) {
+        if (ind) {
+            float4 e = ind[i];
+            v = make_float4(d.x + e.x, d.y + e.y, d.z + e.z, 1.0f);
+        } else {
+            v = make_float4(d.x, d.y, d.z, 1.0f);
+        }
+    }
+    light[size_t(t.y + y) * a.aw + t.x + x] = v;
+}
+
+// the last bounce's light as the texels' indirect, the fallback texels' own kept
+__global__ void k_final_ind(uint32_t n, const uint8_t *state, const float4 *e, const float4 *fixed_ind, float4 *ind) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ind[i] = state[i] == 5 ? fixed_ind[i] : e ? e[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// known during the bounces: the final flags less the fallback's
+__global__ void k_known_bounce(uint32_t n, const uint8_t *known, const uint8_t *state, uint8_t *kb) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) kb[i] = state[i] == 5 ? 0 : known[i];
+}
+
+// ---- the records' order for the adjoint ----
+
+// sort keys: a lit surface record by its atlas texel; one that takes the fallback, or sky, after them; back
+// faces and unknown materials (no term) last
+__global__ void k_record_keys(const uint2 *rec, uint64_t n_rec, const float4 *light, uint32_t n_light, uint32_t M,
+                              uint32_t *keys, uint32_t *vals) {
+    for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n_rec; r += uint64_t(gridDim.x) * blockDim.x) {
+        uint2 q = rec[r];
+        uint32_t kind = q.x >> 30, key = LIT_NONE;
+        if (kind == KIND_SKY) key = UNLIT;
+        else if (kind == KIND_SURFACE && (q.x & 0x3fffffffu) < M)
+            key = (q.y < n_light && light[q.y].w > 0.5f) ? q.y : UNLIT;
+        keys[r] = key;
+        vals[r] = uint32_t(r);
+    }
+}
+
+// the sorted records: x = kind << 30 | item, y = material (surface) or the direction's y (sky)
+__global__ void k_record_sorted(const uint2 *rec, const uint32_t *vals, uint64_t n, uint32_t rays, uint2 *sorted) {
+    for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += uint64_t(gridDim.x) * blockDim.x) {
+        uint32_t r = vals[q];
+        uint2 v = rec[r];
+        uint32_t kind = v.x >> 30;
+        sorted[q] = make_uint2((kind << 30) | (r / rays), kind == KIND_SKY ? v.y : (v.x & 0x3fffffffu));
+    }
+}
+
+// offs[l] = the first sorted record whose key is >= l, for l = 0..n_light, then the first UNLIT and the
+// first LIT_NONE key
+__global__ void k_record_offsets(const uint32_t *keys, uint64_t n, uint32_t n_light, uint64_t *offs) {
+    uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l > n_light + 2) return;
+    uint32_t want = l <= n_light ? l : l == n_light + 1 ? UNLIT : LIT_NONE;
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint64_t mid = (lo + hi) >> 1;
+        if (keys[mid] < want) lo = mid + 1;
+        else hi = mid;
+    }
+    offs[l] = lo;
+}
+
+// ---- transposes: a thread writes its own texel's gradient, summing what it fed in a fixed order ----
+
+// the composite's block average (bake.rs:364-391): a texel's share of its block's gradient; the fallback
+// texels' light is fixed
+__global__ void k_composite_t(PostArgs a, CompositeArgs c, const float4 *g_blocks, float4 *g_ind) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_texels) return;
+    float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c.known[i] != 0 && c.state[i] != 5) {
+        const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, i)];
+        uint32_t li = i - t.off, ax = t.x + li % t.w, ay = t.y + li / t.w;
+        uint32_t bx = ax / c.ds, by = ay / c.ds;
+        float s3 = 0.0f;
+        for (uint32_t y = by * c.ds; y < min((by + 1) * c.ds, c.ah); y++)
+            for (uint32_t x = bx * c.ds; x < min((bx + 1) * c.ds, c.aw); x++) {
+                uint32_t j = c.owner[size_t(y) * c.aw + x];
+                if (j != NONE && c.known[j] != 0) s3 += c.known[j] == 2 ? 1.0f : 1e-3f;
+            }
+        float k = c.known[i] == 2 ? 1.0f : 1e-3f;
+        float4 gb = g_blocks[by * c.iw + bx];
+        g = make_float4(gb.x * k / s3, gb.y * k / s3, gb.z * k / s3, 0.f);
+    }
+    g_ind[i] = g;
+}
+
+__device__ __forceinline__ int flagged_around(const uint8_t *was, uint32_t i, uint32_t iw, uint32_t ih) {
+    uint32_t x = i % iw, y = i / iw;
+    int n = 0;
+    for (uint32_t yy = y > 0 ? y - 1 : 0; yy < min(y + 2, ih); yy++)
+        for (uint32_t xx = x > 0 ? x - 1 : 0; xx < min(x + 2, iw); xx++) n += was[yy * iw + xx] ? 1 : 0;
+    return n;
+}
+
+// one dilation pass (bake.rs:394-421) transposed
+__global__ void k_dilate_t(const uint8_t *was, const float4 *g_out, float4 *g_in, uint32_t iw, uint32_t ih) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= iw * ih) return;
+    float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (was[j]) {
+        g = g_out[j];
+        uint32_t x = j % iw, y = j / iw;
+        for (uint32_t yy = y > 0 ? y - 1 : 0; yy < min(y + 2, ih); yy++)
+            for (uint32_t xx = x > 0 ? x - 1 : 0; xx < min(x + 2, iw); xx++) {
+                uint32_t i = yy * iw + xx;
+                if (was[i]) continue;
+                float f = float(flagged_around(was, i, iw, ih));
+                float4 go = g_out[i];
+                g.x += go.x / f, g.y += go.y / f, g.z += go.z / f;
+            }
+    } else if (flagged_around(was, j, iw, ih) == 0) {
+        g = g_out[j];
+    }
+    g_in[j] = g;
+}
+
+// the dilation's flags alone
+__global__ void k_dilate_mask(const uint8_t *was, uint8_t *now, uint32_t iw, uint32_t ih) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= iw * ih) return;
+    now[i] = was[i] || flagged_around(was, i, iw, ih) > 0;
+}
+
+// How a texel not yet filled fills in one ring (filter.rs:58-94): 1 from its own chart's flagged
+// neighbours, 2 from any flagged neighbour (a texel of no chart), 0 not; n the neighbours averaged.
+__device__ __forceinline__ int fill_mode(const PostArgs &a, const DTile &t, const uint8_t *was, uint32_t i, int x, int y,
+                                         int &n) {
+    uint32_t ci = a.chart[i];
+    int no = 0, na = 0;
+    for (int yy = y > 0 ? y - 1 : 0; yy < min(y + 2, int(t.h)); yy++)
+        for (int xx = x > 0 ? x - 1 : 0; xx < min(x + 2, int(t.w)); xx++) {
+            uint32_t q = t.off + uint32_t(yy) * t.w + uint32_t(xx);
+            if (!was[q]) continue;
+            if (ci != NONE && a.chart[q] == ci) no++;
+            else na++;
+        }
+    if (no > 0) {
+        n = no;
+        return 1;
+    }
+    if (na > 0 && ci == NONE) {
+        n = na;
+        return 2;
+    }
+    n = 0;
+    return 0;
+}
+
+// one fill ring's flags alone
+__global__ void k_fill_mask(PostArgs a, const uint8_t *was, uint8_t *now) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_texels) return;
+    uint8_t k = was[i];
+    if (!k) {
+        const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, i)];
+        int li = int(i - t.off), n;
+        k = fill_mode(a, t, was, i, li % int(t.w), li / int(t.w), n) != 0;
+    }
+    now[i] = k;
+}
+
+// one fill ring transposed, given the ring's starting flags
+__global__ void k_fill_t(PostArgs a, const uint8_t *was, const float4 *g_out, float4 *g_in) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= a.n_texels) return;
+    const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, j)];
+    int lj = int(j - t.off), x = lj % int(t.w), y = lj / int(t.w);
+    float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+    int n;
+    if (was[j]) {
+        g = g_out[j];
+        for (int yy = y > 0 ? y - 1 : 0; yy < min(y + 2, int(t.h)); yy++)
+            for (int xx = x > 0 ? x - 1 : 0; xx < min(x + 2, int(t.w)); xx++) {
+                uint32_t i = t.off + uint32_t(yy) * t.w + uint32_t(xx);
+                if (was[i]) continue;
+                int mode = fill_mode(a, t, was, i, xx, yy, n);
+                if (mode == 2 || (mode == 1 && a.chart[j] == a.chart[i])) {
+                    float4 go = g_out[i];
+                    float f = float(n);
+                    g.x += go.x / f, g.y += go.y / f, g.z += go.z / f;
+                }
+            }
+    } else if (fill_mode(a, t, was, j, x, y, n) == 0) {
+        g = g_out[j];
+    }
+    g_in[j] = g;
+}
+
+// the bounce smoothing's weight sums (filter.rs:20-53 over the gathered texels)
+__global__ void k_smooth_wsum(PostArgs a, int r, const float *w, float *wsum) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_texels) return;
+    float s = 0.0f;
+    if (a.gathered[i] && r > 0) {
+        const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, i)];
+        int li = int(i - t.off), x = li % int(t.w), y = li / int(t.w);
+        for (int yy = y > r ? y - r : 0; yy < min(y + r + 1, int(t.h)); yy++)
+            for (int xx = x > r ? x - r : 0; xx < min(x + r + 1, int(t.w)); xx++) {
+                uint32_t j = t.off + uint32_t(yy) * t.w + uint32_t(xx);
+                if (!a.gathered[j] || !same(a.chart, a.tex, i, j)) continue;
+                s += w[(yy - y + r) * (2 * r + 1) + (xx - x + r)];
+            }
+    }
+    wsum[i] = s;
+}
+
+// the bounce smoothing transposed (the Gaussian is symmetric: w(-d) = w(d))
+__global__ void k_smooth_t(PostArgs a, const float4 *g_out, int r, const float *w, const float *wsum, float4 *g_in) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= a.n_texels) return;
+    float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!a.gathered[j] || r == 0) {
+        g = g_out[j];
+    } else {
+        const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, j)];
+        int lj = int(j - t.off), x = lj % int(t.w), y = lj / int(t.w);
+        for (int yy = y > r ? y - r : 0; yy < min(y + r + 1, int(t.h)); yy++)
+            for (int xx = x > r ? x - r : 0; xx < min(x + r + 1, int(t.w)); xx++) {
+                uint32_t i = t.off + uint32_t(yy) * t.w + uint32_t(xx);
+                if (!a.gathered[i] || !same(a.chart, a.tex, i, j)) continue;
+                float f = w[(yy - y + r) * (2 * r + 1) + (xx - x + r)] / wsum[i];
+                float4 go = g_out[i];
+                g.x += go.x * f, g.y += go.y * f, g.z += go.z * f;
+            }
+    }
+    g_in[j] = g;
+}
+
+// the scatter of gather results (bake.rs:309-316) transposed
+__global__ void k_scatter_t(const uint32_t *idx, uint32_t n, const float4 *g_e, float4 *g_res) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) g_res[k] = g_e[idx[k]];
+}
+
+// write_light transposed: a known texel's atlas gradient goes to its direct light (summed over the
+// bounces) and to the previous bounce's indirect
+__global__ void k_light_t(PostArgs a, const uint8_t *kb, const float4 *g_light, float4 *g_dl, float4 *g_ind) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_texels) return;
+    float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (kb[i] >= 1) {
+        const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, i)];
+        uint32_t li = i - t.off;
+        g = g_light[size_t(t.y + li / t.w) * a.aw + t.x + li % t.w];
+    }
+    float4 d = g_dl[i];
+    g_dl[i] = make_float4(d.x + g.x, d.y + g.y, d.z + g.z, 0.f);
+    if (g_ind) g_ind[i] = g;
+}
+
+// Theta's gradient slots in a block's partial sums: albedo (3 a material of this chunk), then zenith,
+// horizon, ground and fallback (3 each).
+constexpr int FIXED_SLOTS = 12;
+
+// Per-thread accumulators in shared memory ([slot][thread]: a thread adds to its own column only),
+// then each slot summed over the block's threads in thread order: the same bits every launch.
+__device__ __forceinline__ void block_slots_out(double *acc, int slots, double *partial) {
+    __syncthreads();
+    for (int s = threadIdx.x; s < slots; s += blockDim.x) {
+        double v = 0.0;
+        for (int l = 0; l < int(blockDim.x); l++) v += acc[size_t(s) * blockDim.x + l];
+        partial[size_t(blockIdx.x) * slots + s] = v;
+    }
+}
+
+// The lit records, atlas texel by atlas texel (sorted): the atlas gradient (the texel's light fed each
+// record's term al / pi * e) and the albedo gradients of the chunk's materials (e / pi * pi / rays).
+__global__ void k_lit_t(const uint64_t *offs, const uint2 *sorted, uint32_t n_light, const float4 *light, Theta th,
+                        uint32_t m0, uint32_t mc, uint32_t rays, const float4 *g_res, float4 *g_light, int write_light,
+                        double *partial) {
+    extern __shared__ double acc[];  // [3 mc + FIXED_SLOTS][blockDim.x]
+    const int slots = 3 * int(mc) + FIXED_SLOTS;
+    for (int s = 0; s < slots; s++) acc[size_t(s) * blockDim.x + threadIdx.x] = 0.0;
+    float frays = __uint2float_rn(rays);
+    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < n_light; l += gridDim.x * blockDim.x) {
+        uint64_t b = offs[l], e = offs[l + 1];
+        if (b == e) {
+            if (write_light) g_light[l] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        float4 L = light[l];
+        float gx = 0.f, gy = 0.f, gz = 0.f;
+        for (uint64_t q = b; q < e; q++) {
+            uint2 s = sorted[q];
+            uint32_t k = s.x & 0x3fffffffu, m = s.y;
+            float4 g = g_res[k];
+            float cx = g.x / frays, cy = g.y / frays, cz = g.z / frays;
+            if (write_light) {
+                float3 al = th.albedo(m);
+                gx += cx * al.x, gy += cy * al.y, gz += cz * al.z;
+            }
+            if (m >= m0 && m < m0 + mc) {
+                size_t base = size_t(3 * (m - m0)) * blockDim.x + threadIdx.x;
+                acc[base] += double(cx) * double(L.x);
+                acc[base + blockDim.x] += double(cy) * double(L.y);
+                acc[base + 2 * blockDim.x] += double(cz) * double(L.z);
+            }
+        }
+        if (write_light) g_light[l] = make_float4(gx, gy, gz, 0.f);
+    }
+    block_slots_out(acc, slots, partial);
+}
+
+// The sky records and the surface records that take the fallback light: the sky's gradients, the
+// fallback's, and the albedo gradients of the chunk's materials lit by the fallback.
+__global__ void k_unlit_t(const uint2 *sorted, uint64_t n, Theta th, uint32_t m0, uint32_t mc, uint32_t rays,
+                          const float4 *g_res, int fixed_slots, double *partial) {
+    extern __shared__ double acc[];
+    const int slots = 3 * int(mc) + FIXED_SLOTS;
+    for (int s = 0; s < slots; s++) acc[size_t(s) * blockDim.x + threadIdx.x] = 0.0;
+    const double frays = double(rays), q = 3.14159265358979323846 / frays;
+    float3 fb = th.fallback();
+    double f[FIXED_SLOTS] = {0};
+    for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += uint64_t(gridDim.x) * blockDim.x) {
+        uint2 s = sorted[r];
+        uint32_t kind = s.x >> 30, k = s.x & 0x3fffffffu;
+        float4 g = g_res[k];
+        if (kind == KIND_SKY) {
+            double y = double(__uint_as_float(s.y));
+            if (y < 0.0) {
+                f[6] += g.x * q, f[7] += g.y * q, f[8] += g.z * q;
+            } else {
+                f[0] += g.x * q * y, f[1] += g.y * q * y, f[2] += g.z * q * y;
+                f[3] += g.x * q * (1.0 - y), f[4] += g.y * q * (1.0 - y), f[5] += g.z * q * (1.0 - y);
+            }
+        } else {
+            uint32_t m = s.y;
+            float3 al = th.albedo(m);
+            f[9] += g.x * double(al.x) / frays, f[10] += g.y * double(al.y) / frays, f[11] += g.z * double(al.z) / frays;
+            if (m >= m0 && m < m0 + mc) {
+                size_t base = size_t(3 * (m - m0)) * blockDim.x + threadIdx.x;
+                acc[base] += g.x * double(fb.x) / frays;
+                acc[base + blockDim.x] += g.y * double(fb.y) / frays;
+                acc[base + 2 * blockDim.x] += g.z * double(fb.z) / frays;
+            }
+        }
+    }
+    if (fixed_slots)
+        for (int c = 0; c < FIXED_SLOTS; c++) acc[size_t(3 * mc + c) * blockDim.x + threadIdx.x] = f[c];
+    block_slots_out(acc, slots, partial);
+}
+
+// the sun's gradient: the direct light is s * dl0, so d/ds = sum over texels of g_dl . dl0
+__global__ void k_sun_t(uint32_t n, const float4 *g_dl, const float4 *dl0, double *partial) {
+    __shared__ double acc[256];
+    double v = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 g = g_dl[i], d = dl0[i];
+        v += double(g.x) * d.x + double(g.y) * d.y + double(g.z) * d.z;
+    }
+    acc[threadIdx.x] = v;
+    block_slots_out(acc, 1, partial);
+}
+
+// Theta's gradient from the partial sums, in a fixed order: pass by pass (bounce, kind, material chunk),
+// block by block.
+struct PartialSet {
+    const double *p;   // [blocks][slots]
+    uint32_t m0, mc;   // the chunk's materials
+    int fixed;         // holds the fixed slots
+};
+
+__global__ void k_theta_final(const PartialSet *sets, int n_sets, int blocks, const double *sun, int sun_blocks,
+                              uint32_t M, float *g_theta) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t n_out = 3 * M + 10;
+    if (j >= n_out) return;
+    // output j reads slot(s): albedo 3m+c; zenith/horizon/ground; the fallback feeds zenith and horizon
+    double v = 0.0;
+    if (j == 3 * M + 9) {
+        for (int b = 0; b < sun_blocks; b++) v += sun[b];
+        g_theta[j] = float(v);
+        return;
+    }
+    for (int s = 0; s < n_sets; s++) {
+        const PartialSet &ps = sets[s];
+        int slots = 3 * int(ps.mc) + FIXED_SLOTS;
+        for (int b = 0; b < blocks; b++) {
+            const double *row = ps.p + size_t(b) * slots;
+            if (j < 3 * M) {
+                uint32_t m = j / 3;
+                if (m >= ps.m0 && m < ps.m0 + ps.mc) v += row[j - 3 * ps.m0];
+            } else if (ps.fixed) {
+                uint32_t c = j - 3 * M;  // 0..8: zenith, horizon, ground
+                v += row[3 * ps.mc + c];
+                if (c < 6) v += row[3 * ps.mc + 9 + c % 3] * (0.5 * 3.14159265358979323846);
+            }
+        }
+    }
+    g_theta[j] = float(v);
+}
+
+}  // namespace lbd
+
+namespace {
+
+inline dim3 tg(uint64_t n) { return dim3(uint32_t((n + 255) / 256)); }
+
+constexpr int T_THREADS = 128;          // threads of the adjoint's reduction kernels
+constexpr size_t T_SMEM = 160 * 1024;   // their shared memory at most
+
+}  // namespace
+
+struct lb_transport {
+    lb_plan *plan = nullptr;
+    lb_gpu *g = nullptr;
+    uint32_t M = 0, B = 0, n_gath = 0, rays = 0, n_light = 0, n_tex = 0, iw = 0, ih = 0;
+    uint32_t K = 0;                      // checkpoints kept by the forward
+    std::vector<uint32_t> ck_bounce;     // the bounce each checkpoint holds
+    int rings = 0, r = 0, blocks = 0, sun_blocks = 0;
+    uint32_t mc = 0;                     // materials a reduction pass covers
+    uint64_t n_rec = 0, n_lit = 0, unlit0 = 0, n_unlit = 0;
+    std::vector<float> theta0;
+    PostArgs a{};
+    CompositeArgs c{};
+    DBuf theta, rec, sorted, offs, kb, dl0, fixed_ind, masks, wsum, has0, has1, ckpt, work, res, e0, e1, fk_a, fk_b,
+        ind, out_atlas, out_tmp, out_has, out_has_b, out_direct, out_validity;
+    DBuf g_in, g_blocks_a, g_blocks_b, g_ind, g_a, g_b, g_res, g_light, g_dl, partials, sun_partials, sets_d, g_theta;
+    std::vector<lbd::PartialSet> sets;
+    cudaGraphExec_t fwd = nullptr, bwd = nullptr;
+    bool forward_done = false;
+    ~lb_transport() {
+        if (fwd) cudaGraphExecDestroy(fwd);
+        if (bwd) cudaGraphExecDestroy(bwd);
+        if (plan) lb_plan_free(plan);
+    }
+    lbd::Theta th() const { return lbd::Theta{theta.as<float>(), M}; }
+    float4 *slot(uint32_t j) const { return ckpt.as<float4>() + size_t(j) * n_light; }
+};
+
+namespace {
+
+// the bounces' light after bounce b of the forward: res, filters, write (the atlas rewritten in place)
+void bounce(lb_transport &t, float4 *light, uint32_t b, float4 *next, cudaStream_t st, float4 **filled) {
+    lbd::k_eval<<<t.g->sms * 8, 256, 0, st>>>(t.rec.as<uint2>(), t.n_gath, t.rays, light, t.n_light, t.th(),
+                                             t.res.as<float4>());
+    ck(cudaGetLastError(), "transport eval");
+    ck(lb_bounce_filters(t.a, t.res.as<float4>(), t.r, t.plan->wr.as<float>(), t.rings, t.fk_a.as<uint8_t>(),
+                         t.fk_b.as<uint8_t>(), t.e0.as<float4>(), t.e1.as<float4>(), filled, st),
+       "transport filters");
+    if (next && t.n_tex)
+        lbd::k_write_light<<<tg(t.n_tex), 256, 0, st>>>(t.a, t.kb.as<uint8_t>(), t.dl0.as<float4>(), t.th(), *filled,
+                                                        next);
+    (void)b;
+}
+
+void light0(lb_transport &t, float4 *light, cudaStream_t st) {
+    if (t.n_tex)
+        lbd::k_write_light<<<tg(t.n_tex), 256, 0, st>>>(t.a, t.kb.as<uint8_t>(), t.dl0.as<float4>(), t.th(), nullptr,
+                                                        light);
+    ck(cudaGetLastError(), "transport light");
+}
+
+// the forward, from theta (on the device) to the indirect atlas in out_atlas
+void record_forward(lb_transport &t, cudaStream_t st) {
+    bool all = t.K >= t.B;
+    float4 *filled = nullptr;
+    if (t.B > 0) {
+        float4 *cur = all ? t.slot(0) : t.work.as<float4>();
+        light0(t, cur, st);
+        uint32_t next_ck = 0;
+        for (uint32_t b = 0; b < t.B; b++) {
+            if (!all && next_ck < t.K && t.ck_bounce[next_ck] == b) {
+                ck(cudaMemcpyAsync(t.slot(next_ck), cur, size_t(t.n_light) * 16, cudaMemcpyDeviceToDevice, st),
+                   "checkpoint");
+                next_ck++;
+            }
+            float4 *nxt = b + 1 < t.B ? (all ? t.slot(b + 1) : cur) : nullptr;
+            bounce(t, cur, b, nxt, st, &filled);
+            if (nxt) cur = nxt;
+        }
+    }
+    if (t.n_tex)
+        lbd::k_final_ind<<<tg(t.n_tex), 256, 0, st>>>(t.n_tex, t.plan->state.as<uint8_t>(), filled,
+                                                      t.fixed_ind.as<float4>(), t.ind.as<float4>());
+    ck(lb_composite(t.c, t.out_tmp.as<float4>(), t.out_has_b.as<uint8_t>(), st), "transport composite");
+}
+
+// the adjoint, from the atlas gradient in g_in to theta's gradient in g_theta
+void record_backward(lb_transport &t, cudaStream_t st) {
+    const PostArgs &a = t.a;
+    uint64_t nb = uint64_t(t.iw) * t.ih;
+    ck(cudaMemsetAsync(t.g_dl.p, 0, t.g_dl.bytes, st), "memset");
+    // the dilations transposed, last first, then the composite
+    lbd::k_dilate_t<<<tg(nb), 256, 0, st>>>(t.has1.as<uint8_t>(), t.g_in.as<float4>(), t.g_blocks_a.as<float4>(), t.iw,
+                                            t.ih);
+    lbd::k_dilate_t<<<tg(nb), 256, 0, st>>>(t.has0.as<uint8_t>(), t.g_blocks_a.as<float4>(), t.g_blocks_b.as<float4>(),
+                                            t.iw, t.ih);
+    if (t.n_tex)
+        lbd::k_composite_t<<<tg(t.n_tex), 256, 0, st>>>(a, t.c, t.g_blocks_b.as<float4>(), t.g_ind.as<float4>());
+    ck(cudaGetLastError(), "transport composite^T");
+    bool all = t.K >= t.B;
+    size_t smem = size_t(3 * t.mc + lbd::FIXED_SLOTS) * T_THREADS * sizeof(double);
+    int set = 0;
+    for (int32_t b = int32_t(t.B) - 1; b >= 0; b--) {
+        // the light this bounce read: kept, or recomputed from the nearest earlier checkpoint
+        float4 *light;
+        if (all) {
+            light = t.slot(uint32_t(b));
+        } else {
+            uint32_t j = 0;
+            while (j + 1 < t.K && t.ck_bounce[j + 1] <= uint32_t(b)) j++;
+            light = t.work.as<float4>();
+            ck(cudaMemcpyAsync(light, t.slot(j), size_t(t.n_light) * 16, cudaMemcpyDeviceToDevice, st), "restore");
+            float4 *filled = nullptr;
+            for (uint32_t bb = t.ck_bounce[j]; bb < uint32_t(b); bb++) bounce(t, light, bb, light, st, &filled);
+        }
+        if (t.n_tex) {
+            // fill rings transposed (last ring first), the smoothing, the scatter
+            float4 *outs[2] = {t.g_a.as<float4>(), t.g_b.as<float4>()};
+            float4 *gw = t.g_ind.as<float4>();
+            for (int q = t.rings - 1, o = 0; q >= 0; q--, o ^= 1) {
+                lbd::k_fill_t<<<tg(t.n_tex), 256, 0, st>>>(a, t.masks.as<uint8_t>() + size_t(q) * t.n_tex, gw, outs[o]);
+                gw = outs[o];
+            }
+            float4 *gs = gw == outs[0] ? outs[1] : outs[0];
+            lbd::k_smooth_t<<<tg(t.n_tex), 256, 0, st>>>(a, gw, t.r, t.plan->wr.as<float>(), t.wsum.as<float>(), gs);
+            if (t.n_gath)
+                lbd::k_scatter_t<<<tg(t.n_gath), 256, 0, st>>>(t.plan->gath_idx.as<uint32_t>(), t.n_gath, gs,
+                                                               t.g_res.as<float4>());
+        }
+        ck(cudaGetLastError(), "transport filters^T");
+        // the records transposed: the atlas gradient and theta's partial sums, chunk by chunk of materials
+        for (uint32_t m0 = 0, first = 1; m0 < std::max(t.M, 1u); m0 += t.mc, first = 0) {
+            uint32_t mc = std::min(t.mc, std::max(t.M, 1u) - m0);
+            lbd::k_lit_t<<<t.blocks, T_THREADS, smem, st>>>(
+                t.offs.as<uint64_t>(), t.sorted.as<uint2>(), t.n_light, light, t.th(), m0, mc, t.rays, t.g_res.as<float4>(),
+                t.g_light.as<float4>(), int(first), const_cast<double *>(t.sets[set].p));
+            set++;
+            lbd::k_unlit_t<<<t.blocks, T_THREADS, smem, st>>>(t.sorted.as<uint2>() + t.unlit0, t.n_unlit, t.th(), m0, mc,
+                                                             t.rays, t.g_res.as<float4>(), int(first),
+                                                             const_cast<double *>(t.sets[set].p));
+            set++;
+        }
+        ck(cudaGetLastError(), "transport records^T");
+        // write_light transposed: into the direct light, and the previous bounce's indirect
+        if (t.n_tex)
+            lbd::k_light_t<<<tg(t.n_tex), 256, 0, st>>>(a, t.kb.as<uint8_t>(), t.g_light.as<float4>(), t.g_dl.as<float4>(),
+                                                        b > 0 ? t.g_ind.as<float4>() : nullptr);
+    }
+    lbd::k_sun_t<<<t.sun_blocks, 256, 0, st>>>(t.n_tex, t.g_dl.as<float4>(), t.dl0.as<float4>(),
+                                              t.sun_partials.as<double>());
+    uint32_t n_out = 3 * t.M + 10;
+    lbd::k_theta_final<<<tg(n_out), 256, 0, st>>>(t.sets_d.as<lbd::PartialSet>(), int(t.sets.size()), t.blocks,
+                                                  t.sun_partials.as<double>(), t.sun_blocks, t.M, t.g_theta.as<float>());
+    ck(cudaGetLastError(), "transport theta");
+}
+
+cudaGraphExec_t capture(lb_transport &t, void (*rec)(lb_transport &, cudaStream_t)) {
+    cudaStream_t st = t.g->stream;
+    ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        rec(t, st);
+    } catch (...) {
+        cudaGraph_t gr = nullptr;
+        cudaStreamEndCapture(st, &gr);
+        if (gr) cudaGraphDestroy(gr);
+        throw;
+    }
+    cudaGraph_t gr = nullptr;
+    ck(cudaStreamEndCapture(st, &gr), "end capture");
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+    cudaGraphDestroy(gr);
+    ck(e, "graph instantiate");
+    return ex;
+}
+
+template <class T> void up(DBuf &d, const std::vector<T> &v, cudaStream_t st) {
+    d.alloc(v.size() * sizeof(T));
+    if (!v.empty()) ck(cudaMemcpyAsync(d.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st), "upload");
+}
+
+void build(lb_transport &t, uint32_t max_checkpoints) {
+    lb_plan &p = *t.plan;
+    cudaStream_t st = t.g->stream;
+    const lb::SceneHeader &h = p.scene.header;
+    if (p.n_dirty_texels != p.n_all)
+        throw std::runtime_error("lb_transport_create: every tile must be baked (no cache)");
+    // the bake at theta0: its arrays hold every fixed input
+    if (lb_plan_launch(&p) != LB_OK) throw std::runtime_error(lb_last_error());
+    ck(cudaStreamSynchronize(st), "bake");
+    t.M = uint32_t(h.materials.size());
+    t.B = h.bake.gi_bounces;
+    t.rays = p.P.params.counts[2];
+    t.n_light = p.aw * p.ah;
+    t.n_tex = p.n_dirty_texels;
+    t.iw = p.iw;
+    t.ih = p.ih;
+    t.r = int(h.bake.gi_filter * p.ds);
+    t.rings = int(h.lightmap.padding + 2 * p.ds + 2);
+    ck(cudaMemcpy(&t.n_gath, p.gath_count.p, 4, cudaMemcpyDeviceToHost), "gathered count");
+    if (t.n_gath >= (1u << 30)) throw std::runtime_error("lb_transport_create: too many gathered texels");
+    t.n_rec = uint64_t(t.n_gath) * t.rays;
+    if (t.n_rec >= (1ull << 31)) throw std::runtime_error("lb_transport_create: more than 2^31 gather rays");
+    // theta0: the scene's albedos and sky, the sun at its own irradiance
+    t.theta0.clear();
+    for (auto &m : h.materials) t.theta0.insert(t.theta0.end(), m.albedo.begin(), m.albedo.end());
+    for (auto *c : {&h.sky.zenith, &h.sky.horizon, &h.sky.ground}) t.theta0.insert(t.theta0.end(), c->begin(), c->end());
+    t.theta0.push_back(1.0f);
+    up(t.theta, t.theta0, st);
+    t.a = lb_plan_post_args(p);
+    size_t N = std::max<size_t>(t.n_tex, 1);
+    // fixed inputs: known during the bounces, the direct light at the scene's irradiance, the fallback
+    // texels' light
+    t.kb.alloc(N);
+    t.dl0.alloc(N * 16);
+    t.fixed_ind.alloc(N * 16);
+    if (t.n_tex) {
+        lbd::k_known_bounce<<<tg(t.n_tex), 256, 0, st>>>(t.n_tex, p.known.as<uint8_t>(), p.state.as<uint8_t>(),
+                                                         t.kb.as<uint8_t>());
+        ck(cudaMemcpyAsync(t.dl0.p, p.dl.p, size_t(t.n_tex) * 16, cudaMemcpyDeviceToDevice, st), "dl0");
+        ck(cudaMemcpyAsync(t.fixed_ind.p, p.ind.p, size_t(t.n_tex) * 16, cudaMemcpyDeviceToDevice, st), "ind");
+    }
+    // the bounce fill's flags ring by ring, the smoothing's weight sums
+    t.masks.alloc(size_t(t.rings + 1) * N);
+    t.wsum.alloc(N * 4);
+    if (t.n_tex) {
+        ck(cudaMemcpyAsync(t.masks.p, p.gathered.p, t.n_tex, cudaMemcpyDeviceToDevice, st), "masks");
+        for (int q = 0; q < t.rings; q++)
+            lbd::k_fill_mask<<<tg(t.n_tex), 256, 0, st>>>(t.a, t.masks.as<uint8_t>() + size_t(q) * t.n_tex,
+                                                          t.masks.as<uint8_t>() + size_t(q + 1) * t.n_tex);
+        lbd::k_smooth_wsum<<<tg(t.n_tex), 256, 0, st>>>(t.a, t.r, p.wr.as<float>(), t.wsum.as<float>());
+    }
+    // the composite's arguments (its outputs in the transport's own arrays) and its dilation flags
+    uint64_t nb = uint64_t(t.iw) * t.ih;
+    t.ind.alloc(N * 16);
+    t.out_atlas.alloc(nb * 16);
+    t.out_tmp.alloc(nb * 16);
+    t.out_has.alloc(nb);
+    t.out_has_b.alloc(nb);
+    t.out_direct.alloc(size_t(t.n_light) * 8);
+    t.out_validity.alloc(t.n_light);
+    t.c.owner = p.owner.as<uint32_t>();
+    t.c.known = p.known.as<uint8_t>();
+    t.c.state = p.state.as<uint8_t>();
+    t.c.field = p.field.as<float>();
+    t.c.ao = p.ao.as<float>();
+    t.c.ind = t.ind.as<float4>();
+    t.c.aw = p.aw;
+    t.c.ah = p.ah;
+    t.c.iw = p.iw;
+    t.c.ih = p.ih;
+    t.c.ds = p.ds;
+    t.c.direct_out = t.out_direct.as<float2>();
+    t.c.validity = t.out_validity.as<uint8_t>();
+    t.c.indirect = t.out_atlas.as<float4>();
+    t.c.has = t.out_has.as<uint8_t>();
+    // has0: the composite's own flags (before its dilations), from the bake's indirect through one run
+    t.has0.alloc(nb);
+    t.has1.alloc(nb);
+    {
+        CompositeArgs c0 = t.c;
+        c0.ind = p.ind.as<float4>();
+        c0.has = t.has0.as<uint8_t>();
+        c0.indirect = t.out_tmp.as<float4>();
+        // composite alone (no dilation): its flags are has0
+        ck(lb_composite_blocks(c0, st), "composite flags");
+        if (nb) lbd::k_dilate_mask<<<tg(nb), 256, 0, st>>>(t.has0.as<uint8_t>(), t.has1.as<uint8_t>(), t.iw, t.ih);
+    }
+    // every gather ray's outcome
+    t.rec.alloc(t.n_rec * 8);
+    t.res.alloc(std::max<size_t>(t.n_gath, 1) * 16);
+    if (t.n_rec) {
+        lbd::Scene S = lb_scene_view(p.dscene);
+        lbd::k_records<<<t.g->sms * 8, 128, 0, st>>>(S, p.P.params, p.tex.as<float4>(), p.gath_idx.as<uint32_t>(),
+                                                    p.posg.as<float4>(), t.n_gath, t.n_light, t.rec.as<uint2>());
+        ck(cudaGetLastError(), "records");
+    }
+    // the records sorted for the adjoint: lit ones by atlas texel, then sky and fallback-lit, then none
+    t.sorted.alloc(t.n_rec * 8);
+    t.offs.alloc(size_t(t.n_light + 3) * 8);
+    {
+        DBuf keys, vals, keys2, vals2, temp;
+        size_t n = std::max<uint64_t>(t.n_rec, 1);
+        keys.alloc(n * 4);
+        vals.alloc(n * 4);
+        keys2.alloc(n * 4);
+        vals2.alloc(n * 4);
+        if (t.n_rec) {
+            lbd::k_record_keys<<<t.g->sms * 8, 256, 0, st>>>(t.rec.as<uint2>(), t.n_rec, p.light.as<float4>(), t.n_light,
+                                                            t.M, keys.as<uint32_t>(), vals.as<uint32_t>());
+            size_t tb = 0;
+            ck(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.as<uint32_t>(), keys2.as<uint32_t>(), vals.as<uint32_t>(),
+                                               vals2.as<uint32_t>(), int(t.n_rec), 0, 32, st),
+               "sort size");
+            temp.alloc(tb);
+            ck(cub::DeviceRadixSort::SortPairs(temp.p, tb, keys.as<uint32_t>(), keys2.as<uint32_t>(), vals.as<uint32_t>(),
+                                               vals2.as<uint32_t>(), int(t.n_rec), 0, 32, st),
+               "sort");
+            lbd::k_record_sorted<<<t.g->sms * 8, 256, 0, st>>>(t.rec.as<uint2>(), vals2.as<uint32_t>(), t.n_rec, t.rays,
+                                                              t.sorted.as<uint2>());
+        }
+        lbd::k_record_offsets<<<tg(t.n_light + 3), 256, 0, st>>>(keys2.as<uint32_t>(), t.n_rec, t.n_light,
+                                                                 t.offs.as<uint64_t>());
+        ck(cudaGetLastError(), "record order");
+        std::vector<uint64_t> tail(3);
+        ck(cudaMemcpyAsync(tail.data(), t.offs.as<uint64_t>() + t.n_light, 24, cudaMemcpyDeviceToHost, st), "offsets");
+        ck(cudaStreamSynchronize(st), "record order");
+        t.n_lit = tail[0];
+        t.unlit0 = tail[0];
+        t.n_unlit = tail[2] - tail[0];
+    }
+    // checkpoints: every bounce's light when the budget allows, else K spread evenly (the first is bounce 0)
+    t.K = max_checkpoints == 0 ? t.B : std::min(max_checkpoints, t.B);
+    t.ck_bounce.clear();
+    for (uint32_t j = 0; j < t.K; j++) t.ck_bounce.push_back(uint32_t(uint64_t(j) * t.B / t.K));
+    t.ckpt.alloc(size_t(std::max(t.K, 1u)) * t.n_light * 16);
+    ck(cudaMemsetAsync(t.ckpt.p, 0, t.ckpt.bytes, st), "checkpoints");
+    t.work.alloc(size_t(t.n_light) * 16);
+    ck(cudaMemsetAsync(t.work.p, 0, t.work.bytes, st), "work");
+    t.e0.alloc(N * 16);
+    t.e1.alloc(N * 16);
+    t.fk_a.alloc(N);
+    t.fk_b.alloc(N);
+    // the adjoint's arrays and its fixed reduction grid
+    t.g_in.alloc(nb * 16);
+    t.g_blocks_a.alloc(nb * 16);
+    t.g_blocks_b.alloc(nb * 16);
+    t.g_ind.alloc(N * 16);
+    t.g_a.alloc(N * 16);
+    t.g_b.alloc(N * 16);
+    t.g_dl.alloc(N * 16);
+    t.g_res.alloc(std::max<size_t>(t.n_gath, 1) * 16);
+    t.g_light.alloc(size_t(t.n_light) * 16);
+    t.g_theta.alloc(size_t(3 * t.M + 10) * 4);
+    t.blocks = t.g->sms * 2;
+    t.sun_blocks = t.g->sms * 2;
+    size_t per_mat = size_t(3) * T_THREADS * sizeof(double), fixed = size_t(lbd::FIXED_SLOTS) * T_THREADS * sizeof(double);
+    t.mc = uint32_t(std::max<size_t>(1, (T_SMEM - fixed) / per_mat));
+    t.mc = std::min(t.mc, std::max(t.M, 1u));
+    size_t smem = size_t(3 * t.mc + lbd::FIXED_SLOTS) * T_THREADS * sizeof(double);
+    ck(cudaFuncSetAttribute(lbd::k_lit_t, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem");
+    ck(cudaFuncSetAttribute(lbd::k_unlit_t, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem");
+    uint32_t chunks = (std::max(t.M, 1u) + t.mc - 1) / t.mc;
+    size_t per_set = size_t(t.blocks) * (3 * t.mc + lbd::FIXED_SLOTS);
+    size_t n_sets = size_t(t.B) * chunks * 2;
+    t.partials.alloc(std::max<size_t>(n_sets, 1) * per_set * sizeof(double));
+    t.sun_partials.alloc(size_t(t.sun_blocks) * sizeof(double));
+    t.sets.clear();
+    for (size_t s = 0; s < n_sets; s++) {
+        uint32_t chunk = uint32_t((s / 2) % chunks);
+        uint32_t m0 = chunk * t.mc, mc = std::min(t.mc, std::max(t.M, 1u) - m0);
+        lbd::PartialSet ps{t.partials.as<double>() + s * per_set, m0, mc, int(chunk == 0)};
+        t.sets.push_back(ps);
+    }
+    // a chunk's partial rows are laid out with its own slot count: give every set the chunk's mc
+    up(t.sets_d, t.sets, st);
+    ck(cudaStreamSynchronize(st), "transport arrays");
+    t.fwd = capture(t, record_forward);
+    t.bwd = capture(t, record_backward);
+}
+
+int fail(const std::exception &e) {
+    lb_set_error(e.what());
+    return LB_ECUDA;
+}
+
+}  // namespace
+
+extern "C" {
+
+lb_transport *lb_transport_create(lb_gpu *g, const uint8_t *scene, size_t len, uint32_t max_checkpoints) {
+    if (!g || !scene) {
+        lb_set_error("lb_transport_create: bad arguments");
+        return nullptr;
+    }
+    lb_bake_options o{};
+    lb_plan *p = lb_plan_create(g, scene, len, &o);
+    if (!p) return nullptr;
+    auto t = std::make_unique<lb_transport>();
+    t->plan = p;
+    t->g = g;
+    try {
+        build(*t, max_checkpoints);
+        return t.release();
+    } catch (const std::exception &e) {
+        lb_set_error(e.what());
+    }
+    return nullptr;
+}
+
+int lb_transport_info(const lb_transport *t, lb_transport_shape *info) {
+    if (!t || !info) return LB_EINVAL;
+    std::memset(info, 0, sizeof *info);
+    info->n_materials = t->M;
+    info->n_params = 3 * t->M + 10;
+    info->bounces = t->B;
+    info->checkpoints = t->K;
+    info->indirect_width = t->iw;
+    info->indirect_height = t->ih;
+    info->gathered = t->n_gath;
+    info->rays = t->rays;
+    info->records = t->n_rec;
+    info->lit_records = t->n_lit;
+    info->unlit_records = t->n_unlit;
+    info->checkpoint_bytes = uint64_t(std::max(t->K, 1u)) * t->n_light * 16;
+    return LB_OK;
+}
+
+int lb_transport_theta0(const lb_transport *t, float *theta) {
+    if (!t || !theta) return LB_EINVAL;
+    std::memcpy(theta, t->theta0.data(), t->theta0.size() * 4);
+    return LB_OK;
+}
+
+int lb_transport_forward_async(lb_transport *t, const float *d_theta, float *d_indirect) {
+    if (!t || !d_theta || !d_indirect) return LB_EINVAL;
+    cudaStream_t st = t->g->stream;
+    cudaError_t e = cudaMemcpyAsync(t->theta.p, d_theta, t->theta.bytes, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaGraphLaunch(t->fwd, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_indirect, t->out_atlas.p, size_t(t->iw) * t->ih * 16, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return lb_cuda_fail(e, "lb_transport_forward");
+    t->forward_done = true;
+    return LB_OK;
+}
+
+int lb_transport_backward_async(lb_transport *t, const float *d_g_indirect, float *d_g_theta) {
+    if (!t || !d_g_indirect || !d_g_theta) return LB_EINVAL;
+    if (!t->forward_done) {
+        lb_set_error("lb_transport_backward: no forward to differentiate");
+        return LB_EINVAL;
+    }
+    cudaStream_t st = t->g->stream;
+    cudaError_t e = cudaMemcpyAsync(t->g_in.p, d_g_indirect, size_t(t->iw) * t->ih * 16, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaGraphLaunch(t->bwd, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_g_theta, t->g_theta.p, t->g_theta.bytes, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return lb_cuda_fail(e, "lb_transport_backward");
+    return LB_OK;
+}
+
+int lb_transport_forward(lb_transport *t, const float *theta, float *indirect) {
+    if (!t || !theta || !indirect) return LB_EINVAL;
+    cudaStream_t st = t->g->stream;
+    cudaError_t e = cudaMemcpyAsync(t->theta.p, theta, t->theta.bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaGraphLaunch(t->fwd, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(indirect, t->out_atlas.p, size_t(t->iw) * t->ih * 16, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return lb_cuda_fail(e, "lb_transport_forward");
+    t->forward_done = true;
+    return LB_OK;
+}
+
+int lb_transport_backward(lb_transport *t, const float *g_indirect, float *g_theta) {
+    if (!t || !g_indirect || !g_theta) return LB_EINVAL;
+    if (!t->forward_done) {
+        lb_set_error("lb_transport_backward: no forward to differentiate");
+        return LB_EINVAL;
+    }
+    cudaStream_t st = t->g->stream;
+    cudaError_t e = cudaMemcpyAsync(t->g_in.p, g_indirect, size_t(t->iw) * t->ih * 16, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaGraphLaunch(t->bwd, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(g_theta, t->g_theta.p, t->g_theta.bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return lb_cuda_fail(e, "lb_transport_backward");
+    return LB_OK;
+}
+
+int lb_transport_bake_indirect(lb_transport *t, float *indirect) {
+    if (!t || !indirect) return LB_EINVAL;
+    cudaError_t e = cudaMemcpyAsync(indirect, t->plan->indirect.p, size_t(t->iw) * t->ih * 16, cudaMemcpyDeviceToHost,
+                                    t->g->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t->g->stream);
+    if (e != cudaSuccess) return lb_cuda_fail(e, "lb_transport_bake_indirect");
+    return LB_OK;
+}
+
+size_t lb_transport_export(lb_transport *t, const char *name, void *out, size_t cap) {
+    if (!t || !name) return 0;
+    lb_plan &p = *t->plan;
+    const void *src = nullptr;
+    size_t bytes = 0;
+    std::vector<uint8_t> host;
+    std::string n = name;
+    auto dev = [&](const DBuf &d, size_t b) {
+        src = d.p;
+        bytes = b;
+    };
+    if (n == "records") dev(t->rec, t->n_rec * 8);
+    else if (n == "gathered_index") dev(p.gath_idx, size_t(t->n_gath) * 4);
+    else if (n == "texels") dev(p.tex, size_t(t->n_tex) * 64);
+    else if (n == "sample_points") dev(p.posg, size_t(t->n_tex) * 16);
+    else if (n == "chart") dev(p.chart, size_t(t->n_tex) * 4);
+    else if (n == "gathered") dev(p.gathered, t->n_tex);
+    else if (n == "known") dev(p.known, t->n_tex);
+    else if (n == "known_bounce") dev(t->kb, t->n_tex);
+    else if (n == "state") dev(p.state, t->n_tex);
+    else if (n == "direct_light") dev(t->dl0, size_t(t->n_tex) * 16);
+    else if (n == "fixed_indirect") dev(t->fixed_ind, size_t(t->n_tex) * 16);
+    else if (n == "owner") dev(p.owner, size_t(t->n_light) * 4);
+    else if (n == "light_flags") {
+        // the atlas's known flags (w of the light atlas)
+        std::vector<float> l(size_t(t->n_light) * 4);
+        if (cudaMemcpy(l.data(), p.light.p, l.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+        host.resize(t->n_light);
+        for (size_t i = 0; i < t->n_light; i++) host[i] = l[4 * i + 3] > 0.5f;
+        bytes = host.size();
+    } else if (n == "tiles") {
+        bytes = p.dirty.size() * sizeof(DTile);
+        host.resize(bytes);
+        std::memcpy(host.data(), p.tiles_all.data(), bytes);
+    } else if (n == "smooth_weights") dev(p.wr, size_t(2 * t->r + 1) * (2 * t->r + 1) * 4);
+    else if (n == "shape") {
+        // aw, ah, iw, ih, ds, smoothing radius, fill rings, bounces, rays, gathered, texels, materials
+        uint32_t v[12] = {p.aw, p.ah, p.iw, p.ih, p.ds, uint32_t(t->r), uint32_t(t->rings), t->B, t->rays, t->n_gath,
+                          t->n_tex, t->M};
+        host.resize(sizeof v);
+        std::memcpy(host.data(), v, sizeof v);
+        bytes = sizeof v;
+    } else {
+        lb_set_error("lb_transport_export: unknown array");
+        return 0;
+    }
+    if (!out) return bytes;
+    if (cap < bytes) {
+        lb_set_error("lb_transport_export: buffer too small");
+        return 0;
+    }
+    if (!host.empty()) std::memcpy(out, host.data(), bytes);
+    else if (bytes && cudaMemcpy(out, src, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        lb_set_error("lb_transport_export: copy failed");
+        return 0;
+    }
+    return bytes;
+}
+
+void lb_transport_free(lb_transport *t) {
+    if (t) {
+        cudaStreamSynchronize(t->g->stream);
+        delete t;
+    }
+}
+
+}  // extern "C"

@@ -227,4 +227,70 @@ def reference_test(box_x: float = 8.0) -> bytes:
     return _assemble(groups, materials, sun, sky, lightmap, bake, volume, {"test": True})
 
 
+def uneven_tiles(seed: int = 0, tiles: int = 8, tri_range=(5_000, 500_000), grid: float = 0.25,
+                 bounces: int = 3) -> bytes:
+    """Tiles of uneven weight for the batched bake: a tiles x tiles grid of 16 m tiles (the layout's tile
+    size) on a flat-ish heightfield, each tile's triangle count drawn lognormal over tri_range and made up
+    with small open cylinders (64 triangles each) crowded into the tile, so that both the triangles a ray
+    meets and the texels a tile holds (its atlas region) vary by orders of magnitude. Materials, ray counts
+    and bounces as map_100m; the volume is left out."""
+    rng = np.random.default_rng(seed)
+    extent = 16.0 * tiles
+    noise = _value_noise(rng, 3, 0.5, extent)
+    ground = heightfield(0.0, 0.0, extent, extent, grid, noise)
+    per_tile_ground = len(ground) // 3 // (tiles * tiles)
+    lo, hi = np.log(tri_range[0]), np.log(tri_range[1])
+    counts = np.exp(np.clip(rng.normal((lo + hi) / 2, (hi - lo) / 4, size=tiles * tiles), lo, hi)).astype(int)
+    materials = [_material(f"m{k}", rng.uniform(0.15, 0.85, size=3)) for k in range(16)]
+    per_mat = [[] for _ in range(16)]
+    for t, want in enumerate(counts):
+        tx, tz = (t % tiles) * 16.0, (t // tiles) * 16.0
+        n_cyl = max(0, (int(want) - per_tile_ground) // 64)
+        if n_cyl == 0:
+            continue
+        x = tx + rng.uniform(0.5, 15.5, n_cyl)
+        z = tz + rng.uniform(0.5, 15.5, n_cyl)
+        r = rng.uniform(0.03, 0.25, n_cyl)
+        h = rng.uniform(0.3, 4.0, n_cyl)
+        yaw = rng.uniform(0.0, 2 * math.pi, n_cyl)
+        m = rng.integers(0, 16, n_cyl)
+        base = noise(x, z) - 0.1
+        for k in range(n_cyl):
+            per_mat[int(m[k])].append(cylinder(x[k], base[k], z[k], r[k], h[k], yaw[k]))
+    groups = [("ground", 0, ground)]
+    for k in range(16):
+        if per_mat[k]:
+            groups.append((f"props{k}", k, np.concatenate(per_mat[k])))
+    sky = {"zenith": [0.5, 0.6, 0.8], "horizon": [0.5, 0.6, 0.8], "ground": [0.5, 0.6, 0.8]}
+    sun = {"direction": sun_direction(40.0, 130.0), "radiusDeg": 0.5, "irradiance": [3.0, 3.0, 3.0]}
+    lightmap = {"texelsPerMeter": 4.0, "tileSize": 16.0, "chartAngleDeg": 40.0, "padding": 2, "atlasWidth": 4096,
+                "indirectDownscale": 2}
+    bake = _defaults_bake(aoRays=256, aoReach=2.0, giRays=128, giBounces=bounces)
+    return _assemble(groups, materials, sun, sky, lightmap, bake, None,
+                     {"workload": "uneven_tiles", "seed": seed, "tile_triangles": [int(c) for c in counts]})
+
+
+def with_light(scene: bytes, albedo=None, zenith=None, horizon=None, ground=None, irradiance=None) -> bytes:
+    """The same scene with other light parameters: materials' albedos (one rgb a material), the sky's
+    colours, the sun's irradiance. Only the header changes (scene.rs:164-181: "LBSC", version, header
+    length, header JSON padded to 4 bytes, then the meshes)."""
+    import json
+    import struct
+    hl = struct.unpack_from("<I", scene, 8)[0]
+    h = json.loads(scene[12:12 + hl])
+    if albedo is not None:
+        for m, a in zip(h["materials"], np.asarray(albedo, np.float32).reshape(-1, 3)):
+            m["albedo"] = [float(v) for v in a]
+    for key, v in (("zenith", zenith), ("horizon", horizon), ("ground", ground)):
+        if v is not None:
+            h["sky"][key] = [float(c) for c in np.asarray(v, np.float32)]
+    if irradiance is not None:
+        h["sun"]["irradiance"] = [float(c) for c in np.asarray(irradiance, np.float32)]
+    head = json.dumps(h, separators=(",", ":")).encode()
+    pad = lambda n: (n + 3) & ~3  # noqa: E731
+    rest = scene[pad(12 + hl):]
+    body = scene[:8] + struct.pack("<I", len(head)) + head
+    return body + b"\0" * (pad(len(body)) - len(body)) + rest
+
+
 WORKLOADS = {"small_map": small_map, "map_100m": map_100m, "reference_test": reference_test}

@@ -51,6 +51,8 @@ def lib():
         l.or_ray_ambiguous.argtypes = [vp, sz, vp, sz, vp, sz, vp, vp, vp, C.c_float, C.c_uint32, C.c_double]
         l.or_item_rays.restype = sz
         l.or_item_rays.argtypes = [C.c_int, vp, vp, sz, C.c_uint32, vp, vp, vp, vp, vp, vp, sz]
+        l.or_gather_records.restype = C.c_int
+        l.or_gather_records.argtypes = [vp, sz, vp, sz, vp, sz, vp, sz, vp, vp, sz, sz, vp, C.c_int]
         l.or_pcg.restype = C.c_uint32
         l.or_pcg.argtypes = [C.c_uint32]
         l.or_rand.restype = C.c_float
@@ -142,6 +144,21 @@ def item_rays(pass_: int, params, item, index: int, pick: int = 0, cap: int = 40
                            _p(anyh), _p(key), _p(kind), cap)
     n = min(n, cap)
     return {"o": o[:n], "d": d[:n], "tmax": tmax[:n], "any": anyh[:n], "key": key[:n], "kind": kind[:n]}
+
+
+def gather_records(scene: Scene, params, items: np.ndarray, n_light: int, threads: int = 0) -> np.ndarray:
+    """Every gather ray's outcome (oracle.h: or_gather_records): (n, rays, 4) uint32 of kind (0 sky,
+    1 back face, 2 surface), material, atlas texel (0xffffffff: none), bits of the direction's y."""
+    items = np.ascontiguousarray(items)
+    rays = int(params.counts[2])
+    out = np.zeros((len(items), rays, 4), np.uint32)
+    rc = lib().or_gather_records(_p(scene.nodes), len(scene.nodes), _p(scene.tris), len(scene.tris),
+                                 _p(scene.materials), len(scene.materials),
+                                 _p(scene.charts) if len(scene.charts) else None, len(scene.charts), C.byref(params),
+                                 _p(items), len(items), int(n_light), _p(out), int(threads))
+    if rc != 0:
+        raise RuntimeError(f"oracle gather records failed: {rc}")
+    return out
 
 
 def pcg(v: int) -> int:
