@@ -203,7 +203,9 @@ def kernel_only(args):
     items = (direct if args.kernel_only == "direct" else gather)[: args.items]
     gpu = lb.Gpu.new(0)
     gpu.set_pass_kernel(1)
-    bvh, refill, near, order = (int(x) for x in args.walk.split(","))
+    walk = [int(x) for x in args.walk.split(",")]
+    bvh, refill, near, order = walk[:4]
+    gpu.set_register_cap(walk[4] if len(walk) > 4 else 0)
     gpu.set_bvh(bvh)
     gpu.set_refill(refill)
     gpu.set_near(near)
@@ -436,8 +438,9 @@ def main():
             tp[j] += h
             tm[j] -= h
             fd = (loss(tp) - loss(tm)) / (2 * h)
-            checks.append({"param": j, "adjoint": float(grad[j]), "central_difference": fd,
-                           "rel_err": abs(fd - grad[j]) / max(abs(grad[j]), 1e-30)})
+            gj = float(grad[j])
+            checks.append({"param": j, "adjoint": gj, "central_difference": float(fd),
+                           "rel_err": float(abs(fd - gj) / max(abs(gj), 1e-30))})
         tr.close()
         one = lb.Transport(scene, gpu, max_checkpoints=1)
         one.forward_async(th.data_ptr(), out_t.data_ptr())

@@ -134,6 +134,10 @@ int lb_set_ray_order(lb_gpu *gpu, int direct, int gather);
  * and every occlusion ray tests that list instead of walking the tree. Same hits (between triangles
  * at exactly equal distance the first found in list order). */
 int lb_set_near(lb_gpu *gpu, int on);
+/* Register cap of the warp kernels over the BVH2 (direct and gather, without counting): 0 (default) the
+ * compiler's own budget; 3 or 4 registers capped so that this many 256-thread blocks share an SM (more
+ * warps in flight, some values spilled). Same results. */
+int lb_set_register_cap(lb_gpu *gpu, int blocks);
 /* Lane refill in the warp kernels' occlusion and gather rays over the BVH2 (default off): a lane whose
  * ray has ended starts the item's next one instead of waiting for its round. Same results. */
 int lb_set_refill(lb_gpu *gpu, int on);

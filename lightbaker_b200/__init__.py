@@ -152,6 +152,10 @@ class Gpu:
         """Leaf lists for the warp kernels' occlusion rays (BVH2). Same results."""
         N.check(N.lib().lb_set_near(self._h, int(on)), "lb_set_near")
 
+    def set_register_cap(self, blocks: int) -> None:
+        """0: the compiler's register budget; 3 or 4: registers capped for that many blocks an SM."""
+        N.check(N.lib().lb_set_register_cap(self._h, int(blocks)), "lb_set_register_cap")
+
     def set_bvh(self, width: int) -> None:
         """The BVH the warp kernels walk: 2 (the reference's) or 8 (8-wide, compressed). Same results."""
         N.check(N.lib().lb_set_bvh(self._h, int(width)), "lb_set_bvh")

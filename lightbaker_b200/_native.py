@@ -95,6 +95,7 @@ SIGNATURES = {
     "lb_set_bvh": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_set_refill": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_set_near": (C.c_int, [C.c_void_p, C.c_int]),
+    "lb_set_register_cap": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_get_counters": (C.c_int, [C.c_void_p, C.POINTER(Counters)]),
     "lb_gpu_stream": (C.c_void_p, [C.c_void_p]),
     "lb_gpu_sync": (C.c_int, [C.c_void_p]),

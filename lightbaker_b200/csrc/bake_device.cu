@@ -319,13 +319,15 @@ void autotune(lb_plan &p) {
     cudaEventCreate(&e1);
     const int orders[] = {8, 2, 0};
     struct Shape {
-        int bvh, refill, near;
+        int bvh, refill, near, occ;
     };
-    const Shape shapes[] = {{2, 0, 1}, {2, 0, 0}, {2, 1, 0}, {8, 0, 0}};
+    // walks (BVH2 with leaf lists, plain, with lane refill; the 8-wide BVH) and register caps
+    const Shape shapes[] = {{2, 0, 1, 0}, {2, 0, 1, 3}, {2, 0, 1, 4}, {2, 0, 0, 0}, {2, 0, 0, 3},
+                            {2, 0, 0, 4}, {2, 1, 0, 0}, {8, 0, 0, 0}};
     std::string report;
     for (int pass : {LB_PASS_DIRECT, LB_PASS_GATHER}) {
         float best = 1e30f;
-        int best_order = 8, best_blocks = 0, best_bvh = 2, best_refill = 0, best_near = 0;
+        int best_order = 8, best_blocks = 0, best_bvh = 2, best_refill = 0, best_near = 0, best_occ = 0;
         for (const Shape &sh : shapes)
         for (int order : orders) {
             if (pass == LB_PASS_GATHER && sh.near) continue;
@@ -333,6 +335,7 @@ void autotune(lb_plan &p) {
             probe.pass = pass;
             probe.sms = p.g->sms;
             probe.bvh = sh.bvh;
+            probe.occ = sh.occ;
             int full = lb_warp_pass_blocks(probe);
             int per_sm = std::max(1, full / std::max(1, p.g->sms));
             for (int bps = per_sm; bps >= 1; bps = bps > 1 ? std::max(1, bps / 2) : 0) {
@@ -353,6 +356,7 @@ void autotune(lb_plan &p) {
                 w.bvh = sh.bvh;
                 w.refill = sh.refill;
                 w.near = sh.near;
+                w.occ = sh.occ;
                 float t = 0;
                 for (int rep = 0; rep < 2; rep++) {
                     ck(cudaEventRecord(e0, st), "autotune");
@@ -368,6 +372,7 @@ void autotune(lb_plan &p) {
                     best_bvh = sh.bvh;
                     best_refill = sh.refill;
                     best_near = sh.near;
+                    best_occ = sh.occ;
                 }
                 if (bps == 1) break;
             }
@@ -378,14 +383,17 @@ void autotune(lb_plan &p) {
             p.bvh_direct = best_bvh;
             p.refill_direct = best_refill;
             p.near_direct = best_near;
+            p.occ_direct = best_occ;
         } else {
             p.group_gather = best_order;
             p.blocks_gather = best_blocks;
             p.bvh_gather = best_bvh;
             p.refill_gather = best_refill;
+            p.occ_gather = best_occ;
         }
         report += std::string(pass == LB_PASS_DIRECT ? "direct" : "gather") + ": bvh " + std::to_string(best_bvh) +
-                  ", refill " + std::to_string(best_refill) + ", near " + std::to_string(best_near) + ", order " + std::to_string(best_order) + ", " +
+                  ", refill " + std::to_string(best_refill) + ", near " + std::to_string(best_near) + ", order " +
+                  std::to_string(best_order) + ", register cap " + std::to_string(best_occ) + ", " +
                   std::to_string(best_blocks / std::max(1, p.g->sms)) + " blocks/SM (" + std::to_string(best) +
                   " ms on " + std::to_string(sample.size()) + " texels); ";
     }
@@ -429,6 +437,7 @@ void capture(lb_plan &p) {
             w.bvh = p.bvh_direct;
             w.refill = p.refill_direct;
             w.near = p.near_direct;
+            w.occ = p.occ_direct;
             ck(lb_launch_pass_warp(w, st), "direct pass");
         }
         ck(lb_post_direct(a, int(h.lightmap.padding) + 4, s, st), "direct texel passes");
@@ -453,6 +462,7 @@ void capture(lb_plan &p) {
             gw.group = p.group_gather;
             gw.bvh = p.bvh_gather;
             gw.refill = p.refill_gather;
+            gw.occ = p.occ_gather;
             ck(lb_launch_pass_warp(gw, st), "gather pass");
             ck(lb_post_bounce(a, p.gather_out.as<float4>(), int(b.gi_filter * p.ds), p.wr.as<float>(),
                               int(h.lightmap.padding + 2 * p.ds + 2), s, st),

@@ -40,6 +40,8 @@ struct WarpPass {
     int bvh;                  // 2: the reference's BVH2; 8: the 8-wide BVH (S->nodes8)
     int refill;               // BVH2 occlusion and gather rays: a lane starts the item's next ray when its own ends
     int near;                 // BVH2 occlusion rays: test a leaf list gathered once an item (lb_device.cuh)
+    int occ;                  // BVH2 direct and gather passes without counting: 3 or 4 caps registers so that
+                              // this many 256-thread blocks fit an SM; else the compiler's own budget
 };
 cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream);
 // The persistent grid's size for a pass: SMs x resident blocks of 256 threads.

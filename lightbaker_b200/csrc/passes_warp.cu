@@ -130,9 +130,9 @@ __device__ __forceinline__ void flush_counts(Count &c, unsigned long long *count
     }
 }
 
-// trace.wgsl:170-243
-template <int BVH, bool COUNT>
-__global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
+// trace.wgsl:170-243. OCC: blocks of 256 threads an SM must hold (the compiler's register budget).
+template <int BVH, bool COUNT, int OCC = 1>
+__global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
                                                    unsigned long long *counters, int group, int refill, int near) {
     __shared__ float s_term[WARPS][AO_CAP];
@@ -324,8 +324,8 @@ __global__ void __launch_bounds__(256) direct_warp(Scene S, lb_params P, const f
 }
 
 // trace.wgsl:245-270
-template <int BVH, bool COUNT>
-__global__ void __launch_bounds__(256) gather_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
+template <int BVH, bool COUNT, int OCC = 1>
+__global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const float4 *pos_override, const uint32_t *n_dev, uint32_t n_host,
                                                    uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
                                                    unsigned long long *counters, int group, int refill) {
@@ -519,29 +519,33 @@ __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const f
 
 }  // namespace lbd
 
-template <int BVH, bool COUNT> int blocks_for(int pass) {
+template <int BVH, bool COUNT, int OCC = 1> int blocks_for(int pass) {
     const int T = 256;
     int per_sm = 0;
     cudaError_t e;
     switch (pass) {
-    case LB_PASS_DIRECT: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::direct_warp<BVH, COUNT>, T, 0); break;
-    case LB_PASS_GATHER: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::gather_warp<BVH, COUNT>, T, 0); break;
+    case LB_PASS_DIRECT:
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::direct_warp<BVH, COUNT, OCC>, T, 0);
+        break;
+    case LB_PASS_GATHER:
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::gather_warp<BVH, COUNT, OCC>, T, 0);
+        break;
     default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::volume_warp<BVH, COUNT>, T, 0); break;
     }
     return (e != cudaSuccess || per_sm < 1) ? 1 : per_sm;
 }
 
-template <int BVH, bool COUNT> void launch(const WarpPass &w, int blocks, cudaStream_t stream) {
+template <int BVH, bool COUNT, int OCC = 1> void launch(const WarpPass &w, int blocks, cudaStream_t stream) {
     const int T = 256;
     switch (w.pass) {
     case LB_PASS_DIRECT:
-        lbd::direct_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base,
-                                                               w.out, w.counters, w.group, w.refill, w.near);
+        lbd::direct_warp<BVH, COUNT, OCC><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base,
+                                                                    w.out, w.counters, w.group, w.refill, w.near);
         break;
     case LB_PASS_GATHER:
-        lbd::gather_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host,
-                                                               w.base, w.light, w.n_light, w.out, w.counters, w.group,
-                                                               w.refill);
+        lbd::gather_warp<BVH, COUNT, OCC><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host,
+                                                                    w.base, w.light, w.n_light, w.out, w.counters,
+                                                                    w.group, w.refill);
         break;
     default:
         lbd::volume_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light, w.out,
@@ -550,8 +554,16 @@ template <int BVH, bool COUNT> void launch(const WarpPass &w, int blocks, cudaSt
     }
 }
 
+// the register-capped variants exist for the BVH2 walk without counting (the product's passes)
+static bool capped(const WarpPass &w) {
+    return w.bvh == 2 && !w.full_count && w.pass != LB_PASS_VOLUME && (w.occ == 3 || w.occ == 4);
+}
+
 int lb_warp_pass_blocks(const WarpPass &w) {
-    int per_sm = w.bvh == 8 ? (w.full_count ? blocks_for<8, true>(w.pass) : blocks_for<8, false>(w.pass))
+    int per_sm;
+    if (capped(w)) per_sm = w.occ == 3 ? blocks_for<2, false, 3>(w.pass) : blocks_for<2, false, 4>(w.pass);
+    else
+        per_sm = w.bvh == 8 ? (w.full_count ? blocks_for<8, true>(w.pass) : blocks_for<8, false>(w.pass))
                             : (w.full_count ? blocks_for<2, true>(w.pass) : blocks_for<2, false>(w.pass));
     return w.sms * per_sm;
 }
@@ -566,7 +578,10 @@ cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream) {
         if (need == 0) return cudaSuccess;
         if ((uint32_t)blocks > need) blocks = (int)need;
     }
-    if (w.bvh == 8) {
+    if (capped(w)) {
+        if (w.occ == 3) launch<2, false, 3>(w, blocks, stream);
+        else launch<2, false, 4>(w, blocks, stream);
+    } else if (w.bvh == 8) {
         if (w.full_count) launch<8, true>(w, blocks, stream);
         else launch<8, false>(w, blocks, stream);
     } else {

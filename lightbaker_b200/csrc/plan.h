@@ -94,6 +94,7 @@ struct lb_plan {
     int bvh_direct = 2, bvh_gather = 2, bvh_volume = 2;  // BVH width for the warp passes
     int refill_direct = 0, refill_gather = 0;          // lane refill for the warp passes
     int near_direct = 1;                               // leaf lists for the occlusion rays
+    int occ_direct = 0, occ_gather = 0;                // register caps (WarpPass::occ)
     std::string tuned;  // what the autotuner picked
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;

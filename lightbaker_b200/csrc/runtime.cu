@@ -289,6 +289,12 @@ int lb_set_near(lb_gpu *g, int on) {
     return LB_OK;
 }
 
+int lb_set_register_cap(lb_gpu *g, int blocks) {
+    if (!g || !(blocks == 0 || blocks == 3 || blocks == 4)) return LB_EINVAL;
+    g->occ = blocks;
+    return LB_OK;
+}
+
 int lb_set_refill(lb_gpu *g, int on) {
     if (!g) return LB_EINVAL;
     g->refill = on != 0;
@@ -347,6 +353,7 @@ int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const fl
         w.bvh = g->bvh;
         w.refill = g->refill;
         w.near = g->near;
+        w.occ = g->occ;
         LB_CUDA(lb_launch_pass_warp(w, g->stream), "pass launch");
     } else {
         LB_CUDA(lb_launch_pass_bvh2(pass, S, P, items, n, base, light, n_light, out, g->counters, g->counting,

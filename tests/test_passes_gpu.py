@@ -89,6 +89,38 @@ def test_passes_bit_exact(gpu, oracle_mod, name, limit, kernel, order, bvh, refi
     gpu.set_near(1)
 
 
+@pytest.mark.parametrize("cap,near", [(3, 1), (4, 1), (3, 0), (4, 0)])
+@pytest.mark.parametrize("name,limit", [("small_map", 12000), ("map_100m", 3000)])
+def test_register_capped_passes_bit_exact(gpu, oracle_mod, name, limit, cap, near):
+    """The register-capped warp kernels (their own instantiations, used without counting) give the oracle's
+    records too."""
+    scene = scenes.WORKLOADS[name]()
+    P = lb.prepare(scene)
+    buffers = gpu.scene(P.nodes, P.tris, P.materials, P.charts)
+    sc = oracle_mod.Scene.of(P)
+    rng = np.random.default_rng(2)
+    items = P.covered_texels()
+    items = items[np.sort(rng.choice(len(items), size=min(limit, len(items)), replace=False))]
+    gpu.set_pass_kernel(1)
+    gpu.set_ray_order(0, 0)
+    gpu.set_near(near)
+    gpu.set_register_cap(cap)
+    try:
+        g = gpu.run(lb.Pass.DIRECT, buffers, P.params, items)
+        c, _ = oracle_mod.run(0, sc, P.params, items)
+        _compare(g, c, f"{name} direct, cap {cap}")
+        light = _light_for(P, rng)
+        gi = items[: limit // 4]
+        g = gpu.run(lb.Pass.GATHER, buffers, P.params, gi, light)
+        c, _ = oracle_mod.run(1, sc, P.params, gi, light)
+        _compare(g, c, f"{name} gather, cap {cap}")
+    finally:
+        gpu.set_register_cap(0)
+        gpu.set_pass_kernel(0)
+        gpu.set_ray_order(8, 8)
+        gpu.set_near(1)
+
+
 def test_empty_and_edge_cases(gpu, oracle_mod):
     P = lb.prepare(scenes.small_map())
     buffers = gpu.scene(P.nodes, P.tris, P.materials, P.charts)
