@@ -195,10 +195,48 @@ def reference_arm(args):
         "e2e": {"value": value, "unit": "Grays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def adjoint_only(args):
+    """The transport's forward and backward alone on the workload, for a profiler: no flush."""
+    import torch
+    import lightbaker_b200 as lb
+    from lightbaker_b200 import scenes
+    scene = scenes.WORKLOADS[args.workload]()
+    gpu = lb.Gpu.new(0)
+    tr = lb.Transport(scene, gpu)
+    dev = torch.device("cuda", 0)
+    th = torch.from_numpy(tr.theta0()).to(dev)
+    out = torch.empty((tr.ih, tr.iw, 4), dtype=torch.float32, device=dev)
+    g_in = torch.rand((tr.ih, tr.iw, 4), dtype=torch.float32, device=dev)
+    g_th = torch.empty(tr.n_params, dtype=torch.float32, device=dev)
+    stream = torch.cuda.ExternalStream(gpu.stream, device=dev)
+    torch.cuda.synchronize()
+    res = {}
+    for name, fn in (("forward", lambda: tr.forward_async(th.data_ptr(), out.data_ptr())),
+                     ("backward", lambda: tr.backward_async(g_in.data_ptr(), g_th.data_ptr()))):
+        times = []
+        for i in range(args.warmup + args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+            fn()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            gpu.sync()
+            if i >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+        res[name + "_ms"] = statistics.median(times)
+    print(json.dumps({"kernel": "adjoint", "workload": args.workload, **res,
+                      "backward_over_forward": res["backward_ms"] / res["forward_ms"]}))
+    tr.close()
+    gpu.close()
+
+
 def kernel_only(args):
     """One pass kind alone over a slice of the workload's items, for a profiler: no flush, no bake."""
     import torch
     import lightbaker_b200 as lb
+    if args.kernel_only == "adjoint":
+        return adjoint_only(args)
     scene, P, direct, gather, probes, light = load_workload(args.workload, 0)
     items = (direct if args.kernel_only == "direct" else gather)[: args.items]
     gpu = lb.Gpu.new(0)
@@ -247,7 +285,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--kernel-only", choices=["direct", "gather"], default=None,
+    ap.add_argument("--device-only", action="store_true",
+                    help="time the device bake's steps and stop (for a profiler's launch list)")
+    ap.add_argument("--kernel-only", choices=["direct", "gather", "adjoint"], default=None,
                     help="run one warp-per-item pass over --items texels of the workload, warmup + steps times "
                          "(for profiler captures; prints its own line)")
     ap.add_argument("--items", type=int, default=262144)
@@ -313,6 +353,16 @@ def main():
     value = rays_step * world / (ms_per_step / 1e3) / 1e9
     baked = plan.result()
     plan.close()
+    if args.device_only:
+        # for a profiler's launch list: the device bake's steps alone
+        if rank == 0:
+            print(json.dumps({"metric": "Grays/s", "value": value, "unit": "Grays/s", "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                              "device_only": True, "autotune": tuning, "graph_kernels": kernels}))
+        gpu.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     # ---- the dominant kernels alone: the warp-per-item passes over the same items ----
     buffers = gpu.scene(P.nodes, P.tris, P.materials, P.charts)
@@ -386,6 +436,7 @@ def main():
         st = pb.stats
         plain = {"bake_seconds": pw, "grays_e2e": st.rays * world / pw / 1e9,
                  "grays_passes": st.rays / (st.t_direct + st.t_bounces + st.t_volume) / 1e9,
+                 "pass_seconds": st.t_direct + st.t_bounces + st.t_volume, "rays": int(st.rays),
                  "stages_s": {"layout_bvh": st.t_layout, "direct": st.t_direct, "bounces": st.t_bounces,
                               "volume": st.t_volume}}
         pb.close()
@@ -487,6 +538,8 @@ def main():
                        "bvh_nodes": int(P.info.n_nodes), "direct_texels": int(baked.stats.texels_baked),
                        "bounces": int(P.info.gi_bounces), "probes": int(len(probes)),
                        "rays_per_step": int(rays_step), "rays_direct_gather_volume": [int(r) for r in rays3],
+                       "rays_counted": "traced on the device; the gather rays of the first bounce only (later "
+                                       "bounces evaluate its recorded outcomes: same rays, same bits)",
                        "l2": "flushed before every step (256 MB write)",
                        "path": "device-resident bake, one CUDA graph, warp-per-item BVH2 passes",
                        "autotune": tuning,
@@ -507,7 +560,8 @@ def main():
                     "host_prepare_s": e2e_stats.t_layout},
             "plain": plain,
             "adjoint": adjoint,
-            "batched_vs_plain": (value / plain["grays_passes"]) if plain else None,
+            # the same bake (same outputs): the drop-in's pass seconds over the device step's seconds
+            "batched_vs_plain": (plain["pass_seconds"] / (ms_per_step / 1e3)) if plain else None,
             "gpu_launches": kernels * args.steps,
             "clocks": clock_info,
         }

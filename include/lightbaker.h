@@ -217,6 +217,9 @@ typedef struct lb_bake_options {
     void (*log)(void *ctx, const char *line);   /* NULL: quiet */
     void *log_ctx;
     int autotune;                               /* device bake: time the passes' shapes on a sample first */
+    int trace_every_bounce;                     /* device bake: trace the gather rays again in every bounce
+                                                 * (default 0: the first bounce records each ray's outcome
+                                                 * and later bounces evaluate the records; same results) */
 } lb_bake_options;
 
 typedef struct lb_bake lb_bake;

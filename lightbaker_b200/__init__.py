@@ -308,10 +308,11 @@ class Bake:
             pass
 
 
-def _options(cache, log, autotune=False):
+def _options(cache, log, autotune=False, trace_every_bounce=False):
     opts = N.BakeOptions()
     opts.cache_dir = str(cache).encode() if cache else None
     opts.autotune = int(bool(autotune))
+    opts.trace_every_bounce = int(bool(trace_every_bounce))
     keep = None
     if log is not None:
         keep = N.LOG_CB(lambda ctx, line: log(line.decode("utf-8", "replace")))
@@ -329,10 +330,11 @@ def bake(scene: bytes, gpu: Gpu, cache=None, log=None) -> Bake:
     return Bake(h)
 
 
-def bake_device(scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False) -> Bake:
+def bake_device(scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False, trace_every_bounce=False) -> Bake:
     """The device-resident bake: every dirty tile rebaked in one CUDA graph (same results as bake()).
-    autotune: time the passes' ray order and grid on a sample of the texels first (lb_bake_options)."""
-    opts, keep = _options(cache, log, autotune)
+    autotune: time the passes' ray order and grid on a sample of the texels first; trace_every_bounce:
+    trace the gather rays in every bounce instead of evaluating the first bounce's records (lb_bake_options)."""
+    opts, keep = _options(cache, log, autotune, trace_every_bounce)
     h = N.lib().lb_bake_device(gpu.handle, scene, len(scene), C.byref(opts))
     del keep
     if not h:
@@ -344,8 +346,8 @@ class Plan:
     """A device bake in steps: the host work and the graph once (`Plan(scene, gpu)`), then `launch()`
     (the graph enqueued on gpu.stream; repeatable), `rays()`, `result()`."""
 
-    def __init__(self, scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False):
-        self._opts, self._keep = _options(cache, log, autotune)
+    def __init__(self, scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False, trace_every_bounce=False):
+        self._opts, self._keep = _options(cache, log, autotune, trace_every_bounce)
         self._h = N.lib().lb_plan_create(gpu.handle, scene, len(scene), C.byref(self._opts))
         if not self._h:
             raise LightbakerError(N.last_error())

@@ -76,7 +76,8 @@ class Tracer(C.Structure):
 
 
 class BakeOptions(C.Structure):
-    _fields_ = [("cache_dir", C.c_char_p), ("log", LOG_CB), ("log_ctx", C.c_void_p), ("autotune", C.c_int)]
+    _fields_ = [("cache_dir", C.c_char_p), ("log", LOG_CB), ("log_ctx", C.c_void_p), ("autotune", C.c_int),
+                ("trace_every_bounce", C.c_int)]
 
 
 # every exported entry point: name -> (restype, argtypes)

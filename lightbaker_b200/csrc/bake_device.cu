@@ -150,6 +150,22 @@ void build(lb_plan &p) {
             cov_idx.push_back(i);
         }
     p.n_cov = uint32_t(cov_idx.size());
+    // at most one gathered texel a chart in each ds x ds block (bake.rs:286-297): the gather records' bound
+    p.max_gathered = 0;
+    for (size_t wi = 0; wi < p.dirty.size(); wi++) {
+        const DTile &t = p.tiles_all[wi];
+        std::vector<uint64_t> keys;
+        for (uint32_t y = 0; y < t.h; y++)
+            for (uint32_t x = 0; x < t.w; x++) {
+                const lb_texel &tx = tex[t.off + y * t.w + x];
+                if (!lb::covered(tx)) continue;
+                uint32_t chart;
+                std::memcpy(&chart, &tx.normal[3], 4);
+                keys.push_back((uint64_t((y / p.ds) * ((t.w + p.ds - 1) / p.ds) + x / p.ds) << 32) | chart);
+            }
+        std::sort(keys.begin(), keys.end());
+        p.max_gathered += uint64_t(std::unique(keys.begin(), keys.end()) - keys.begin());
+    }
 
     // cached tiles' light, the atlas owner map and the atlas the first bounce reads
     std::vector<uint8_t> known(p.n_all, 0), state(p.n_all, 0);
@@ -264,6 +280,15 @@ void build(lb_plan &p) {
     p.has.alloc(size_t(p.iw) * p.ih);
     p.has_b.alloc(size_t(p.iw) * p.ih);
     p.counters.alloc(12 * 8);
+    // the first bounce's gather records, which the later bounces evaluate instead of tracing again (their
+    // rays are the first bounce's: the keys depend on the gathered texel, not the bounce), and theta at the
+    // scene's own values for that evaluation
+    std::vector<float> theta;
+    for (auto &m : h.materials) theta.insert(theta.end(), m.albedo.begin(), m.albedo.end());
+    for (auto *c : {&h.sky.zenith, &h.sky.horizon, &h.sky.ground}) theta.insert(theta.end(), c->begin(), c->end());
+    theta.push_back(1.0f);
+    p.theta0.alloc(theta.size() * 4);
+    p.records.alloc(p.reuse && b.gi_bounces > 1 ? p.max_gathered * p.P.params.counts[2] * 8 : 16);
 
     cudaStream_t st = p.g->stream;
     auto up = [&](DBuf &d, const void *src, size_t bytes) {
@@ -272,6 +297,7 @@ void build(lb_plan &p) {
             p.g->h2d += bytes;
         }
     };
+    up(p.theta0, theta.data(), theta.size() * 4);
     up(p.tiles_d, p.tiles_all.data(), p.tiles_all.size() * sizeof(DTile));
     up(p.tex, tex.data(), tex.size() * 64);
     up(p.cov_idx, cov_idx.data(), cov_idx.size() * 4);
@@ -463,7 +489,18 @@ void capture(lb_plan &p) {
             gw.bvh = p.bvh_gather;
             gw.refill = p.refill_gather;
             gw.occ = p.occ_gather;
-            ck(lb_launch_pass_warp(gw, st), "gather pass");
+            bool replay = p.reuse && b.gi_bounces > 1;
+            if (replay && bounce > 0) {
+                // the same rays met the same surfaces: evaluate the first bounce's records against this
+                // bounce's atlas (the sums in ray order, as the pass sums them)
+                ck(lb_eval_records(p.records.as<uint2>(), p.gath_count.as<uint32_t>(), 0, params.counts[2],
+                                   p.light.as<float4>(), p.aw * p.ah, p.theta0.as<float>(),
+                                   uint32_t(h.materials.size()), p.gather_out.as<float4>(), p.g->sms, st),
+                   "gather records");
+            } else {
+                gw.rec = replay ? p.records.as<uint2>() : nullptr;
+                ck(lb_launch_pass_warp(gw, st), "gather pass");
+            }
             ck(lb_post_bounce(a, p.gather_out.as<float4>(), int(b.gi_filter * p.ds), p.wr.as<float>(),
                               int(h.lightmap.padding + 2 * p.ds + 2), s, st),
                "bounce texel passes");
@@ -565,6 +602,7 @@ lb_plan *lb_plan_create(lb_gpu *g, const uint8_t *scene, size_t len, const lb_ba
             p->opt.log = [fn, ctx](const std::string &s) { fn(ctx, s.c_str()); };
         }
         p->autotune = opts && opts->autotune;
+        p->reuse = !(opts && opts->trace_every_bounce);
         p->group_direct = g->group_direct;
         p->group_gather = g->group_gather;
         p->bvh_direct = p->bvh_gather = p->bvh_volume = g->bvh;

@@ -569,6 +569,29 @@ __device__ __forceinline__ Hit walk(const Scene &S, float3 o, float3 d, float tm
     return trace<COUNT>(S, o, d, tmax, any, ray, seed, c);
 }
 
+// A gather ray's outcome, all a bounce needs to evaluate it again against another light atlas:
+// x = kind << 30 | material; y = the direction's y (sky, as bits) or the atlas texel the hit reads
+// (surface; 0xffffffff when it reads none and takes the fallback), as bounced() finds it.
+constexpr uint32_t KIND_SKY = 0u, KIND_BACK = 1u, KIND_SURFACE = 2u;
+__device__ __forceinline__ uint2 gather_record(const Scene &S, const lb_params &P, uint32_t n_light, float3 o,
+                                               float3 d, const Hit &h) {
+    if (h.tri == NONE) return make_uint2(KIND_SKY << 30, __float_as_uint(d.y));
+    if (h.back) return make_uint2(KIND_BACK << 30, 0u);
+    float4 v0 = __ldg(&S.tris[3 * h.tri]), e1 = __ldg(&S.tris[3 * h.tri + 1]);
+    uint32_t m = __float_as_uint(v0.w), ch = __float_as_uint(e1.w), li = NONE;
+    if (ch != NONE && ch < S.n_charts) {
+        float3 p = add(o, scl(d, h.t));
+        float4 r0 = __ldg(&S.charts[2 * ch]), r1 = __ldg(&S.charts[2 * ch + 1]);
+        float x = r0.x * p.x + r0.y * p.y + r0.z * p.z + r0.w * 1.0f;
+        float y = r1.x * p.x + r1.y * p.y + r1.z * p.z + r1.w * 1.0f;
+        int ix = min(max(int(floorf(x)), 0), int(P.atlas[0]) - 1);
+        int iy = min(max(int(floorf(y)), 0), int(P.atlas[1]) - 1);
+        uint32_t l = uint32_t(iy) * P.atlas[0] + uint32_t(ix);
+        if (l < n_light) li = l;
+    }
+    return make_uint2((KIND_SURFACE << 30) | min(m, 0x3fffffffu), li);
+}
+
 // trace.wgsl:133-148
 __device__ __forceinline__ float3 bounced(const Scene &S, const lb_params &P, const float4 *light, uint32_t n_light,
                                           float3 o, float3 d, const Hit &h) {

@@ -42,7 +42,14 @@ struct WarpPass {
     int near;                 // BVH2 occlusion rays: test a leaf list gathered once an item (lb_device.cuh)
     int occ;                  // BVH2 direct and gather passes without counting: 3 or 4 caps registers so that
                               // this many 256-thread blocks fit an SM; else the compiler's own budget
+    uint2 *rec;               // optional (gather): every ray's outcome, [item][ray] (lb_device.cuh gather_record)
 };
+// The gather records evaluated against a light atlas and theta (albedo 3 a material, zenith, horizon,
+// ground, sun scale; transport.cu): each item's gather result, its terms summed in ray order, equal to
+// what the gather pass gives for the same light.
+cudaError_t lb_eval_records(const uint2 *rec, const uint32_t *n_dev, uint32_t n_host, uint32_t rays,
+                            const float4 *light, uint32_t n_light, const float *theta, uint32_t n_mats, float4 *out,
+                            int sms, cudaStream_t stream);
 cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream);
 // The persistent grid's size for a pass: SMs x resident blocks of 256 threads.
 int lb_warp_pass_blocks(const WarpPass &w);

@@ -323,12 +323,12 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
     flush_counts<COUNT>(c, counters);
 }
 
-// trace.wgsl:245-270
+// trace.wgsl:245-270. rec (optional): each ray's outcome ([item][ray], gather_record) for later bounces.
 template <int BVH, bool COUNT, int OCC = 1>
 __global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const float4 *pos_override, const uint32_t *n_dev, uint32_t n_host,
                                                    uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
-                                                   unsigned long long *counters, int group, int refill) {
+                                                   unsigned long long *counters, int group, int refill, uint2 *rec) {
     __shared__ float3 s_term[WARPS][GI_CAP];
     __shared__ uint8_t s_on[WARPS][GI_CAP];
     const int lane = threadIdx.x & 31;
@@ -379,6 +379,7 @@ __global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, co
                     } else term = bounced(S, P, light, n_light, wk.o, wk.d, wk.hit);
                     s_term[w][r] = term;
                     s_on[w][r] = on;
+                    if (rec) rec[size_t(k) * rays + r] = gather_record(S, P, n_light, wk.o, wk.d, wk.hit);
                 }
                 unsigned fm = __ballot_sync(FULL, fin);
                 if (fin) {
@@ -418,6 +419,7 @@ __global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, co
                     term = bounced(S, P, light, n_light, o, d, h);
                     on = true;
                 }
+                if (rec) rec[size_t(k) * rays + r] = gather_record(S, P, n_light, o, d, h);
             }
             if (ord.grouped) {
                 s_term[w][r] = term;
@@ -545,7 +547,7 @@ template <int BVH, bool COUNT, int OCC = 1> void launch(const WarpPass &w, int b
     case LB_PASS_GATHER:
         lbd::gather_warp<BVH, COUNT, OCC><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host,
                                                                     w.base, w.light, w.n_light, w.out, w.counters,
-                                                                    w.group, w.refill);
+                                                                    w.group, w.refill, w.rec);
         break;
     default:
         lbd::volume_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light, w.out,

@@ -95,6 +95,9 @@ struct lb_plan {
     int refill_direct = 0, refill_gather = 0;          // lane refill for the warp passes
     int near_direct = 1;                               // leaf lists for the occlusion rays
     int occ_direct = 0, occ_gather = 0;                // register caps (WarpPass::occ)
+    bool reuse = true;          // later bounces evaluate the first bounce's gather records
+    uint64_t max_gathered = 0;  // a bound on the gathered texels (records are sized by it)
+    lbplan::DBuf records, theta0;
     std::string tuned;  // what the autotuner picked
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;

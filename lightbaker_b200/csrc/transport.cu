@@ -58,30 +58,7 @@ struct Theta {
     }
 };
 
-constexpr uint32_t KIND_SKY = 0u, KIND_BACK = 1u, KIND_SURFACE = 2u;
 constexpr uint32_t LIT_NONE = 0xffffffffu, UNLIT = 0xfffffffeu;
-
-// A gather ray's outcome: x = kind << 30 | material; y = the direction's y (sky, as bits) or the atlas
-// texel the hit reads (surface; 0xffffffff when it reads none and takes the fallback).
-__device__ __forceinline__ uint2 gather_record(const Scene &S, const lb_params &P, uint32_t n_light, float3 o,
-                                               float3 d, const Hit &h) {
-    if (h.tri == NONE) return make_uint2(KIND_SKY << 30, __float_as_uint(d.y));
-    if (h.back) return make_uint2(KIND_BACK << 30, 0u);
-    float4 v0 = __ldg(&S.tris[3 * h.tri]), e1 = __ldg(&S.tris[3 * h.tri + 1]);
-    uint32_t m = __float_as_uint(v0.w), ch = __float_as_uint(e1.w), li = NONE;
-    // bounced (trace.wgsl:133-148): the chart's atlas texel under the hit point
-    if (ch != NONE && ch < S.n_charts) {
-        float3 p = add(o, scl(d, h.t));
-        float4 r0 = __ldg(&S.charts[2 * ch]), r1 = __ldg(&S.charts[2 * ch + 1]);
-        float x = r0.x * p.x + r0.y * p.y + r0.z * p.z + r0.w * 1.0f;
-        float y = r1.x * p.x + r1.y * p.y + r1.z * p.z + r1.w * 1.0f;
-        int ix = min(max(int(floorf(x)), 0), int(P.atlas[0]) - 1);
-        int iy = min(max(int(floorf(y)), 0), int(P.atlas[1]) - 1);
-        uint32_t l = uint32_t(iy) * P.atlas[0] + uint32_t(ix);
-        if (l < n_light) li = l;
-    }
-    return make_uint2((KIND_SURFACE << 30) | min(m, 0x3fffffffu), li);
-}
 
 // The gather pass's rays (trace.wgsl:245-270) for the gathered texels, each ray's outcome recorded
 // ([item][ray]); a thread a ray.
@@ -112,10 +89,11 @@ __global__ void k_records(Scene S, lb_params P, const float4 *tex, const uint32_
 
 // The records against the light and theta: each gathered texel's gather result, its terms summed in ray
 // order as the gather pass sums them (trace.wgsl:258-269); a warp an item.
-__global__ void k_eval(const uint2 *rec, uint32_t n, uint32_t rays, const float4 *light, uint32_t n_light, Theta th,
-                       float4 *out) {
+__global__ void k_eval(const uint2 *rec, const uint32_t *n_dev, uint32_t n_host, uint32_t rays, const float4 *light,
+                       uint32_t n_light, Theta th, float4 *out) {
     const int lane = threadIdx.x & 31;
     uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t n = n_dev ? *n_dev : n_host;
     float frays = __uint2float_rn(rays);
     float3 zen = th.zenith(), hor = th.horizon(), gro = th.ground(), fb = th.fallback();
     for (uint32_t k = warp; k < n; k += warps) {
@@ -274,23 +252,33 @@ __device__ __forceinline__ int flagged_around(const uint8_t *was, uint32_t i, ui
     return n;
 }
 
-// one dilation pass (bake.rs:394-421) transposed
-__global__ void k_dilate_t(const uint8_t *was, const float4 *g_out, float4 *g_in, uint32_t iw, uint32_t ih) {
+// A texel's part in one dilation pass (bake.rs:394-421), from the pass's starting flags: 0x80 flagged, else
+// the flagged neighbours it averages (0: none, it keeps its value)
+__global__ void k_dilate_plan(const uint8_t *was, uint8_t *plan, uint32_t iw, uint32_t ih) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= iw * ih) return;
+    plan[i] = was[i] ? 0x80 : uint8_t(flagged_around(was, i, iw, ih));
+}
+
+// one dilation pass transposed
+__global__ void k_dilate_t(const uint8_t *plan, const float4 *g_out, float4 *g_in, uint32_t iw, uint32_t ih) {
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= iw * ih) return;
     float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (was[j]) {
+    uint8_t pj = plan[j];
+    if (pj & 0x80) {
         g = g_out[j];
         uint32_t x = j % iw, y = j / iw;
         for (uint32_t yy = y > 0 ? y - 1 : 0; yy < min(y + 2, ih); yy++)
             for (uint32_t xx = x > 0 ? x - 1 : 0; xx < min(x + 2, iw); xx++) {
                 uint32_t i = yy * iw + xx;
-                if (was[i]) continue;
-                float f = float(flagged_around(was, i, iw, ih));
+                uint8_t pi = plan[i];
+                if (pi & 0x80) continue;
+                float f = float(pi);
                 float4 go = g_out[i];
                 g.x += go.x / f, g.y += go.y / f, g.z += go.z / f;
             }
-    } else if (flagged_around(was, j, iw, ih) == 0) {
+    } else if (pj == 0) {
         g = g_out[j];
     }
     g_in[j] = g;
@@ -328,41 +316,46 @@ __device__ __forceinline__ int fill_mode(const PostArgs &a, const DTile &t, cons
     return 0;
 }
 
-// one fill ring's flags alone
-__global__ void k_fill_mask(PostArgs a, const uint8_t *was, uint8_t *now) {
+// A texel's part in one fill ring, from the ring's starting flags: 0x80 flagged; else mode << 4 | n
+// (fill_mode), and its flag for the next ring
+__global__ void k_fill_plan(PostArgs a, const uint8_t *was, uint8_t *plan, uint8_t *now) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n_texels) return;
-    uint8_t k = was[i];
-    if (!k) {
-        const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, i)];
-        int li = int(i - t.off), n;
-        k = fill_mode(a, t, was, i, li % int(t.w), li / int(t.w), n) != 0;
+    if (was[i]) {
+        plan[i] = 0x80;
+        now[i] = 1;
+        return;
     }
-    now[i] = k;
+    const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, i)];
+    int li = int(i - t.off), n;
+    int mode = fill_mode(a, t, was, i, li % int(t.w), li / int(t.w), n);
+    plan[i] = uint8_t((mode << 4) | n);
+    now[i] = mode != 0;
 }
 
-// one fill ring transposed, given the ring's starting flags
-__global__ void k_fill_t(PostArgs a, const uint8_t *was, const float4 *g_out, float4 *g_in) {
+// one fill ring transposed
+__global__ void k_fill_t(PostArgs a, const uint8_t *plan, const float4 *g_out, float4 *g_in) {
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= a.n_texels) return;
-    const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, j)];
-    int lj = int(j - t.off), x = lj % int(t.w), y = lj / int(t.w);
     float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
-    int n;
-    if (was[j]) {
+    uint8_t pj = plan[j];
+    if (pj & 0x80) {
         g = g_out[j];
+        const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, j)];
+        int lj = int(j - t.off), x = lj % int(t.w), y = lj / int(t.w);
+        uint32_t cj = a.chart[j];
         for (int yy = y > 0 ? y - 1 : 0; yy < min(y + 2, int(t.h)); yy++)
             for (int xx = x > 0 ? x - 1 : 0; xx < min(x + 2, int(t.w)); xx++) {
                 uint32_t i = t.off + uint32_t(yy) * t.w + uint32_t(xx);
-                if (was[i]) continue;
-                int mode = fill_mode(a, t, was, i, xx, yy, n);
-                if (mode == 2 || (mode == 1 && a.chart[j] == a.chart[i])) {
+                uint8_t pi = plan[i];
+                int mode = (pi & 0x80) ? 0 : pi >> 4;
+                if (mode == 2 || (mode == 1 && cj == a.chart[i])) {
                     float4 go = g_out[i];
-                    float f = float(n);
+                    float f = float(pi & 15);
                     g.x += go.x / f, g.y += go.y / f, g.z += go.z / f;
                 }
             }
-    } else if (fill_mode(a, t, was, j, x, y, n) == 0) {
+    } else if ((pj >> 4) == 0) {
         g = g_out[j];
     }
     g_in[j] = g;
@@ -574,6 +567,13 @@ __global__ void k_theta_final(const PartialSet *sets, int n_sets, int blocks, co
 
 }  // namespace lbd
 
+cudaError_t lb_eval_records(const uint2 *rec, const uint32_t *n_dev, uint32_t n_host, uint32_t rays,
+                            const float4 *light, uint32_t n_light, const float *theta, uint32_t n_mats, float4 *out,
+                            int sms, cudaStream_t stream) {
+    lbd::k_eval<<<sms * 8, 256, 0, stream>>>(rec, n_dev, n_host, rays, light, n_light, lbd::Theta{theta, n_mats}, out);
+    return cudaGetLastError();
+}
+
 namespace {
 
 inline dim3 tg(uint64_t n) { return dim3(uint32_t((n + 255) / 256)); }
@@ -614,9 +614,9 @@ namespace {
 
 // the bounces' light after bounce b of the forward: res, filters, write (the atlas rewritten in place)
 void bounce(lb_transport &t, float4 *light, uint32_t b, float4 *next, cudaStream_t st, float4 **filled) {
-    lbd::k_eval<<<t.g->sms * 8, 256, 0, st>>>(t.rec.as<uint2>(), t.n_gath, t.rays, light, t.n_light, t.th(),
-                                             t.res.as<float4>());
-    ck(cudaGetLastError(), "transport eval");
+    ck(lb_eval_records(t.rec.as<uint2>(), nullptr, t.n_gath, t.rays, light, t.n_light, t.theta.as<float>(), t.M,
+                       t.res.as<float4>(), t.g->sms, st),
+       "transport eval");
     ck(lb_bounce_filters(t.a, t.res.as<float4>(), t.r, t.plan->wr.as<float>(), t.rings, t.fk_a.as<uint8_t>(),
                          t.fk_b.as<uint8_t>(), t.e0.as<float4>(), t.e1.as<float4>(), filled, st),
        "transport filters");
@@ -794,15 +794,21 @@ void build(lb_transport &t, uint32_t max_checkpoints) {
         ck(cudaMemcpyAsync(t.dl0.p, p.dl.p, size_t(t.n_tex) * 16, cudaMemcpyDeviceToDevice, st), "dl0");
         ck(cudaMemcpyAsync(t.fixed_ind.p, p.ind.p, size_t(t.n_tex) * 16, cudaMemcpyDeviceToDevice, st), "ind");
     }
-    // the bounce fill's flags ring by ring, the smoothing's weight sums
-    t.masks.alloc(size_t(t.rings + 1) * N);
+    // the bounce fill's plan ring by ring (from the gathered flags on), the smoothing's weight sums
+    t.masks.alloc(size_t(std::max(t.rings, 1)) * N);
     t.wsum.alloc(N * 4);
     if (t.n_tex) {
-        ck(cudaMemcpyAsync(t.masks.p, p.gathered.p, t.n_tex, cudaMemcpyDeviceToDevice, st), "masks");
-        for (int q = 0; q < t.rings; q++)
-            lbd::k_fill_mask<<<tg(t.n_tex), 256, 0, st>>>(t.a, t.masks.as<uint8_t>() + size_t(q) * t.n_tex,
-                                                          t.masks.as<uint8_t>() + size_t(q + 1) * t.n_tex);
+        DBuf fa, fb;
+        fa.alloc(N);
+        fb.alloc(N);
+        ck(cudaMemcpyAsync(fa.p, p.gathered.p, t.n_tex, cudaMemcpyDeviceToDevice, st), "fill flags");
+        uint8_t *was = fa.as<uint8_t>(), *now = fb.as<uint8_t>();
+        for (int q = 0; q < t.rings; q++) {
+            lbd::k_fill_plan<<<tg(t.n_tex), 256, 0, st>>>(t.a, was, t.masks.as<uint8_t>() + size_t(q) * t.n_tex, now);
+            std::swap(was, now);
+        }
         lbd::k_smooth_wsum<<<tg(t.n_tex), 256, 0, st>>>(t.a, t.r, p.wr.as<float>(), t.wsum.as<float>());
+        ck(cudaStreamSynchronize(st), "fill plan");
     }
     // the composite's arguments (its outputs in the transport's own arrays) and its dilation flags
     uint64_t nb = uint64_t(t.iw) * t.ih;
@@ -828,17 +834,23 @@ void build(lb_transport &t, uint32_t max_checkpoints) {
     t.c.validity = t.out_validity.as<uint8_t>();
     t.c.indirect = t.out_atlas.as<float4>();
     t.c.has = t.out_has.as<uint8_t>();
-    // has0: the composite's own flags (before its dilations), from the bake's indirect through one run
+    // the dilations' plans: from the composite's own flags (its block averages alone, run once), then
+    // the first pass's
     t.has0.alloc(nb);
     t.has1.alloc(nb);
-    {
+    if (nb) {
+        DBuf f0, f1;
+        f0.alloc(nb);
+        f1.alloc(nb);
         CompositeArgs c0 = t.c;
         c0.ind = p.ind.as<float4>();
-        c0.has = t.has0.as<uint8_t>();
+        c0.has = f0.as<uint8_t>();
         c0.indirect = t.out_tmp.as<float4>();
-        // composite alone (no dilation): its flags are has0
         ck(lb_composite_blocks(c0, st), "composite flags");
-        if (nb) lbd::k_dilate_mask<<<tg(nb), 256, 0, st>>>(t.has0.as<uint8_t>(), t.has1.as<uint8_t>(), t.iw, t.ih);
+        lbd::k_dilate_plan<<<tg(nb), 256, 0, st>>>(f0.as<uint8_t>(), t.has0.as<uint8_t>(), t.iw, t.ih);
+        lbd::k_dilate_mask<<<tg(nb), 256, 0, st>>>(f0.as<uint8_t>(), f1.as<uint8_t>(), t.iw, t.ih);
+        lbd::k_dilate_plan<<<tg(nb), 256, 0, st>>>(f1.as<uint8_t>(), t.has1.as<uint8_t>(), t.iw, t.ih);
+        ck(cudaStreamSynchronize(st), "dilation plan");
     }
     // every gather ray's outcome
     t.rec.alloc(t.n_rec * 8);

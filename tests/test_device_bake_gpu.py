@@ -31,9 +31,15 @@ def test_device_bake_equals_drop_in(gpu, name):
     dev = lb.bake_device(s, gpu)
     same(dev, plain)
     assert dev.stats.rays_direct == plain.stats.rays_direct
-    assert dev.stats.rays_gather == plain.stats.rays_gather
+    # later bounces evaluate the first bounce's records: only its gather rays are traced
+    bounces = lb.prepare(s).info.gi_bounces
+    assert dev.stats.rays_gather * bounces == plain.stats.rays_gather
     assert dev.stats.rays_volume == plain.stats.rays_volume
     assert dev.stats.tiles_baked == plain.stats.tiles_baked
+    # tracing every bounce again gives the same bits and the drop-in's ray count
+    again = lb.bake_device(s, gpu, trace_every_bounce=True)
+    same(again, plain)
+    assert again.stats.rays_gather == plain.stats.rays_gather
 
 
 def test_uneven_tiles_in_one_graph(gpu):
@@ -46,7 +52,7 @@ def test_uneven_tiles_in_one_graph(gpu):
     plain = lb.bake(s, gpu)
     dev = lb.bake_device(s, gpu, autotune=True)
     same(dev, plain)
-    assert dev.stats.rays_gather == plain.stats.rays_gather and dev.stats.tiles_baked == len(areas)
+    assert dev.stats.rays_gather * 2 == plain.stats.rays_gather and dev.stats.tiles_baked == len(areas)
 
 
 def test_autotuned_device_bake_equals_drop_in(gpu):
