@@ -288,7 +288,8 @@ void build(lb_plan &p) {
     for (auto *c : {&h.sky.zenith, &h.sky.horizon, &h.sky.ground}) theta.insert(theta.end(), c->begin(), c->end());
     theta.push_back(1.0f);
     p.theta0.alloc(theta.size() * 4);
-    p.records.alloc(p.reuse && b.gi_bounces > 1 ? p.max_gathered * p.P.params.counts[2] * 8 : 16);
+    bool recording = (p.reuse && b.gi_bounces > 1) || (p.keep_records && b.gi_bounces > 0);
+    p.records.alloc(recording ? p.max_gathered * p.P.params.counts[2] * 8 : 16);
 
     cudaStream_t st = p.g->stream;
     auto up = [&](DBuf &d, const void *src, size_t bytes) {
@@ -489,7 +490,7 @@ void capture(lb_plan &p) {
             gw.bvh = p.bvh_gather;
             gw.refill = p.refill_gather;
             gw.occ = p.occ_gather;
-            bool replay = p.reuse && b.gi_bounces > 1;
+            bool replay = p.reuse && b.gi_bounces > 1, record = replay || p.keep_records;
             if (replay && bounce > 0) {
                 // the same rays met the same surfaces: evaluate the first bounce's records against this
                 // bounce's atlas (the sums in ray order, as the pass sums them)
@@ -498,7 +499,7 @@ void capture(lb_plan &p) {
                                    uint32_t(h.materials.size()), p.gather_out.as<float4>(), p.g->sms, st),
                    "gather records");
             } else {
-                gw.rec = replay ? p.records.as<uint2>() : nullptr;
+                gw.rec = record && bounce == 0 ? p.records.as<uint2>() : nullptr;
                 ck(lb_launch_pass_warp(gw, st), "gather pass");
             }
             ck(lb_post_bounce(a, p.gather_out.as<float4>(), int(b.gi_filter * p.ds), p.wr.as<float>(),
@@ -581,11 +582,7 @@ template <class T> std::vector<T> down(lb_plan &p, const DBuf &d, size_t n, size
     return v;
 }
 
-}  // namespace
-
-extern "C" {
-
-lb_plan *lb_plan_create(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_options *opts) {
+lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_options *opts, bool keep_records) {
     if (!g || !scene) {
         lb_set_error("lb_plan_create: bad arguments");
         return nullptr;
@@ -603,11 +600,13 @@ lb_plan *lb_plan_create(lb_gpu *g, const uint8_t *scene, size_t len, const lb_ba
         }
         p->autotune = opts && opts->autotune;
         p->reuse = !(opts && opts->trace_every_bounce);
+        p->keep_records = keep_records;
         p->group_direct = g->group_direct;
         p->group_gather = g->group_gather;
         p->bvh_direct = p->bvh_gather = p->bvh_volume = g->bvh;
         p->refill_direct = p->refill_gather = g->refill;
         p->near_direct = g->near;
+        p->occ_direct = p->occ_gather = g->occ;
         build(*p);
         if (p->autotune) autotune(*p);
         capture(*p);
@@ -620,6 +619,19 @@ lb_plan *lb_plan_create(lb_gpu *g, const uint8_t *scene, size_t len, const lb_ba
         lb_set_error(e.what());
     }
     return nullptr;
+}
+
+}  // namespace
+
+lb_plan *lb_plan_create_recording(lb_gpu *g, const uint8_t *scene, size_t len) {
+    lb_bake_options o{};
+    return create_plan(g, scene, len, &o, true);
+}
+
+extern "C" {
+
+lb_plan *lb_plan_create(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_options *opts) {
+    return create_plan(g, scene, len, opts, false);
 }
 
 int lb_plan_launch(lb_plan *p) {

@@ -316,11 +316,12 @@ __device__ __forceinline__ float box_front(float3 o, float3 n, float4 mn, float4
     return (x - o.x) * n.x + (y - o.y) * n.y + (z - o.z) * n.z;
 }
 
-// Warp-wide: the leaves within reach r of o on the n side (by a margin), into list, nearest first.
-// Returns their count, or -1 when a level or the list would overflow. All lanes return the same value.
+// Warp-wide: the leaves within reach r of o on the n side (by a margin), into list, nearest first, with
+// their boxes' squared distances from o in dist2. Returns their count, or -1 when a level or the list would
+// overflow. All lanes return the same value.
 template <bool COUNT>
 __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float3 n, uint32_t *fa, uint32_t *fb,
-                                        uint32_t *list, int lane, Count &c) {
+                                        uint32_t *list, float *dist2, int lane, Count &c) {
     const unsigned FULLM = 0xffffffffu;
     float rr = r * 1.0001f + 1e-5f, r2 = rr * rr, margin = -(r * 1e-3f + 1e-4f);
     float4 rlo = __ldg(&S.nodes[0]), rhi = __ldg(&S.nodes[1]);
@@ -378,6 +379,7 @@ __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float
     __syncwarp();
     uint32_t mine[BALL_LEAVES / 32];
     int rank[BALL_LEAVES / 32];
+    float mykey[BALL_LEAVES / 32];
     for (int q = 0; q < BALL_LEAVES / 32; q++) {
         int i = q * 32 + lane;
         rank[q] = -1;
@@ -390,11 +392,15 @@ __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float
             }
             rank[q] = rk;
             mine[q] = list[i];
+            mykey[q] = ki;
         }
     }
     __syncwarp();
     for (int q = 0; q < BALL_LEAVES / 32; q++)
-        if (rank[q] >= 0) fa[rank[q]] = mine[q];
+        if (rank[q] >= 0) {
+            fa[rank[q]] = mine[q];
+            dist2[rank[q]] = mykey[q];
+        }
     __syncwarp();
     for (int i = lane; i < nl; i += 32) list[i] = fa[i];
     __syncwarp();
@@ -402,16 +408,21 @@ __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float
 }
 
 // trace() over a leaf list: the nearest accepted hit within tmax among the listed leaves' triangles,
-// with the walk's box test (culled by the nearest hit so far) and triangle test.
+// with the walk's box test (culled by the nearest hit so far) and triangle test. The list is nearest
+// first from the ray's origin (dist2: each box's squared distance from it), so once a box lies farther
+// than the nearest hit so far (by a relative margin far above the rounding of t, |d| and the distance),
+// neither it nor any later box can hold a nearer hit and the walk ends: the same hit as the whole list.
 template <bool COUNT>
-__device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, int nl, float3 o, float3 d, float tmax,
-                                          uint32_t ray, uint32_t seed, Count &c) {
+__device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, const float *dist2, int nl, float3 o,
+                                          float3 d, float tmax, uint32_t ray, uint32_t seed, Count &c) {
     Hit hit{tmax, NONE, false};
     c.rays++;
     float3 dd = mk(fabsf(d.x) < 1e-12f ? 1e-12f : d.x, fabsf(d.y) < 1e-12f ? 1e-12f : d.y,
                    fabsf(d.z) < 1e-12f ? 1e-12f : d.z);
     float3 inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+    float lim = tmax * 1.0001f + 1e-5f, lim2 = lim * lim;
     for (int k = 0; k < nl; k++) {
+        if (dist2[k] > lim2) break;
         uint32_t node = list[k];
         float4 lo = __ldg(&S.nodes[2 * node]), hi = __ldg(&S.nodes[2 * node + 1]);
         if (COUNT) c.nodes++;
@@ -431,7 +442,11 @@ __device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, 
             float v = dot3(d, q) * id;
             if (v < 0.0f || u + v > 1.0f) continue;
             float t = dot3(xyz(e2), q) * id;
-            if (t > 1e-4f && t < hit.t && stops<COUNT>(S, i, v0.w, ray, seed, c)) hit = Hit{t, i, det < 0.0f};
+            if (t > 1e-4f && t < hit.t && stops<COUNT>(S, i, v0.w, ray, seed, c)) {
+                hit = Hit{t, i, det < 0.0f};
+                lim = t * 1.0001f + 1e-5f;
+                lim2 = lim * lim;
+            }
         }
     }
     return hit;

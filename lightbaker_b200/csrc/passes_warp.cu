@@ -139,6 +139,7 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
     __shared__ uint8_t s_hit[WARPS][AO_CAP];
     __shared__ uint32_t s_front[WARPS][2][BALL_FRONT];
     __shared__ uint32_t s_list[WARPS][BALL_LEAVES];
+    __shared__ float s_dist[WARPS][BALL_LEAVES];
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -217,14 +218,14 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
         // the leaves within reach of this texel's occlusion rays, once for all of them
         int nl = -1;
         if (BVH == 2 && near && rays <= AO_CAP)
-            nl = ball_leaves<COUNT>(S, o, P.reach[0], nrm, s_front[w][0], s_front[w][1], s_list[w], lane, c);
+            nl = ball_leaves<COUNT>(S, o, P.reach[0], nrm, s_front[w][0], s_front[w][1], s_list[w], s_dist[w], lane, c);
         if (nl >= 0) {
             uint32_t myback = 0;
             for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
                 uint32_t r = ord.ray(r0 >> 5);
                 if (r < rays) {
                     float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
-                    Hit h = trace_list<COUNT>(S, s_list[w], nl, o, d, P.reach[0], key + r + 2000u, seed, c);
+                    Hit h = trace_list<COUNT>(S, s_list[w], s_dist[w], nl, o, d, P.reach[0], key + r + 2000u, seed, c);
                     float term = 0.0f;
                     bool hit = h.tri != NONE;
                     if (hit) {

@@ -96,6 +96,7 @@ struct lb_plan {
     int near_direct = 1;                               // leaf lists for the occlusion rays
     int occ_direct = 0, occ_gather = 0;                // register caps (WarpPass::occ)
     bool reuse = true;          // later bounces evaluate the first bounce's gather records
+    bool keep_records = false;  // record the first bounce's gather rays whatever the bounce count
     uint64_t max_gathered = 0;  // a bound on the gathered texels (records are sized by it)
     lbplan::DBuf records, theta0;
     std::string tuned;  // what the autotuner picked
@@ -113,3 +114,5 @@ struct lb_plan {
 
 // The plan's arguments for the texel passes over its dirty tiles.
 PostArgs lb_plan_post_args(lb_plan &p);
+// A plan of every tile (no cache) whose first gather pass records every ray's outcome in `records`.
+lb_plan *lb_plan_create_recording(lb_gpu *g, const uint8_t *scene, size_t len);

@@ -33,6 +33,7 @@
 
 #include "../../include/lightbaker.h"
 #include "lb_device.cuh"
+#include "lb_kernels.h"
 #include "lb_post.h"
 #include "lb_texel.cuh"
 #include "plan.h"
@@ -60,84 +61,39 @@ struct Theta {
 
 constexpr uint32_t LIT_NONE = 0xffffffffu, UNLIT = 0xfffffffeu;
 
-// The gather pass's rays (trace.wgsl:245-270) for the gathered texels, each ray's outcome recorded
-// ([item][ray]); a thread a ray.
-__global__ void k_records(Scene S, lb_params P, const float4 *tex, const uint32_t *idx, const float4 *posg,
-                          uint32_t n, uint32_t n_light, uint2 *rec) {
-    uint32_t rays = P.counts[2];
-    uint64_t total = uint64_t(n) * rays;
-    uint32_t seed = __float_as_uint(P.reach[3]);
-    Count c;
-    c.zero();
-    float frays = __uint2float_rn(rays);
-    for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total;
-         g += uint64_t(gridDim.x) * blockDim.x) {
-        uint32_t k = uint32_t(g / rays), r = uint32_t(g % rays);
-        uint32_t t = idx[k];
-        float4 p4 = posg[t], n4 = __ldg(&tex[4 * t + 1]), dx4 = __ldg(&tex[4 * t + 2]), dy4 = __ldg(&tex[4 * t + 3]);
-        float3 nrm = xyz(n4), pos = xyz(p4), dx = xyz(dx4), dy = xyz(dy4);
-        Frame f = frame(nrm);
-        uint32_t key = k * 7919u;
-        float s1 = rnd(key, 11u, seed), s2 = rnd(key, 13u, seed);
-        float jx = rnd(key + r, 19u, seed) - 0.5f, jy = rnd(key + r, 23u, seed) - 0.5f;
-        float3 o = add(add(add(pos, scl(dx, jx)), scl(dy, jy)), scl(nrm, P.reach[2]));
-        float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
-        Hit h = trace<false>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c);
-        rec[g] = gather_record(S, P, n_light, o, d, h);
-    }
-}
-
 // The records against the light and theta: each gathered texel's gather result, its terms summed in ray
-// order as the gather pass sums them (trace.wgsl:258-269); a warp an item.
+// order as the gather pass sums them (trace.wgsl:258-269); a thread an item, reading its records in turn.
 __global__ void k_eval(const uint2 *rec, const uint32_t *n_dev, uint32_t n_host, uint32_t rays, const float4 *light,
                        uint32_t n_light, Theta th, float4 *out) {
-    const int lane = threadIdx.x & 31;
-    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t n = n_dev ? *n_dev : n_host;
-    float frays = __uint2float_rn(rays);
-    float3 zen = th.zenith(), hor = th.horizon(), gro = th.ground(), fb = th.fallback();
-    for (uint32_t k = warp; k < n; k += warps) {
+    const float frays = __uint2float_rn(rays);
+    const float3 zen = th.zenith(), hor = th.horizon(), gro = th.ground(), fb = th.fallback();
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint2 *rk = rec + size_t(k) * rays;
         float3 sum = mk(0.f, 0.f, 0.f);
         uint32_t nback = 0;
-        for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
-            uint32_t r = r0 + uint32_t(lane);
-            float3 term = mk(0.f, 0.f, 0.f);
-            bool on = false, bk = false;
-            if (r < rays) {
-                uint2 q = rec[size_t(k) * rays + r];
-                uint32_t kind = q.x >> 30;
-                if (kind == KIND_SKY) {
-                    // trace.wgsl:63-66
-                    float y = __uint_as_float(q.y);
-                    term = y < 0.0f ? gro : add(scl(hor, 1.0f - y), scl(zen, y));
-                    on = true;
-                } else if (kind == KIND_BACK) {
-                    bk = true;
-                } else {
-                    uint32_t m = q.x & 0x3fffffffu;
-                    float3 al = m < th.M ? th.albedo(m) : mk(0.f, 0.f, 0.f);
-                    float3 e = fb;
-                    if (q.y < n_light) {
-                        float4 l = light[q.y];
-                        if (l.w > 0.5f) e = mk(l.x, l.y, l.z);
-                    }
-                    term = mulv(mk(al.x / PI, al.y / PI, al.z / PI), e);
-                    on = true;
+        for (uint32_t r = 0; r < rays; r++) {
+            uint2 q = __ldg(&rk[r]);
+            uint32_t kind = q.x >> 30;
+            if (kind == KIND_SKY) {
+                // trace.wgsl:63-66
+                float y = __uint_as_float(q.y);
+                sum = add(sum, y < 0.0f ? gro : add(scl(hor, 1.0f - y), scl(zen, y)));
+            } else if (kind == KIND_BACK) {
+                nback++;
+            } else {
+                uint32_t m = q.x & 0x3fffffffu;
+                float3 al = m < th.M ? th.albedo(m) : mk(0.f, 0.f, 0.f);
+                float3 e = fb;
+                if (q.y < n_light) {
+                    float4 l = __ldg(&light[q.y]);
+                    if (l.w > 0.5f) e = mk(l.x, l.y, l.z);
                 }
+                sum = add(sum, mulv(mk(al.x / PI, al.y / PI, al.z / PI), e));
             }
-            unsigned mask = __ballot_sync(0xffffffffu, on);
-#pragma unroll 1
-            for (int l = 0; l < 32; l++) {
-                float x = __shfl_sync(0xffffffffu, term.x, l), y = __shfl_sync(0xffffffffu, term.y, l),
-                      z = __shfl_sync(0xffffffffu, term.z, l);
-                if (mask & (1u << l)) sum = add(sum, mk(x, y, z));
-            }
-            nback += __popc(__ballot_sync(0xffffffffu, bk));
         }
-        if (lane == 0) {
-            float3 e = scl(sum, PI);
-            out[k] = make_float4(e.x / frays, e.y / frays, e.z / frays, __uint2float_rn(nback) / frays);
-        }
+        float3 e = scl(sum, PI);
+        out[k] = make_float4(e.x / frays, e.y / frays, e.z / frays, __uint2float_rn(nback) / frays);
     }
 }
 
@@ -455,22 +411,34 @@ __global__ void k_lit_t(const uint64_t *offs, const uint2 *sorted, uint32_t n_li
         }
         float4 L = light[l];
         float gx = 0.f, gy = 0.f, gz = 0.f;
-        for (uint64_t q = b; q < e; q++) {
-            uint2 s = sorted[q];
-            uint32_t k = s.x & 0x3fffffffu, m = s.y;
-            float4 g = g_res[k];
-            float cx = g.x / frays, cy = g.y / frays, cz = g.z / frays;
-            if (write_light) {
-                float3 al = th.albedo(m);
-                gx += cx * al.x, gy += cy * al.y, gz += cz * al.z;
-            }
+        // a texel's records are a chart's, so nearly always of one material: sum the records' weights
+        // while the material stays, and add weight x light to its albedo slot when it changes
+        uint32_t mr = sorted[b].y;
+        float3 al = th.albedo(mr);
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        auto flush = [&](uint32_t m) {
             if (m >= m0 && m < m0 + mc) {
                 size_t base = size_t(3 * (m - m0)) * blockDim.x + threadIdx.x;
-                acc[base] += double(cx) * double(L.x);
-                acc[base + blockDim.x] += double(cy) * double(L.y);
-                acc[base + 2 * blockDim.x] += double(cz) * double(L.z);
+                acc[base] += sx * double(L.x);
+                acc[base + blockDim.x] += sy * double(L.y);
+                acc[base + 2 * blockDim.x] += sz * double(L.z);
             }
+        };
+        for (uint64_t q = b; q < e; q++) {
+            uint2 s = __ldg(&sorted[q]);
+            uint32_t k = s.x & 0x3fffffffu, m = s.y;
+            if (m != mr) {
+                flush(mr);
+                sx = sy = sz = 0.0;
+                mr = m;
+                al = th.albedo(m);
+            }
+            float4 g = __ldg(&g_res[k]);
+            float cx = g.x / frays, cy = g.y / frays, cz = g.z / frays;
+            gx += cx * al.x, gy += cy * al.y, gz += cz * al.z;
+            sx += double(cx), sy += double(cy), sz += double(cz);
         }
+        flush(mr);
         if (write_light) g_light[l] = make_float4(gx, gy, gz, 0.f);
     }
     block_slots_out(acc, slots, partial);
@@ -570,7 +538,7 @@ __global__ void k_theta_final(const PartialSet *sets, int n_sets, int blocks, co
 cudaError_t lb_eval_records(const uint2 *rec, const uint32_t *n_dev, uint32_t n_host, uint32_t rays,
                             const float4 *light, uint32_t n_light, const float *theta, uint32_t n_mats, float4 *out,
                             int sms, cudaStream_t stream) {
-    lbd::k_eval<<<sms * 8, 256, 0, stream>>>(rec, n_dev, n_host, rays, light, n_light, lbd::Theta{theta, n_mats}, out);
+    lbd::k_eval<<<sms * 16, 128, 0, stream>>>(rec, n_dev, n_host, rays, light, n_light, lbd::Theta{theta, n_mats}, out);
     return cudaGetLastError();
 }
 
@@ -595,7 +563,8 @@ struct lb_transport {
     std::vector<float> theta0;
     PostArgs a{};
     CompositeArgs c{};
-    DBuf theta, rec, sorted, offs, kb, dl0, fixed_ind, masks, wsum, has0, has1, ckpt, work, res, e0, e1, fk_a, fk_b,
+    const uint2 *records = nullptr;  // the plan's gather records, [item][ray]
+    DBuf theta, sorted, offs, kb, dl0, fixed_ind, masks, wsum, has0, has1, ckpt, work, res, e0, e1, fk_a, fk_b,
         ind, out_atlas, out_tmp, out_has, out_has_b, out_direct, out_validity;
     DBuf g_in, g_blocks_a, g_blocks_b, g_ind, g_a, g_b, g_res, g_light, g_dl, partials, sun_partials, sets_d, g_theta;
     std::vector<lbd::PartialSet> sets;
@@ -614,7 +583,7 @@ namespace {
 
 // the bounces' light after bounce b of the forward: res, filters, write (the atlas rewritten in place)
 void bounce(lb_transport &t, float4 *light, uint32_t b, float4 *next, cudaStream_t st, float4 **filled) {
-    ck(lb_eval_records(t.rec.as<uint2>(), nullptr, t.n_gath, t.rays, light, t.n_light, t.theta.as<float>(), t.M,
+    ck(lb_eval_records(t.records, nullptr, t.n_gath, t.rays, light, t.n_light, t.theta.as<float>(), t.M,
                        t.res.as<float4>(), t.g->sms, st),
        "transport eval");
     ck(lb_bounce_filters(t.a, t.res.as<float4>(), t.r, t.plan->wr.as<float>(), t.rings, t.fk_a.as<uint8_t>(),
@@ -852,15 +821,9 @@ void build(lb_transport &t, uint32_t max_checkpoints) {
         lbd::k_dilate_plan<<<tg(nb), 256, 0, st>>>(f1.as<uint8_t>(), t.has1.as<uint8_t>(), t.iw, t.ih);
         ck(cudaStreamSynchronize(st), "dilation plan");
     }
-    // every gather ray's outcome
-    t.rec.alloc(t.n_rec * 8);
+    // every gather ray's outcome: the bake's first gather pass recorded them
+    t.records = p.records.as<uint2>();
     t.res.alloc(std::max<size_t>(t.n_gath, 1) * 16);
-    if (t.n_rec) {
-        lbd::Scene S = lb_scene_view(p.dscene);
-        lbd::k_records<<<t.g->sms * 8, 128, 0, st>>>(S, p.P.params, p.tex.as<float4>(), p.gath_idx.as<uint32_t>(),
-                                                    p.posg.as<float4>(), t.n_gath, t.n_light, t.rec.as<uint2>());
-        ck(cudaGetLastError(), "records");
-    }
     // the records sorted for the adjoint: lit ones by atlas texel, then sky and fallback-lit, then none
     t.sorted.alloc(t.n_rec * 8);
     t.offs.alloc(size_t(t.n_light + 3) * 8);
@@ -872,7 +835,7 @@ void build(lb_transport &t, uint32_t max_checkpoints) {
         keys2.alloc(n * 4);
         vals2.alloc(n * 4);
         if (t.n_rec) {
-            lbd::k_record_keys<<<t.g->sms * 8, 256, 0, st>>>(t.rec.as<uint2>(), t.n_rec, p.light.as<float4>(), t.n_light,
+            lbd::k_record_keys<<<t.g->sms * 8, 256, 0, st>>>(t.records, t.n_rec, p.light.as<float4>(), t.n_light,
                                                             t.M, keys.as<uint32_t>(), vals.as<uint32_t>());
             size_t tb = 0;
             ck(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.as<uint32_t>(), keys2.as<uint32_t>(), vals.as<uint32_t>(),
@@ -882,7 +845,7 @@ void build(lb_transport &t, uint32_t max_checkpoints) {
             ck(cub::DeviceRadixSort::SortPairs(temp.p, tb, keys.as<uint32_t>(), keys2.as<uint32_t>(), vals.as<uint32_t>(),
                                                vals2.as<uint32_t>(), int(t.n_rec), 0, 32, st),
                "sort");
-            lbd::k_record_sorted<<<t.g->sms * 8, 256, 0, st>>>(t.rec.as<uint2>(), vals2.as<uint32_t>(), t.n_rec, t.rays,
+            lbd::k_record_sorted<<<t.g->sms * 8, 256, 0, st>>>(t.records, vals2.as<uint32_t>(), t.n_rec, t.rays,
                                                               t.sorted.as<uint2>());
         }
         lbd::k_record_offsets<<<tg(t.n_light + 3), 256, 0, st>>>(keys2.as<uint32_t>(), t.n_rec, t.n_light,
@@ -959,8 +922,7 @@ lb_transport *lb_transport_create(lb_gpu *g, const uint8_t *scene, size_t len, u
         lb_set_error("lb_transport_create: bad arguments");
         return nullptr;
     }
-    lb_bake_options o{};
-    lb_plan *p = lb_plan_create(g, scene, len, &o);
+    lb_plan *p = lb_plan_create_recording(g, scene, len);
     if (!p) return nullptr;
     auto t = std::make_unique<lb_transport>();
     t->plan = p;
@@ -1072,7 +1034,7 @@ size_t lb_transport_export(lb_transport *t, const char *name, void *out, size_t 
         src = d.p;
         bytes = b;
     };
-    if (n == "records") dev(t->rec, t->n_rec * 8);
+    if (n == "records") dev(p.records, t->n_rec * 8);
     else if (n == "gathered_index") dev(p.gath_idx, size_t(t->n_gath) * 4);
     else if (n == "texels") dev(p.tex, size_t(t->n_tex) * 64);
     else if (n == "sample_points") dev(p.posg, size_t(t->n_tex) * 16);

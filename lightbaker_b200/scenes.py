@@ -270,6 +270,45 @@ def uneven_tiles(seed: int = 0, tiles: int = 8, tri_range=(5_000, 500_000), grid
                      {"workload": "uneven_tiles", "seed": seed, "tile_triangles": [int(c) for c in counts]})
 
 
+def stress_map(seed: int = 0, size: float = 400.0, boxes: int = 6000, cylinders: int = 30000, bounces: int = 4,
+               segments: int = 16) -> bytes:
+    """The stress map: size x size m, 0.5 m fractal heightfield (4 octaves, 2 m), boxes (sides 2-15 m) and
+    open cylinder props (r 0.2-1 m, h 1-6 m, `segments` sides), 16 materials; 50 m tiles at 4 texels/m,
+    256 AO rays, `bounces` x 128 gather rays, an L1 SH volume at 2 m (200 x 200 x 32 probes at 400 m).
+    At 400 m: 1.28 M ground triangles + 72 k box + 0.96 M prop triangles."""
+    rng = np.random.default_rng(seed)
+    noise = _value_noise(rng, 4, 2.0, size)
+    ground = heightfield(0.0, 0.0, size, size, 0.5, noise)
+    materials = [_material(f"m{k}", rng.uniform(0.15, 0.85, size=3)) for k in range(16)]
+    per_mat = [[] for _ in range(16)]
+    for _ in range(boxes):
+        sx, sy, sz = rng.uniform(2.0, 15.0, size=3)
+        x, z = rng.uniform(0.0, size - sx), rng.uniform(0.0, size - sz)
+        base = float(noise(np.array(x + sx / 2), np.array(z + sz / 2))) - 0.5
+        per_mat[int(rng.integers(0, 16))].append(np.asarray(cube((x, base, z), (x + sx, base + sy, z + sz)), np.float32))
+    r = rng.uniform(0.2, 1.0, cylinders)
+    h = rng.uniform(1.0, 6.0, cylinders)
+    x = rng.uniform(1.0, size - 1.0, cylinders)
+    z = rng.uniform(1.0, size - 1.0, cylinders)
+    yaw = rng.uniform(0.0, 2 * math.pi, cylinders)
+    m = rng.integers(0, 16, cylinders)
+    base = noise(x, z) - 0.2
+    for k in range(cylinders):
+        per_mat[int(m[k])].append(cylinder(x[k], base[k], z[k], r[k], h[k], yaw[k], segments))
+    groups = [("ground", 0, ground)]
+    for k in range(16):
+        if per_mat[k]:
+            groups.append((f"objects{k}", k, np.concatenate(per_mat[k])))
+    sky = {"zenith": [0.5, 0.6, 0.8], "horizon": [0.5, 0.6, 0.8], "ground": [0.5, 0.6, 0.8]}
+    sun = {"direction": sun_direction(40.0, 130.0), "radiusDeg": 0.5, "irradiance": [3.0, 3.0, 3.0]}
+    lightmap = {"texelsPerMeter": 4.0, "tileSize": 50.0, "chartAngleDeg": 40.0, "padding": 2,
+                "atlasWidth": 8192 if size > 200 else 2048, "indirectDownscale": 2}
+    bake = _defaults_bake(aoRays=256, aoReach=2.0, giRays=128, giBounces=bounces)
+    ny = 32 if size >= 400 else 16
+    volume = {"min": [1.0, 0.5, 1.0], "max": [size - 1.0, 0.5 + 2.0 * (ny - 1), size - 1.0], "step": 2.0, "rays": 128}
+    return _assemble(groups, materials, sun, sky, lightmap, bake, volume, {"workload": "stress_map", "seed": seed})
+
+
 def with_light(scene: bytes, albedo=None, zenith=None, horizon=None, ground=None, irradiance=None) -> bytes:
     """The same scene with other light parameters: materials' albedos (one rgb a material), the sky's
     colours, the sun's irradiance. Only the header changes (scene.rs:164-181: "LBSC", version, header
