@@ -111,6 +111,19 @@ def gather_items(P, by_tile):
     return np.concatenate(out)
 
 
+def parse_tuning(tuning: str) -> dict:
+    """The autotuner's report ("direct: bvh 2, refill 0, near 1, order 0, register cap 0, 2 blocks/SM (...);
+    gather: ...") as {"direct": {"bvh": 2, ...}, "gather": {...}}."""
+    import re
+    out = {}
+    for part in tuning.split(";"):
+        if ":" not in part:
+            continue
+        name, rest = part.split(":", 1)
+        out[name.strip()] = {k.strip(): int(v) for k, v in re.findall(r"([a-z ]+?) (\d+)(?:,|$| blocks)", rest)}
+    return out
+
+
 def scene_header(scene: bytes) -> dict:
     import struct
     hl = struct.unpack("<I", scene[8:12])[0]
@@ -373,8 +386,16 @@ def main():
     out = torch.empty(max(len(direct), len(gather)) * 16, dtype=torch.uint8, device=dev)
     gpu.set_pass_kernel(1)
     kernel_stats = {}
+    shapes = parse_tuning(tuning)
     for name, pass_, items, d_items in (("direct_warp", lb.Pass.DIRECT, direct, d_direct),
                                         ("gather_warp", lb.Pass.GATHER, gather, d_gather)):
+        # the shape the plan's autotuner chose for this pass
+        sh = shapes.get("direct" if pass_ == lb.Pass.DIRECT else "gather", {})
+        gpu.set_bvh(sh.get("bvh", 2))
+        gpu.set_refill(sh.get("refill", 0))
+        gpu.set_near(sh.get("near", 1))
+        gpu.set_register_cap(sh.get("register cap", 0))
+        gpu.set_ray_order(sh.get("order", 8), sh.get("order", 8))
         gpu.set_counting(True)
         gpu.run_async(pass_, buffers, P.params, d_items.data_ptr(), len(items), 0, d_light.data_ptr(), len(light),
                       out.data_ptr())
@@ -400,6 +421,9 @@ def main():
         kernel_stats[name] = {"ms": kms, "rays": walk["rays"], "alg_bytes": alg, "nodes": walk["nodes"],
                               "tris": walk["tris"], "mats": walk["mats"], "items": int(len(items))}
     gpu.set_pass_kernel(0)
+    gpu.set_register_cap(0)
+    gpu.set_ray_order(8, 8)
+    gpu.set_near(1)
     buffers.close()
     del d_direct, d_gather, d_light, out
 
@@ -519,7 +543,8 @@ def main():
         hbm = peaks.get("hbm_gbs")
         peak_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if hbm else "fallback 6650 GB/s"
         hbm = hbm or 6650.0
-        dom = max(kernel_stats, key=lambda k: kernel_stats[k]["ms"] * (1 if k == "direct_warp" else P.info.gi_bounces))
+        # each pass runs once a step (the gathers of later bounces are evaluated from records)
+        dom = max(kernel_stats, key=lambda k: kernel_stats[k]["ms"])
         ks = kernel_stats[dom]
         achieved = ks["alg_bytes"] / (ks["ms"] / 1e3) / 1e9
         traffic = None

@@ -131,7 +131,7 @@ __device__ __forceinline__ void flush_counts(Count &c, unsigned long long *count
 }
 
 // trace.wgsl:170-243. OCC: blocks of 256 threads an SM must hold (the compiler's register budget).
-template <int BVH, bool COUNT, int OCC = 1>
+template <int BVH, bool COUNT, int OCC = 1, int WALK = 0>
 __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
                                                    unsigned long long *counters, int group, int refill, int near) {
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
         const int w = threadIdx.x >> 5;
         // the leaves within reach of this texel's occlusion rays, once for all of them
         int nl = -1;
-        if (BVH == 2 && near && rays <= AO_CAP)
+        if (BVH == 2 && WALK == 1 && near && rays <= AO_CAP)
             nl = ball_leaves<COUNT>(S, o, P.reach[0], nrm, s_front[w][0], s_front[w][1], s_list[w], s_dist[w], lane, c);
         if (nl >= 0) {
             uint32_t myback = 0;
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
                 occ = ordered_add(occ, rr < rays ? s_term[w][rr] : 0.0f, rr < rays && s_hit[w][rr]);
             }
             __syncwarp();
-        } else if (BVH == 2 && refill && rays <= AO_CAP) {
+        } else if (BVH == 2 && WALK == 2 && refill && rays <= AO_CAP) {
             // lane refill: a lane takes the item's next ray as soon as its own has ended
             Walk2<COUNT> wk;
             uint32_t seq = uint32_t(lane), next = 32, r = 0, myback = 0;
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
             }
             nback += __popc(__ballot_sync(FULL, bk));
         }
-        if (nl < 0 && !(BVH == 2 && refill && rays <= AO_CAP) && ord.grouped) {
+        if (nl < 0 && !(BVH == 2 && WALK == 2 && refill && rays <= AO_CAP) && ord.grouped) {
             __syncwarp();
             for (uint32_t r0 = 0; r0 < rays; r0 += 32) occ = ordered_add(occ, s_term[w][r0 + lane], s_hit[w][r0 + lane]);
             __syncwarp();
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
 }
 
 // trace.wgsl:245-270. rec (optional): each ray's outcome ([item][ray], gather_record) for later bounces.
-template <int BVH, bool COUNT, int OCC = 1>
+template <int BVH, bool COUNT, int OCC = 1, int WALK = 0>
 __global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const float4 *pos_override, const uint32_t *n_dev, uint32_t n_host,
                                                    uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, co
         uint32_t nback = 0;
         const RayOrder ord(rays, GI_CAP, group, lane);
         const int w = threadIdx.x >> 5;
-        const bool refilling = BVH == 2 && refill && rays <= GI_CAP;
+        const bool refilling = BVH == 2 && WALK == 2 && refill && rays <= GI_CAP;
         if (refilling) {
             // lane refill: a lane takes the item's next ray as soon as its own has ended
             Walk2<COUNT> wk;
@@ -522,38 +522,63 @@ __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const f
 
 }  // namespace lbd
 
-template <int BVH, bool COUNT, int OCC = 1> int blocks_for(int pass) {
+// The walk a pass's occlusion or gather rays take (a template parameter, so that each kernel carries only
+// its own): 0 the tree walk, 1 leaf lists (BVH2 direct pass; the tree walk when a list overflows),
+// 2 lane refill (BVH2).
+static int walk_of(const WarpPass &w) {
+    if (w.bvh != 2 || w.pass == LB_PASS_VOLUME) return 0;
+    if (w.refill) return 2;
+    return (w.near && w.pass == LB_PASS_DIRECT) ? 1 : 0;
+}
+
+template <int BVH, bool COUNT, int OCC, int WALK> int blocks_walk(int pass) {
     const int T = 256;
     int per_sm = 0;
     cudaError_t e;
     switch (pass) {
     case LB_PASS_DIRECT:
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::direct_warp<BVH, COUNT, OCC>, T, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::direct_warp<BVH, COUNT, OCC, WALK>, T, 0);
         break;
     case LB_PASS_GATHER:
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::gather_warp<BVH, COUNT, OCC>, T, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::gather_warp<BVH, COUNT, OCC, WALK>, T, 0);
         break;
     default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::volume_warp<BVH, COUNT>, T, 0); break;
     }
     return (e != cudaSuccess || per_sm < 1) ? 1 : per_sm;
 }
 
-template <int BVH, bool COUNT, int OCC = 1> void launch(const WarpPass &w, int blocks, cudaStream_t stream) {
+template <int BVH, bool COUNT, int OCC, int WALK> void launch_walk(const WarpPass &w, int blocks, cudaStream_t stream) {
     const int T = 256;
     switch (w.pass) {
     case LB_PASS_DIRECT:
-        lbd::direct_warp<BVH, COUNT, OCC><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base,
-                                                                    w.out, w.counters, w.group, w.refill, w.near);
+        lbd::direct_warp<BVH, COUNT, OCC, WALK><<<blocks, T, 0, stream>>>(
+            *w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base, w.out, w.counters, w.group, w.refill, w.near);
         break;
     case LB_PASS_GATHER:
-        lbd::gather_warp<BVH, COUNT, OCC><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host,
-                                                                    w.base, w.light, w.n_light, w.out, w.counters,
-                                                                    w.group, w.refill, w.rec);
+        lbd::gather_warp<BVH, COUNT, OCC, WALK><<<blocks, T, 0, stream>>>(
+            *w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host, w.base, w.light, w.n_light, w.out, w.counters, w.group,
+            w.refill, w.rec);
         break;
     default:
         lbd::volume_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light, w.out,
                                                                w.slot, w.counters);
         break;
+    }
+}
+
+template <int BVH, bool COUNT, int OCC = 1> int blocks_for(const WarpPass &w) {
+    switch (walk_of(w)) {
+    case 1: return blocks_walk<BVH, COUNT, OCC, 1>(w.pass);
+    case 2: return blocks_walk<BVH, COUNT, OCC, 2>(w.pass);
+    default: return blocks_walk<BVH, COUNT, OCC, 0>(w.pass);
+    }
+}
+
+template <int BVH, bool COUNT, int OCC = 1> void launch(const WarpPass &w, int blocks, cudaStream_t stream) {
+    switch (walk_of(w)) {
+    case 1: launch_walk<BVH, COUNT, OCC, 1>(w, blocks, stream); break;
+    case 2: launch_walk<BVH, COUNT, OCC, 2>(w, blocks, stream); break;
+    default: launch_walk<BVH, COUNT, OCC, 0>(w, blocks, stream); break;
     }
 }
 
@@ -564,10 +589,10 @@ static bool capped(const WarpPass &w) {
 
 int lb_warp_pass_blocks(const WarpPass &w) {
     int per_sm;
-    if (capped(w)) per_sm = w.occ == 3 ? blocks_for<2, false, 3>(w.pass) : blocks_for<2, false, 4>(w.pass);
+    if (capped(w)) per_sm = w.occ == 3 ? blocks_for<2, false, 3>(w) : blocks_for<2, false, 4>(w);
     else
-        per_sm = w.bvh == 8 ? (w.full_count ? blocks_for<8, true>(w.pass) : blocks_for<8, false>(w.pass))
-                            : (w.full_count ? blocks_for<2, true>(w.pass) : blocks_for<2, false>(w.pass));
+        per_sm = w.bvh == 8 ? (w.full_count ? blocks_for<8, true>(w) : blocks_for<8, false>(w))
+                            : (w.full_count ? blocks_for<2, true>(w) : blocks_for<2, false>(w));
     return w.sms * per_sm;
 }
 

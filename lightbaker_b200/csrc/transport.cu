@@ -383,104 +383,158 @@ __global__ void k_light_t(PostArgs a, const uint8_t *kb, const float4 *g_light, 
 // horizon, ground and fallback (3 each).
 constexpr int FIXED_SLOTS = 12;
 
-// Per-thread accumulators in shared memory ([slot][thread]: a thread adds to its own column only),
-// then each slot summed over the block's threads in thread order: the same bits every launch.
-__device__ __forceinline__ void block_slots_out(double *acc, int slots, double *partial) {
+// Theta's per-block partial sums: each warp adds into its own row of slots ([warp][3 mc]; one lane a
+// component, the warp's staged values in lane order), then each slot is summed over the block's warps in
+// warp order: the same bits every launch.
+constexpr int TW = 8;  // warps a block in the adjoint's reduction kernels (256 threads)
+
+__device__ __forceinline__ void warp_stage_add(double *row, uint32_t m0, uint32_t mc, const uint32_t *st_m,
+                                               const double (*st_v)[3], int lane) {
+    __syncwarp();
+    if (lane < 3)
+        for (int j = 0; j < 32; j++) {
+            uint32_t m = st_m[j];
+            if (m >= m0 && m < m0 + mc) row[3 * (m - m0) + lane] += st_v[j][lane];
+        }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void block_rows_out(const double *acc, int S, const double *fixed, double *partial) {
     __syncthreads();
+    const int slots = S + FIXED_SLOTS;
     for (int s = threadIdx.x; s < slots; s += blockDim.x) {
         double v = 0.0;
-        for (int l = 0; l < int(blockDim.x); l++) v += acc[size_t(s) * blockDim.x + l];
+        if (s < S)
+            for (int w = 0; w < TW; w++) v += acc[size_t(w) * S + s];
+        else if (fixed)
+            for (int l = 0; l < int(blockDim.x); l++) v += fixed[size_t(l) * FIXED_SLOTS + (s - S)];
         partial[size_t(blockIdx.x) * slots + s] = v;
     }
 }
 
-// The lit records, atlas texel by atlas texel (sorted): the atlas gradient (the texel's light fed each
-// record's term al / pi * e) and the albedo gradients of the chunk's materials (e / pi * pi / rays).
-__global__ void k_lit_t(const uint64_t *offs, const uint2 *sorted, uint32_t n_light, const float4 *light, Theta th,
-                        uint32_t m0, uint32_t mc, uint32_t rays, const float4 *g_res, float4 *g_light, int write_light,
-                        double *partial) {
-    extern __shared__ double acc[];  // [3 mc + FIXED_SLOTS][blockDim.x]
-    const int slots = 3 * int(mc) + FIXED_SLOTS;
-    for (int s = 0; s < slots; s++) acc[size_t(s) * blockDim.x + threadIdx.x] = 0.0;
-    float frays = __uint2float_rn(rays);
-    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < n_light; l += gridDim.x * blockDim.x) {
-        uint64_t b = offs[l], e = offs[l + 1];
-        if (b == e) {
-            if (write_light) g_light[l] = make_float4(0.f, 0.f, 0.f, 0.f);
-            continue;
-        }
-        float4 L = light[l];
-        float gx = 0.f, gy = 0.f, gz = 0.f;
-        // a texel's records are a chart's, so nearly always of one material: sum the records' weights
-        // while the material stays, and add weight x light to its albedo slot when it changes
-        uint32_t mr = sorted[b].y;
-        float3 al = th.albedo(mr);
-        double sx = 0.0, sy = 0.0, sz = 0.0;
-        auto flush = [&](uint32_t m) {
-            if (m >= m0 && m < m0 + mc) {
-                size_t base = size_t(3 * (m - m0)) * blockDim.x + threadIdx.x;
-                acc[base] += sx * double(L.x);
-                acc[base + blockDim.x] += sy * double(L.y);
-                acc[base + 2 * blockDim.x] += sz * double(L.z);
+// The lit records, atlas texel by atlas texel (sorted; a lane a texel, 32 consecutive texels a warp): the
+// atlas gradient (the texel's light fed each record's term al / pi * e) and the albedo gradients of the
+// chunk's materials (the record's weight c = g / rays times its light). A texel's records are a chart's,
+// so nearly always of one material: its weights are summed and multiplied by its light once; a texel
+// with records of several materials is walked again record by record, lane by lane.
+__global__ void __launch_bounds__(256) k_lit_t(const uint64_t *offs, const uint2 *sorted, uint32_t n_light,
+                                               const float4 *light, Theta th, uint32_t m0, uint32_t mc, uint32_t rays,
+                                               const float4 *g_res, float4 *g_light, int write_light,
+                                               double *partial) {
+    extern __shared__ double acc[];  // [TW][3 mc]
+    __shared__ double st_v[TW][32][3];
+    __shared__ uint32_t st_m[TW][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, S = 3 * int(mc);
+    double *row = acc + size_t(w) * S;
+    for (int q = lane; q < S; q += 32) row[q] = 0.0;
+    const float frays = __uint2float_rn(rays);
+    const uint32_t stride = gridDim.x * TW * 32;
+    for (uint32_t base = (blockIdx.x * TW + w) * 32; base < n_light; base += stride) {
+        uint32_t l = base + lane, mfirst = NONE;
+        bool mixed = false;
+        double vx = 0.0, vy = 0.0, vz = 0.0;
+        float4 L = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint64_t b = 0, e = 0;
+        if (l < n_light) {
+            b = offs[l];
+            e = offs[l + 1];
+            if (b < e) {
+                L = light[l];
+                uint32_t mr = __ldg(&sorted[b]).y;
+                mfirst = mr;
+                float3 al = th.albedo(mr);
+                float gx = 0.f, gy = 0.f, gz = 0.f;
+                for (uint64_t q = b; q < e; q++) {
+                    uint2 sr = __ldg(&sorted[q]);
+                    if (sr.y != mr) {
+                        mixed = true;
+                        mr = sr.y;
+                        al = th.albedo(mr);
+                    }
+                    float4 g = __ldg(&g_res[sr.x & 0x3fffffffu]);
+                    float cx = g.x / frays, cy = g.y / frays, cz = g.z / frays;
+                    gx += cx * al.x, gy += cy * al.y, gz += cz * al.z;
+                    vx += double(cx), vy += double(cy), vz += double(cz);
+                }
+                if (write_light) g_light[l] = make_float4(gx, gy, gz, 0.f);
+            } else if (write_light) {
+                g_light[l] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
-        };
-        for (uint64_t q = b; q < e; q++) {
-            uint2 s = __ldg(&sorted[q]);
-            uint32_t k = s.x & 0x3fffffffu, m = s.y;
-            if (m != mr) {
-                flush(mr);
-                sx = sy = sz = 0.0;
-                mr = m;
-                al = th.albedo(m);
-            }
-            float4 g = __ldg(&g_res[k]);
-            float cx = g.x / frays, cy = g.y / frays, cz = g.z / frays;
-            gx += cx * al.x, gy += cy * al.y, gz += cz * al.z;
-            sx += double(cx), sy += double(cy), sz += double(cz);
         }
-        flush(mr);
-        if (write_light) g_light[l] = make_float4(gx, gy, gz, 0.f);
+        st_m[w][lane] = mixed ? NONE : mfirst;
+        st_v[w][lane][0] = vx * double(L.x);
+        st_v[w][lane][1] = vy * double(L.y);
+        st_v[w][lane][2] = vz * double(L.z);
+        warp_stage_add(row, m0, mc, st_m[w], st_v[w], lane);
+        unsigned mx = __ballot_sync(0xffffffffu, mixed);
+        while (mx) {
+            int src = __ffs(mx) - 1;
+            mx &= mx - 1;
+            if (lane == src)
+                for (uint64_t q = b; q < e; q++) {
+                    uint2 sr = sorted[q];
+                    uint32_t m = sr.y;
+                    if (m < m0 || m >= m0 + mc) continue;
+                    float4 g = g_res[sr.x & 0x3fffffffu];
+                    double *d = row + 3 * (m - m0);
+                    d[0] += double(g.x / frays) * double(L.x);
+                    d[1] += double(g.y / frays) * double(L.y);
+                    d[2] += double(g.z / frays) * double(L.z);
+                }
+            __syncwarp();
+        }
     }
-    block_slots_out(acc, slots, partial);
+    block_rows_out(acc, S, nullptr, partial);
 }
 
-// The sky records and the surface records that take the fallback light: the sky's gradients, the
-// fallback's, and the albedo gradients of the chunk's materials lit by the fallback.
-__global__ void k_unlit_t(const uint2 *sorted, uint64_t n, Theta th, uint32_t m0, uint32_t mc, uint32_t rays,
-                          const float4 *g_res, int fixed_slots, double *partial) {
-    extern __shared__ double acc[];
-    const int slots = 3 * int(mc) + FIXED_SLOTS;
-    for (int s = 0; s < slots; s++) acc[size_t(s) * blockDim.x + threadIdx.x] = 0.0;
-    const double frays = double(rays), q = 3.14159265358979323846 / frays;
-    float3 fb = th.fallback();
+// The sky records and the surface records that take the fallback light (a lane a record): the sky's
+// gradients and the fallback's in each thread's own registers, the albedo gradients of the chunk's
+// materials lit by the fallback staged a warp at a time.
+__global__ void __launch_bounds__(256) k_unlit_t(const uint2 *sorted, uint64_t n, Theta th, uint32_t m0, uint32_t mc,
+                                                 uint32_t rays, const float4 *g_res, int fixed_slots, double *partial) {
+    extern __shared__ double acc[];  // [TW][3 mc]
+    __shared__ double st_v[TW][32][3];
+    __shared__ uint32_t st_m[TW][32];
+    __shared__ double fixed[256 * FIXED_SLOTS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, S = 3 * int(mc);
+    double *row = acc + size_t(w) * S;
+    for (int q = lane; q < S; q += 32) row[q] = 0.0;
+    const double frays = double(rays), qq = 3.14159265358979323846 / frays;
+    const float3 fb = th.fallback();
     double f[FIXED_SLOTS] = {0};
-    for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += uint64_t(gridDim.x) * blockDim.x) {
-        uint2 s = sorted[r];
-        uint32_t kind = s.x >> 30, k = s.x & 0x3fffffffu;
-        float4 g = g_res[k];
-        if (kind == KIND_SKY) {
-            double y = double(__uint_as_float(s.y));
-            if (y < 0.0) {
-                f[6] += g.x * q, f[7] += g.y * q, f[8] += g.z * q;
+    const uint64_t stride = uint64_t(gridDim.x) * TW * 32;
+    for (uint64_t base = (uint64_t(blockIdx.x) * TW + w) * 32; base < n; base += stride) {
+        uint64_t r = base + lane;
+        uint32_t mst = NONE;
+        double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+        if (r < n) {
+            uint2 sr = __ldg(&sorted[r]);
+            uint32_t kind = sr.x >> 30;
+            float4 g = __ldg(&g_res[sr.x & 0x3fffffffu]);
+            if (kind == KIND_SKY) {
+                double y = double(__uint_as_float(sr.y));
+                if (y < 0.0) {
+                    f[6] += g.x * qq, f[7] += g.y * qq, f[8] += g.z * qq;
+                } else {
+                    f[0] += g.x * qq * y, f[1] += g.y * qq * y, f[2] += g.z * qq * y;
+                    f[3] += g.x * qq * (1.0 - y), f[4] += g.y * qq * (1.0 - y), f[5] += g.z * qq * (1.0 - y);
+                }
             } else {
-                f[0] += g.x * q * y, f[1] += g.y * q * y, f[2] += g.z * q * y;
-                f[3] += g.x * q * (1.0 - y), f[4] += g.y * q * (1.0 - y), f[5] += g.z * q * (1.0 - y);
-            }
-        } else {
-            uint32_t m = s.y;
-            float3 al = th.albedo(m);
-            f[9] += g.x * double(al.x) / frays, f[10] += g.y * double(al.y) / frays, f[11] += g.z * double(al.z) / frays;
-            if (m >= m0 && m < m0 + mc) {
-                size_t base = size_t(3 * (m - m0)) * blockDim.x + threadIdx.x;
-                acc[base] += g.x * double(fb.x) / frays;
-                acc[base + blockDim.x] += g.y * double(fb.y) / frays;
-                acc[base + 2 * blockDim.x] += g.z * double(fb.z) / frays;
+                float3 al = th.albedo(sr.y);
+                f[9] += g.x * double(al.x) / frays, f[10] += g.y * double(al.y) / frays;
+                f[11] += g.z * double(al.z) / frays;
+                mst = sr.y;
+                v0 = g.x * double(fb.x) / frays, v1 = g.y * double(fb.y) / frays, v2 = g.z * double(fb.z) / frays;
             }
         }
+        st_m[w][lane] = mst;
+        st_v[w][lane][0] = v0;
+        st_v[w][lane][1] = v1;
+        st_v[w][lane][2] = v2;
+        warp_stage_add(row, m0, mc, st_m[w], st_v[w], lane);
     }
-    if (fixed_slots)
-        for (int c = 0; c < FIXED_SLOTS; c++) acc[size_t(3 * mc + c) * blockDim.x + threadIdx.x] = f[c];
-    block_slots_out(acc, slots, partial);
+    for (int c = 0; c < FIXED_SLOTS; c++) fixed[size_t(threadIdx.x) * FIXED_SLOTS + c] = fixed_slots ? f[c] : 0.0;
+    block_rows_out(acc, S, fixed, partial);
 }
 
 // the sun's gradient: the direct light is s * dl0, so d/ds = sum over texels of g_dl . dl0
@@ -492,7 +546,12 @@ __global__ void k_sun_t(uint32_t n, const float4 *g_dl, const float4 *dl0, doubl
         v += double(g.x) * d.x + double(g.y) * d.y + double(g.z) * d.z;
     }
     acc[threadIdx.x] = v;
-    block_slots_out(acc, 1, partial);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int l = 0; l < int(blockDim.x); l++) t += acc[l];
+        partial[blockIdx.x] = t;
+    }
 }
 
 // Theta's gradient from the partial sums, in a fixed order: pass by pass (bounce, kind, material chunk),
@@ -546,8 +605,8 @@ namespace {
 
 inline dim3 tg(uint64_t n) { return dim3(uint32_t((n + 255) / 256)); }
 
-constexpr int T_THREADS = 128;          // threads of the adjoint's reduction kernels
-constexpr size_t T_SMEM = 160 * 1024;   // their shared memory at most
+constexpr int T_THREADS = 32 * lbd::TW;  // threads of the adjoint's reduction kernels
+constexpr size_t T_SMEM = 128 * 1024;    // their dynamic shared memory at most
 
 }  // namespace
 
@@ -641,7 +700,7 @@ void record_backward(lb_transport &t, cudaStream_t st) {
         lbd::k_composite_t<<<tg(t.n_tex), 256, 0, st>>>(a, t.c, t.g_blocks_b.as<float4>(), t.g_ind.as<float4>());
     ck(cudaGetLastError(), "transport composite^T");
     bool all = t.K >= t.B;
-    size_t smem = size_t(3 * t.mc + lbd::FIXED_SLOTS) * T_THREADS * sizeof(double);
+    size_t smem = size_t(3 * t.mc) * lbd::TW * sizeof(double);
     int set = 0;
     for (int32_t b = int32_t(t.B) - 1; b >= 0; b--) {
         // the light this bounce read: kept, or recomputed from the nearest earlier checkpoint
@@ -881,12 +940,12 @@ void build(lb_transport &t, uint32_t max_checkpoints) {
     t.g_res.alloc(std::max<size_t>(t.n_gath, 1) * 16);
     t.g_light.alloc(size_t(t.n_light) * 16);
     t.g_theta.alloc(size_t(3 * t.M + 10) * 4);
-    t.blocks = t.g->sms * 2;
+    t.blocks = t.g->sms * 4;
     t.sun_blocks = t.g->sms * 2;
-    size_t per_mat = size_t(3) * T_THREADS * sizeof(double), fixed = size_t(lbd::FIXED_SLOTS) * T_THREADS * sizeof(double);
-    t.mc = uint32_t(std::max<size_t>(1, (T_SMEM - fixed) / per_mat));
+    size_t per_mat = size_t(3) * lbd::TW * sizeof(double);
+    t.mc = uint32_t(std::max<size_t>(1, T_SMEM / per_mat));
     t.mc = std::min(t.mc, std::max(t.M, 1u));
-    size_t smem = size_t(3 * t.mc + lbd::FIXED_SLOTS) * T_THREADS * sizeof(double);
+    size_t smem = size_t(3 * t.mc) * lbd::TW * sizeof(double);
     ck(cudaFuncSetAttribute(lbd::k_lit_t, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem");
     ck(cudaFuncSetAttribute(lbd::k_unlit_t, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem");
     uint32_t chunks = (std::max(t.M, 1u) + t.mc - 1) / t.mc;
