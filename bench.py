@@ -547,13 +547,14 @@ def main():
         dom = max(kernel_stats, key=lambda k: kernel_stats[k]["ms"])
         ks = kernel_stats[dom]
         achieved = ks["alg_bytes"] / (ks["ms"] / 1e3) / 1e9
-        traffic = None
-        tfile = ROOT / "profiles" / "traffic.json"
+        # DRAM bytes a launch from an ncu capture (profiles/traffic.txt: workload kernel bytes source)
+        traffic, traffic_src = None, None
+        tfile = ROOT / "profiles" / "traffic.txt"
         if tfile.exists():
-            try:
-                traffic = json.loads(tfile.read_text()).get(args.workload, {}).get(dom)
-            except Exception:
-                traffic = None
+            for row in tfile.read_text().splitlines():
+                f = row.split()
+                if len(f) >= 3 and not row.startswith("#") and f[0] == args.workload and f[1] == dom:
+                    traffic, traffic_src = int(f[2]), (f[3] if len(f) > 3 else None)
         cpu_g, cpu_rays, cpu_secs, cpu_items = cpu_baseline(P, direct, gather, probes, light, args.cpu_seconds)
         line = {
             "metric": "Grays/s", "value": value, "unit": "Grays/s", "n_gpus": world, "steps": args.steps,
@@ -571,7 +572,8 @@ def main():
                        "parallelism": f"independent maps x{world}"},
             "bake_seconds": e2e_t / 1e3,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": traffic, "kernel": dom, "peak_source": peak_src,
+                         "traffic": traffic, "traffic_source": traffic_src and f"profiles/{traffic_src}, scaled by texels",
+                         "kernel": dom, "peak_source": peak_src,
                          "algorithmic_bytes_per_launch": ks["alg_bytes"], "kernel_ms": ks["ms"],
                          "note": "algorithmic bytes = 32 B a node record fetched + 48 B a triangle tested + 16 B a "
                                  "material read + 80 B an item, counted on the device; the BVH lives in L2"},
