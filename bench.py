@@ -111,6 +111,25 @@ def gather_items(P, by_tile):
     return np.concatenate(out)
 
 
+def rank_seed(rank: int) -> int:
+    """Each rank bakes its own map of the workload (weak scaling): the map's seed is the rank."""
+    return rank
+
+
+def reduce_max(x: float, dist, device) -> float:
+    """x's maximum over the ranks (every rank gets it); x itself with one process."""
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
+def job_value(rays_per_rank: int, world: int, ms_max: float) -> float:
+    """Whole-job Grays/s: every rank's rays over the slowest rank's time."""
+    return rays_per_rank * world / (ms_max / 1e3) / 1e9
+
+
 def parse_tuning(tuning: str) -> dict:
     """The autotuner's report ("direct: bvh 2, refill 0, near 1, order 0, register cap 0, 2 blocks/SM (...);
     gather: ...") as {"direct": {"bvh": 2, ...}, "gather": {...}}."""
@@ -321,17 +340,14 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
     import lightbaker_b200 as lb
-    scene, P, direct, gather, probes, light = load_workload(args.workload, rank)
+    scene, P, direct, gather, probes, light = load_workload(args.workload, rank_seed(rank))
     gpu = lb.Gpu.new(local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.ExternalStream(gpu.stream, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
     def max_over_ranks(x: float) -> float:
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return t.item()
+        return reduce_max(x, dist, dev)
 
     # ---- the device-resident bake: graph replays, inputs resident ----
     plan = lb.Plan(scene, gpu, autotune=True)
@@ -363,7 +379,7 @@ def main():
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     ms_per_step = max_over_ranks(sum(ms) / len(ms))
-    value = rays_step * world / (ms_per_step / 1e3) / 1e9
+    value = job_value(rays_step, world, ms_per_step)
     baked = plan.result()
     plan.close()
     if args.device_only:

@@ -289,13 +289,31 @@ __global__ void k_fill_plan(PostArgs a, const uint8_t *was, uint8_t *plan, uint8
     now[i] = mode != 0;
 }
 
+// a flagged texel that a neighbour fills from in this ring gets 0x40 too (the others keep their value
+// and feed nothing: the transpose copies them)
+__global__ void k_fill_plan_mark(PostArgs a, uint8_t *plan) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= a.n_texels || !(plan[j] & 0x80)) return;
+    const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, j)];
+    int lj = int(j - t.off), x = lj % int(t.w), y = lj / int(t.w);
+    bool feeds = false;
+    for (int yy = y > 0 ? y - 1 : 0; yy < min(y + 2, int(t.h)); yy++)
+        for (int xx = x > 0 ? x - 1 : 0; xx < min(x + 2, int(t.w)); xx++) {
+            uint8_t pi = plan[t.off + uint32_t(yy) * t.w + uint32_t(xx)];
+            if (!(pi & 0x80) && (pi >> 4) != 0) feeds = true;
+        }
+    if (feeds) plan[j] = 0xc0;
+}
+
 // one fill ring transposed
 __global__ void k_fill_t(PostArgs a, const uint8_t *plan, const float4 *g_out, float4 *g_in) {
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= a.n_texels) return;
     float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
     uint8_t pj = plan[j];
-    if (pj & 0x80) {
+    if (pj == 0x80) {
+        g = g_out[j];
+    } else if (pj & 0x80) {
         g = g_out[j];
         const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, j)];
         int lj = int(j - t.off), x = lj % int(t.w), y = lj / int(t.w);
@@ -562,22 +580,21 @@ struct PartialSet {
     int fixed;         // holds the fixed slots
 };
 
-__global__ void k_theta_final(const PartialSet *sets, int n_sets, int blocks, const double *sun, int sun_blocks,
-                              uint32_t M, float *g_theta) {
-    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t n_out = 3 * M + 10;
-    if (j >= n_out) return;
-    // output j reads slot(s): albedo 3m+c; zenith/horizon/ground; the fallback feeds zenith and horizon
+// A block an output: its threads take the (set, block) rows in a fixed stride, then a fixed tree.
+__global__ void __launch_bounds__(256) k_theta_final(const PartialSet *sets, int n_sets, int blocks, const double *sun,
+                                                     int sun_blocks, uint32_t M, float *g_theta) {
+    __shared__ double part[256];
+    // output j reads slot(s): albedo 3m+c; zenith/horizon/ground; the fallback feeds zenith and horizon;
+    // the sun its own partials
+    const uint32_t j = blockIdx.x;
     double v = 0.0;
     if (j == 3 * M + 9) {
-        for (int b = 0; b < sun_blocks; b++) v += sun[b];
-        g_theta[j] = float(v);
-        return;
-    }
-    for (int s = 0; s < n_sets; s++) {
-        const PartialSet &ps = sets[s];
-        int slots = 3 * int(ps.mc) + FIXED_SLOTS;
-        for (int b = 0; b < blocks; b++) {
+        for (int b = threadIdx.x; b < sun_blocks; b += blockDim.x) v += sun[b];
+    } else {
+        const int rows = n_sets * blocks;
+        for (int q = threadIdx.x; q < rows; q += blockDim.x) {
+            const PartialSet &ps = sets[q / blocks];
+            int b = q % blocks, slots = 3 * int(ps.mc) + FIXED_SLOTS;
             const double *row = ps.p + size_t(b) * slots;
             if (j < 3 * M) {
                 uint32_t m = j / 3;
@@ -589,7 +606,13 @@ __global__ void k_theta_final(const PartialSet *sets, int n_sets, int blocks, co
             }
         }
     }
-    g_theta[j] = float(v);
+    part[threadIdx.x] = v;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (int(threadIdx.x) < h) part[threadIdx.x] += part[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) g_theta[j] = float(part[0]);
 }
 
 }  // namespace lbd
@@ -751,7 +774,7 @@ void record_backward(lb_transport &t, cudaStream_t st) {
     lbd::k_sun_t<<<t.sun_blocks, 256, 0, st>>>(t.n_tex, t.g_dl.as<float4>(), t.dl0.as<float4>(),
                                               t.sun_partials.as<double>());
     uint32_t n_out = 3 * t.M + 10;
-    lbd::k_theta_final<<<tg(n_out), 256, 0, st>>>(t.sets_d.as<lbd::PartialSet>(), int(t.sets.size()), t.blocks,
+    lbd::k_theta_final<<<n_out, 256, 0, st>>>(t.sets_d.as<lbd::PartialSet>(), int(t.sets.size()), t.blocks,
                                                   t.sun_partials.as<double>(), t.sun_blocks, t.M, t.g_theta.as<float>());
     ck(cudaGetLastError(), "transport theta");
 }
@@ -833,6 +856,7 @@ void build(lb_transport &t, uint32_t max_checkpoints) {
         uint8_t *was = fa.as<uint8_t>(), *now = fb.as<uint8_t>();
         for (int q = 0; q < t.rings; q++) {
             lbd::k_fill_plan<<<tg(t.n_tex), 256, 0, st>>>(t.a, was, t.masks.as<uint8_t>() + size_t(q) * t.n_tex, now);
+            lbd::k_fill_plan_mark<<<tg(t.n_tex), 256, 0, st>>>(t.a, t.masks.as<uint8_t>() + size_t(q) * t.n_tex);
             std::swap(was, now);
         }
         lbd::k_smooth_wsum<<<tg(t.n_tex), 256, 0, st>>>(t.a, t.r, p.wr.as<float>(), t.wsum.as<float>());
