@@ -129,25 +129,6 @@ __device__ __forceinline__ bool inside_list(const Scene &S, const lb_params &P, 
     return nb / 16.0f > __uint_as_float(P.atlas[3]);
 }
 
-// Two inside tests at once, lanes 0..15 from oa (key ka), lanes 16..31 from ob (key kb): bit 0 when oa is
-// inside, bit 1 when ob is. The second test's work is counted only when the first point is inside (a
-// walk of the candidates one at a time would only then have tested the second).
-template <int BVH, bool COUNT>
-__device__ __forceinline__ unsigned inside_pair(const Scene &S, const lb_params &P, uint32_t seed, float3 oa, float3 ob,
-                                                float3 n, uint32_t ka, uint32_t kb, int lane, Count &c) {
-    Count keep = c;
-    Frame f = frame(n);
-    uint32_t r = uint32_t(lane & 15);
-    float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
-    Hit h = walk<BVH, COUNT>(S, lane < 16 ? oa : ob, d, P.ground[3], false, (lane < 16 ? ka : kb) + r + 7000u, seed, c);
-    unsigned m = __ballot_sync(FULL, h.tri != NONE && h.back);
-    float share = __uint_as_float(P.atlas[3]);
-    bool ia = __uint2float_rn(__popc(m & 0xffffu)) / 16.0f > share;
-    bool ib = __uint2float_rn(__popc(m >> 16)) / 16.0f > share;
-    if (!ia && lane >= 16) c = keep;
-    return (ia ? 1u : 0u) | (ib ? 2u : 0u);
-}
-
 template <bool COUNT>
 __device__ __forceinline__ void flush_counts(Count &c, unsigned long long *counters) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -207,21 +188,14 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
                                                    lane, c)
                               : inside_warp<BVH, COUNT>(S, P, seed, add(pos, lift), nrm, key, lane, c);
         if (inside) {
-            // the candidate points two at a time, a half-warp each; the first not inside, in order, wins
-            for (uint32_t q = 1u; q < 9u && pick == 0u; q += 2u) {
-                float2 ca = offset(q), cb = offset(q + 1u);
-                float3 pa = add(add(pos, scl(dx, ca.x)), scl(dy, ca.y));
-                float3 pb = add(add(pos, scl(dx, cb.x)), scl(dy, cb.y));
-                unsigned in = inside_pair<BVH, COUNT>(S, P, seed, add(pa, lift), add(pb, lift), nrm, key + q * 31u,
-                                                      key + (q + 1u) * 31u, lane, c);
-                if (!(in & 1u)) {
-                    at = pa;
+            for (uint32_t q = 1u; q < 9u; q++) {
+                float2 cc = offset(q);
+                float3 p = add(add(pos, scl(dx, cc.x)), scl(dy, cc.y));
+                if (!inside_warp<BVH, COUNT>(S, P, seed, add(p, lift), nrm, key + q * 31u, lane, c)) {
+                    at = p;
                     pick = q;
                     span = 0.4f;
-                } else if (!(in & 2u)) {
-                    at = pb;
-                    pick = q + 1u;
-                    span = 0.4f;
+                    break;
                 }
             }
             if (pick == 0u) {
