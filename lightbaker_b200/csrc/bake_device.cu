@@ -104,20 +104,29 @@ void build(lb_plan &p) {
                                p.P.affines.data(), p.P.affines.size() / 8);
     if (!p.dscene) throw std::runtime_error(lb_last_error());
 
-    // the cache (bake.rs:123-136)
+    // the cache (bake.rs:123-136); without a cache directory nothing is read or written, so the tiles' and
+    // chunks' hashes (only ever cache keys) are not computed
     lb::Cache cache(p.opt.cache);
-    lb::Boxes boxes(p.scene);
-    lb::Hash global = lb::global_hash(p.scene);
+    const bool caching = !p.opt.cache.empty();
+    std::optional<lb::Boxes> boxes;
+    lb::Hash global{};
+    if (caching) {
+        boxes.emplace(p.scene);
+        global = lb::global_hash(p.scene);
+    }
     float reach = b.gi_bounces > 0 ? std::fmax(b.gi_reach, b.ao_reach) : b.ao_reach;
     size_t nt = layout.tiles.size();
     p.hashes.resize(nt);
     p.lights.resize(nt);
+    if (caching) {
 #pragma omp parallel for schedule(dynamic, 1)
-    for (long long ti = 0; ti < (long long)nt; ti++) {
-        const lb::Tile &t = layout.tiles[ti];
-        p.hashes[ti] = lb::hash_reach(p.scene, boxes, global, lb::tile_box(p.scene, layout, t.charts), reach,
-                                      lb::tile_seed(p.scene, layout, t.key, t.charts));
-        if (auto bytes = cache.get("tile", p.hashes[ti])) p.lights[ti] = lb::TileLight::unpack(*bytes, size_t(t.w) * t.h);
+        for (long long ti = 0; ti < (long long)nt; ti++) {
+            const lb::Tile &t = layout.tiles[ti];
+            p.hashes[ti] = lb::hash_reach(p.scene, *boxes, global, lb::tile_box(p.scene, layout, t.charts), reach,
+                                          lb::tile_seed(p.scene, layout, t.key, t.charts));
+            if (auto bytes = cache.get("tile", p.hashes[ti]))
+                p.lights[ti] = lb::TileLight::unpack(*bytes, size_t(t.w) * t.h);
+        }
     }
     for (size_t i = 0; i < nt; i++)
         if (!p.lights[i]) p.dirty.push_back(i);
@@ -219,8 +228,9 @@ void build(lb_plan &p) {
             std::memcpy(seed.data(), &kv.first.first, 4);
             std::memcpy(seed.data() + 4, &kv.first.second, 4);
             seed.insert(seed.end(), vjson.begin(), vjson.end());
-            lb::Hash hash = lb::hash_reach(p.scene, boxes, global, bx, b.gi_reach, seed);
-            auto got = cache.get("probes", hash);
+            lb::Hash hash{};
+            if (caching) hash = lb::hash_reach(p.scene, *boxes, global, bx, b.gi_reach, seed);
+            auto got = caching ? cache.get("probes", hash) : std::nullopt;
             if (got && got->size() == kv.second.size() * 64) {
                 for (size_t i = 0; i < kv.second.size(); i++)
                     std::memcpy(&probes_init[size_t(kv.second[i]) * 16], got->data() + i * 64, 64);
@@ -607,13 +617,22 @@ lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_
         p->refill_direct = p->refill_gather = g->refill;
         p->near_direct = g->near;
         p->occ_direct = p->occ_gather = g->occ;
+        auto t0 = std::chrono::steady_clock::now();
         build(*p);
+        double t_build = since(t0);
+        t0 = std::chrono::steady_clock::now();
         if (p->autotune) autotune(*p);
+        double t_tune = since(t0);
+        t0 = std::chrono::steady_clock::now();
         capture(*p);
-        if (p->opt.log)
+        double t_capture = since(t0);
+        if (p->opt.log) {
             p->opt.log(std::to_string(p->dirty.size()) + " of " + std::to_string(p->P.layout.tiles.size()) +
                        " tiles to bake on the device, " + std::to_string(p->n_cov) + " texels, " +
                        std::to_string(p->n_todo) + " probes");
+            p->opt.log("timing: build " + std::to_string(t_build) + " s, autotune " + std::to_string(t_tune) +
+                       " s, capture " + std::to_string(t_capture) + " s");
+        }
         return p.release();
     } catch (const std::exception &e) {
         lb_set_error(e.what());

@@ -409,18 +409,20 @@ __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float
 
 // trace() over a leaf list: the nearest accepted hit within tmax among the listed leaves' triangles,
 // with the walk's box test (culled by the nearest hit so far) and triangle test. The list is nearest
-// first from the ray's origin (dist2: each box's squared distance from it), so once a box lies farther
-// than the nearest hit so far (by a relative margin far above the rounding of t, |d| and the distance),
-// neither it nor any later box can hold a nearer hit and the walk ends: the same hit as the whole list.
+// first from its centre (dist2: each box's squared distance from it), and the ray starts within `shift`
+// of that centre, so once a box lies farther than the nearest hit so far plus shift (by a relative
+// margin far above the rounding of t, |d| and the distance), neither it nor any later box can hold a
+// nearer hit and the walk ends: the same hit as the whole list.
 template <bool COUNT>
 __device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, const float *dist2, int nl, float3 o,
-                                          float3 d, float tmax, uint32_t ray, uint32_t seed, Count &c) {
+                                          float3 d, float tmax, uint32_t ray, uint32_t seed, Count &c,
+                                          float shift = 0.0f) {
     Hit hit{tmax, NONE, false};
     c.rays++;
     float3 dd = mk(fabsf(d.x) < 1e-12f ? 1e-12f : d.x, fabsf(d.y) < 1e-12f ? 1e-12f : d.y,
                    fabsf(d.z) < 1e-12f ? 1e-12f : d.z);
     float3 inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
-    float lim = tmax * 1.0001f + 1e-5f, lim2 = lim * lim;
+    float lim = (tmax + shift) * 1.0001f + 1e-5f, lim2 = lim * lim;
     for (int k = 0; k < nl; k++) {
         if (dist2[k] > lim2) break;
         uint32_t node = list[k];
@@ -444,7 +446,7 @@ __device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, 
             float t = dot3(xyz(e2), q) * id;
             if (t > 1e-4f && t < hit.t && stops<COUNT>(S, i, v0.w, ray, seed, c)) {
                 hit = Hit{t, i, det < 0.0f};
-                lim = t * 1.0001f + 1e-5f;
+                lim = (t + shift) * 1.0001f + 1e-5f;
                 lim2 = lim * lim;
             }
         }

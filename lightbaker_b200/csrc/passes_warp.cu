@@ -110,19 +110,18 @@ __device__ __forceinline__ bool inside_warp(const Scene &S, const lb_params &P, 
     return nb / 16.0f > __uint_as_float(P.atlas[3]);
 }
 
-// The same test over the texel's leaf list (the list gathered from o: the test's rays start there, head
-// into the same hemisphere and reach no farther than the occlusion rays, so the list holds every leaf they
-// can meet).
+// The same test over the texel's leaf list (a list that holds every leaf the test's rays can meet: they
+// start within `shift` of its centre, head into the same hemisphere and reach no farther than the list).
 template <bool COUNT>
 __device__ __forceinline__ bool inside_list(const Scene &S, const lb_params &P, uint32_t seed, const uint32_t *list,
                                             const float *dist2, int nl, float3 o, float3 n, uint32_t key, int lane,
-                                            Count &c) {
+                                            Count &c, float shift) {
     bool back = false;
     if (lane < 16) {
         Frame f = frame(n);
         uint32_t r = uint32_t(lane);
         float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
-        Hit h = trace_list<COUNT>(S, list, dist2, nl, o, d, P.ground[3], key + r + 7000u, seed, c);
+        Hit h = trace_list<COUNT>(S, list, dist2, nl, o, d, P.ground[3], key + r + 7000u, seed, c, shift);
         back = h.tri != NONE && h.back;
     }
     float nb = __uint2float_rn(__popc(__ballot_sync(FULL, back)));
@@ -177,21 +176,43 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
         uint32_t pick = 0u;
         float span = 1.0f;
         const int wi = threadIdx.x >> 5;
-        // the leaves within the occlusion reach of the texel's own point, gathered once: its inside test
-        // and, when the point stays, its occlusion rays walk them
+        // The leaves around the texel's own point c0, gathered once, far enough for every ray of the inside
+        // tests and the occlusion rays from any candidate point (reach plus the farthest candidate's
+        // distance from c0). A ray from another point o uses the list when o is not behind c0's plane by
+        // more than half the list's front margin (the list leaves out boxes wholly behind that plane, and
+        // every ray here heads into the normal's hemisphere); its walk's early end counts |o - c0|.
+        auto candidate = [&](uint32_t q) -> float3 {
+            if (q == 9u) return add(pos, scl(nrm, PUSH));
+            float2 cc = offset(q);
+            return add(add(pos, scl(dx, cc.x)), scl(dy, cc.y));
+        };
+        const float3 c0 = add(pos, lift);
         int nl = -1;
+        float rball = P.reach[0];
         const bool listed = BVH == 2 && WALK == 1 && near && P.counts[1] <= uint32_t(AO_CAP);
-        if (listed)
-            nl = ball_leaves<COUNT>(S, add(pos, lift), P.reach[0], nrm, s_front[wi][0], s_front[wi][1], s_list[wi],
-                                    s_dist[wi], lane, c);
-        bool inside = nl >= 0 ? inside_list<COUNT>(S, P, seed, s_list[wi], s_dist[wi], nl, add(pos, lift), nrm, key,
-                                                   lane, c)
-                              : inside_warp<BVH, COUNT>(S, P, seed, add(pos, lift), nrm, key, lane, c);
-        if (inside) {
+        if (listed) {
+            float far_ = 0.0f;
+            for (uint32_t q = 1u; q <= 9u; q++) far_ = fmaxf(far_, sqrtf(dot3(sub(add(candidate(q), lift), c0),
+                                                                              sub(add(candidate(q), lift), c0))));
+            rball = P.reach[0] + far_ * 1.001f + 1e-5f;
+            nl = ball_leaves<COUNT>(S, c0, rball, nrm, s_front[wi][0], s_front[wi][1], s_list[wi], s_dist[wi], lane, c);
+        }
+        const float front = -(rball * 1e-3f + 1e-4f) * 0.5f;
+        auto listed_from = [&](float3 o, float &shift) -> bool {
+            float3 v = sub(o, c0);
+            shift = sqrtf(dot3(v, v)) * 1.001f + 1e-6f;
+            return nl >= 0 && dot3(v, nrm) >= front;
+        };
+        auto inside_at = [&](float3 o, uint32_t k) -> bool {
+            float shift;
+            if (listed_from(o, shift))
+                return inside_list<COUNT>(S, P, seed, s_list[wi], s_dist[wi], nl, o, nrm, k, lane, c, shift);
+            return inside_warp<BVH, COUNT>(S, P, seed, o, nrm, k, lane, c);
+        };
+        if (inside_at(c0, key)) {
             for (uint32_t q = 1u; q < 9u; q++) {
-                float2 cc = offset(q);
-                float3 p = add(add(pos, scl(dx, cc.x)), scl(dy, cc.y));
-                if (!inside_warp<BVH, COUNT>(S, P, seed, add(p, lift), nrm, key + q * 31u, lane, c)) {
+                float3 p = candidate(q);
+                if (!inside_at(add(p, lift), key + q * 31u)) {
                     at = p;
                     pick = q;
                     span = 0.4f;
@@ -199,8 +220,8 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
                 }
             }
             if (pick == 0u) {
-                float3 p = add(pos, scl(nrm, PUSH));
-                if (!inside_warp<BVH, COUNT>(S, P, seed, add(p, lift), nrm, key + 331u, lane, c)) {
+                float3 p = candidate(9u);
+                if (!inside_at(add(p, lift), key + 331u)) {
                     at = p;
                     pick = 9u;
                     span = 0.4f;
@@ -245,21 +266,24 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
         uint32_t nback = 0;
         const RayOrder ord(rays, AO_CAP, group, lane);
         const int w = threadIdx.x >> 5;
-        // the leaves within reach of this texel's occlusion rays, once for all of them
-        // a moved point gathers its own leaves (the list above is the texel's own point's)
-        if (pick != 0u) {
+        // the occlusion rays start at o: the texel's own list when it serves o, else o's own
+        float ao_shift = 0.0f;
+        if (pick != 0u && !listed_from(o, ao_shift)) {
+            ao_shift = 0.0f;
             nl = -1;
             if (listed)
                 nl = ball_leaves<COUNT>(S, o, P.reach[0], nrm, s_front[w][0], s_front[w][1], s_list[w], s_dist[w], lane,
                                         c);
         }
+        if (pick == 0u) listed_from(o, ao_shift);
         if (nl >= 0) {
             uint32_t myback = 0;
             for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
                 uint32_t r = ord.ray(r0 >> 5);
                 if (r < rays) {
                     float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
-                    Hit h = trace_list<COUNT>(S, s_list[w], s_dist[w], nl, o, d, P.reach[0], key + r + 2000u, seed, c);
+                    Hit h = trace_list<COUNT>(S, s_list[w], s_dist[w], nl, o, d, P.reach[0], key + r + 2000u, seed, c,
+                                              ao_shift);
                     float term = 0.0f;
                     bool hit = h.tri != NONE;
                     if (hit) {
