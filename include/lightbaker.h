@@ -127,12 +127,14 @@ int lb_run_async(lb_gpu *gpu, lb_scene *scene, int pass, const lb_params *params
 int lb_set_pass_kernel(lb_gpu *gpu, int kind);
 /* The warp kernels' ray order within an item: a warp's 32 rays of a round share the top `group` bits of
  * the ray index (and the bottom bits that remain): large values give the shader's order (bands of
- * elevation), 0 wedges of azimuth. Results are identical; speed is not (lb_autotune picks). */
+ * elevation), 0 (the default) wedges of azimuth. Results are identical; speed is not (the device bake's
+ * autotuner picks). */
 int lb_set_ray_order(lb_gpu *gpu, int direct, int gather);
-/* Leaf lists for the warp kernels' occlusion rays over the BVH2 (default on): a warp gathers once for
- * a texel the leaves within the occlusion reach of its sample point, on its front side, nearest first,
- * and every occlusion ray tests that list instead of walking the tree. Same hits (between triangles
- * at exactly equal distance the first found in list order). */
+/* Leaf lists for the warp kernels' direct pass over the BVH2 (default on): a warp gathers once for a
+ * texel the leaves within the occlusion reach (widened by its farthest candidate point) of its own point,
+ * on its front side, nearest first, and its inside-test and occlusion rays test that list instead of
+ * walking the tree. Same hits (between triangles at exactly equal distance the first found in list
+ * order). */
 int lb_set_near(lb_gpu *gpu, int on);
 /* Register cap of the warp kernels over the BVH2 (direct and gather, without counting): 0 (default) the
  * compiler's own budget; 3 or 4 registers capped so that this many 256-thread blocks share an SM (more

@@ -20,7 +20,7 @@ struct lb_gpu {
     cudaStream_t stream = nullptr;
     bool counting = false;
     int kernel = 0;  // lb_run's kernels: 0 a thread an item, 1 a warp an item
-    int group_direct = 8, group_gather = 8;  // the warp kernels' ray order (passes_warp.cu); 8: the shader's
+    int group_direct = 0, group_gather = 0;  // the warp kernels' ray order (passes_warp.cu); 0: wedges of azimuth
     int bvh = 2;  // the warp kernels' BVH: 2 the reference's, 8 the 8-wide one
     int refill = 0;  // the warp kernels' lane refill (occlusion and gather rays over the BVH2)
     int near = 1;    // the warp kernels' leaf list for occlusion rays (BVH2)
