@@ -34,6 +34,18 @@ def test_bvh2_structure(name):
 
 
 @pytest.mark.parametrize("name", ["reference_test", "small_map", "map_100m"])
+def test_bvh2_bytes_are_the_serial_builds(name):
+    """The BVH2's bytes (node order, triangle order: the opacity coin and the hit indices depend on them)
+    equal those of the serial build the golden hashes were made with (tests/golden/make_bvh_hashes.py)."""
+    import json
+    from pathlib import Path
+    want = json.loads((Path(__file__).parent / "golden" / "bvh_hashes.json").read_text())[name]
+    P = lb.prepare(scenes.WORKLOADS[name]())
+    assert (len(P.nodes), len(P.tris)) == (want["nodes"], want["tris"])
+    assert lb.blake3(P.nodes.tobytes() + P.tris.tobytes()).hex() == want["blake3"]
+
+
+@pytest.mark.parametrize("name", ["reference_test", "small_map", "map_100m"])
 def test_bvh8_collapse(name):
     P = lb.prepare(scenes.WORKLOADS[name]())
     n8, depth = C.c_uint64(), C.c_uint64()
