@@ -340,7 +340,9 @@ void autotune(lb_plan &p) {
     if (p.n_cov == 0) return;
     cudaStream_t st = p.g->stream;
     lbd::Scene S = lb_scene_view(p.dscene);
-    uint32_t want = std::min<uint32_t>(p.n_cov, 16384), stride = std::max<uint32_t>(1, p.n_cov / want);
+    // a sample of texels spread over the map, large enough to keep every SM busy for a while (a small one
+    // times the launch's tail, not its walk)
+    uint32_t want = std::min<uint32_t>(p.n_cov, 65536), stride = std::max<uint32_t>(1, p.n_cov / want);
     std::vector<uint32_t> sample;
     {
         std::vector<uint32_t> all(p.n_cov);
@@ -354,13 +356,13 @@ void autotune(lb_plan &p) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const int orders[] = {8, 2, 0};
+    const int orders[] = {0, 8};
     struct Shape {
         int bvh, refill, near, occ;
     };
-    // walks (BVH2 with leaf lists, plain, with lane refill; the 8-wide BVH) and register caps
-    const Shape shapes[] = {{2, 0, 1, 0}, {2, 0, 1, 3}, {2, 0, 1, 4}, {2, 0, 0, 0}, {2, 0, 0, 3},
-                            {2, 0, 0, 4}, {2, 1, 0, 0}, {8, 0, 0, 0}};
+    // walks (the BVH2 with and without leaf lists) and register caps, each at full occupancy; lane refill
+    // and the 8-wide BVH lost on every workload measured here and are left to the gpu handle's settings
+    const Shape shapes[] = {{2, 0, 1, 0}, {2, 0, 1, 3}, {2, 0, 1, 4}, {2, 0, 0, 0}, {2, 0, 0, 3}, {2, 0, 0, 4}};
     std::string report;
     for (int pass : {LB_PASS_DIRECT, LB_PASS_GATHER}) {
         float best = 1e30f;
@@ -375,7 +377,7 @@ void autotune(lb_plan &p) {
             probe.occ = sh.occ;
             int full = lb_warp_pass_blocks(probe);
             int per_sm = std::max(1, full / std::max(1, p.g->sms));
-            for (int bps = per_sm; bps >= 1; bps = bps > 1 ? std::max(1, bps / 2) : 0) {
+            for (int bps : {per_sm}) {
                 WarpPass w{};
                 w.pass = pass;
                 w.S = &S;
@@ -411,7 +413,6 @@ void autotune(lb_plan &p) {
                     best_near = sh.near;
                     best_occ = sh.occ;
                 }
-                if (bps == 1) break;
             }
         }
         if (pass == LB_PASS_DIRECT) {

@@ -1,8 +1,12 @@
 #include "bvh.h"
 
+#include <omp.h>
+
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <tuple>
+#include <vector>
 
 namespace lb {
 
@@ -26,12 +30,36 @@ float area(Vec3 mn, Vec3 mx) {
     return d.x * d.y + d.y * d.z + d.z * d.x;
 }
 
+// Above this many primitives a node's bounds and bins are gathered by all threads, each over one
+// contiguous run of the primitives, and the runs' results are merged in run order: fmin and fmax keep
+// the first of equal values (so of -0 and +0 too), so the merge gives the serial fold's bits.
+constexpr size_t PARALLEL_BINS = 1 << 15;
+
+// the contiguous run [lo, hi) of n items that part k of parts takes
+inline void run_of(size_t n, int k, int parts, size_t &lo, size_t &hi) {
+    lo = n * size_t(k) / size_t(parts);
+    hi = n * size_t(k + 1) / size_t(parts);
+}
+
 // bvh.rs:119-151: the axis and plane of the cheapest binned split, if one beats a leaf
 bool best_split(const Prim *p, size_t n, int &axis_out, float &at_out) {
     Vec3 cmin = Vec3::splat(INFINITY), cmax = Vec3::splat(-INFINITY), pmin = cmin, pmax = cmax;
-    for (size_t i = 0; i < n; i++) {
-        bounds_add(cmin, cmax, p[i].centre, p[i].centre);
-        bounds_add(pmin, pmax, p[i].min, p[i].max);
+    const int parts = n >= PARALLEL_BINS ? std::max(1, std::min(omp_get_max_threads(), 64)) : 1;
+    {
+        std::vector<Vec3> a(parts, Vec3::splat(INFINITY)), b(parts, Vec3::splat(-INFINITY)), c = a, d = b;
+#pragma omp parallel for schedule(static, 1) if (parts > 1)
+        for (int k = 0; k < parts; k++) {
+            size_t lo, hi;
+            run_of(n, k, parts, lo, hi);
+            for (size_t i = lo; i < hi; i++) {
+                bounds_add(a[k], b[k], p[i].centre, p[i].centre);
+                bounds_add(c[k], d[k], p[i].min, p[i].max);
+            }
+        }
+        for (int k = 0; k < parts; k++) {
+            bounds_add(cmin, cmax, a[k], b[k]);
+            bounds_add(pmin, pmax, c[k], d[k]);
+        }
     }
     float leaf_cost = float(n) * area(pmin, pmax);
     bool have = false;
@@ -47,14 +75,29 @@ bool best_split(const Prim *p, size_t n, int &axis_out, float &at_out) {
             bmax[b] = Vec3::splat(-INFINITY);
             bn[b] = 0;
         }
-        for (size_t i = 0; i < n; i++) {
-            float f = (p[i].centre[axis] - cmin[axis]) / extent * float(BINS);
-            size_t b = f > 0.0f ? size_t(f) : 0;  // Rust `as usize`: truncation, saturating at 0
-            if (b > BINS - 1) b = BINS - 1;
-            bmin[b] = bmin[b].min(p[i].min);
-            bmax[b] = bmax[b].max(p[i].max);
-            bn[b]++;
+        std::vector<Vec3> tmin(size_t(parts) * BINS, Vec3::splat(INFINITY)), tmax(size_t(parts) * BINS, Vec3::splat(-INFINITY));
+        std::vector<uint32_t> tn(size_t(parts) * BINS, 0);
+#pragma omp parallel for schedule(static, 1) if (parts > 1)
+        for (int k = 0; k < parts; k++) {
+            size_t lo, hi;
+            run_of(n, k, parts, lo, hi);
+            Vec3 *mn = &tmin[size_t(k) * BINS], *mx = &tmax[size_t(k) * BINS];
+            uint32_t *cn = &tn[size_t(k) * BINS];
+            for (size_t i = lo; i < hi; i++) {
+                float f = (p[i].centre[axis] - cmin[axis]) / extent * float(BINS);
+                size_t b = f > 0.0f ? size_t(f) : 0;  // Rust `as usize`: truncation, saturating at 0
+                if (b > BINS - 1) b = BINS - 1;
+                mn[b] = mn[b].min(p[i].min);
+                mx[b] = mx[b].max(p[i].max);
+                cn[b]++;
+            }
         }
+        for (int k = 0; k < parts; k++)
+            for (size_t b = 0; b < BINS; b++) {
+                bmin[b] = bmin[b].min(tmin[size_t(k) * BINS + b]);
+                bmax[b] = bmax[b].max(tmax[size_t(k) * BINS + b]);
+                bn[b] += tn[size_t(k) * BINS + b];
+            }
         for (size_t s = 1; s < BINS; s++) {
             uint32_t ln = 0, rn = 0;
             Vec3 lmin = Vec3::splat(INFINITY), lmax = Vec3::splat(-INFINITY), rmin = lmin, rmax = lmax;
@@ -92,6 +135,43 @@ size_t partition(Prim *p, size_t n, int axis, float at) {
         }
     return i;
 }
+// bvh.rs:62-104 over prims[start, end) alone: its nodes in the order the walk allocates them, node 0 the
+// range's root; an inner node's `first` is its left child's local index, a leaf's the global index of its
+// first triangle.
+void build_subtree(std::vector<Prim> &prims, size_t start0, size_t end0, std::vector<lb_node> &nodes) {
+    nodes.assign(1, lb_node{});
+    auto set = [&](size_t ni, Vec3 mn, uint32_t first, Vec3 mx, uint32_t count) {
+        nodes[ni] = lb_node{{mn.x, mn.y, mn.z}, first, {mx.x, mx.y, mx.z}, count};
+    };
+    std::vector<std::tuple<size_t, size_t, size_t>> stack{{0, start0, end0}};
+    while (!stack.empty()) {
+        auto [ni, start, end] = stack.back();
+        stack.pop_back();
+        Prim *slice = prims.data() + start;
+        size_t n = end - start;
+        Vec3 bmin = Vec3::splat(INFINITY), bmax = Vec3::splat(-INFINITY);
+        for (size_t i = 0; i < n; i++) bounds_add(bmin, bmax, slice[i].min, slice[i].max);
+        int axis;
+        float at;
+        bool split = n > LEAF && best_split(slice, n, axis, at);
+        if (!split) {
+            set(ni, bmin, uint32_t(start), bmax, uint32_t(n));
+            continue;
+        }
+        size_t mid = start + partition(slice, n, axis, at);
+        if (mid == start || mid == end) mid = start + n / 2;
+        if (mid - start == 0 || end - mid == 0) {
+            set(ni, bmin, uint32_t(start), bmax, uint32_t(n));
+            continue;
+        }
+        size_t left = nodes.size();
+        nodes.push_back(lb_node{});
+        nodes.push_back(lb_node{});
+        set(ni, bmin, uint32_t(left), bmax, 0);
+        stack.emplace_back(left + 1, mid, end);
+        stack.emplace_back(left, start, mid);
+    }
+}
 }  // namespace
 
 // bvh.rs:50-106
@@ -121,36 +201,92 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
         out.tris.push_back(lb_tri{});
         return out;
     }
-    auto set = [&](size_t ni, Vec3 mn, uint32_t first, Vec3 mx, uint32_t count) {
-        out.nodes[ni] = lb_node{{mn.x, mn.y, mn.z}, first, {mx.x, mx.y, mx.z}, count};
+    // The serial walk below (bvh.rs:62-104) pops a node, decides it a leaf or splits its primitives in
+    // place and allocates its two children next, then walks the left subtree before the right one. So
+    // every subtree's nodes but its root come out as one contiguous run, in the order the same walk over
+    // the subtree alone allocates them. Nodes of fewer than `cut` primitives become subtrees built on
+    // their own (in parallel: their primitive ranges are disjoint); the top of the tree is walked first,
+    // then walked again in the serial order, each subtree's run spliced in when its root is popped.
+    // Indices, node bytes and triangle order are the serial build's.
+    struct Top {
+        size_t start, end;
+        bool leaf = false, task = false;
+        Vec3 bmin, bmax;
+        int left = -1, right = -1;
+        size_t task_id = 0;
     };
-    std::vector<std::tuple<size_t, size_t, size_t>> stack{{0, 0, prims.size()}};
-    while (!stack.empty()) {
-        auto [ni, start, end] = stack.back();
-        stack.pop_back();
+    const size_t cut = std::max<size_t>(2048, prims.size() / 256);
+    std::vector<Top> top;
+    std::vector<std::pair<size_t, size_t>> tasks;
+    top.push_back(Top{0, prims.size()});
+    std::vector<int> todo{0};
+    while (!todo.empty()) {
+        int id = todo.back();
+        todo.pop_back();
+        size_t start = top[id].start, end = top[id].end, n = end - start;
+        if (n < cut) {
+            top[id].task = true;
+            top[id].task_id = tasks.size();
+            tasks.emplace_back(start, end);
+            continue;
+        }
         Prim *slice = prims.data() + start;
-        size_t n = end - start;
         Vec3 bmin = Vec3::splat(INFINITY), bmax = Vec3::splat(-INFINITY);
         for (size_t i = 0; i < n; i++) bounds_add(bmin, bmax, slice[i].min, slice[i].max);
+        top[id].bmin = bmin;
+        top[id].bmax = bmax;
         int axis;
         float at;
         bool split = n > LEAF && best_split(slice, n, axis, at);
+        size_t mid = 0;
+        if (split) {
+            mid = start + partition(slice, n, axis, at);
+            if (mid == start || mid == end) mid = start + n / 2;
+            if (mid - start == 0 || end - mid == 0) split = false;
+        }
         if (!split) {
-            set(ni, bmin, uint32_t(start), bmax, uint32_t(n));
+            top[id].leaf = true;
             continue;
         }
-        size_t mid = start + partition(slice, n, axis, at);
-        if (mid == start || mid == end) mid = start + n / 2;
-        if (mid - start == 0 || end - mid == 0) {
-            set(ni, bmin, uint32_t(start), bmax, uint32_t(n));
-            continue;
+        int l = int(top.size()), r = l + 1;
+        top.push_back(Top{start, mid});
+        top.push_back(Top{mid, end});
+        top[id].left = l;
+        top[id].right = r;
+        todo.push_back(r);
+        todo.push_back(l);
+    }
+    std::vector<std::vector<lb_node>> runs(tasks.size());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long k = 0; k < (long long)tasks.size(); k++) build_subtree(prims, tasks[k].first, tasks[k].second, runs[k]);
+    auto set = [&](size_t ni, Vec3 mn, uint32_t first, Vec3 mx, uint32_t count) {
+        out.nodes[ni] = lb_node{{mn.x, mn.y, mn.z}, first, {mx.x, mx.y, mx.z}, count};
+    };
+    std::vector<std::pair<size_t, int>> stack{{0, 0}};
+    while (!stack.empty()) {
+        auto [ni, id] = stack.back();
+        stack.pop_back();
+        const Top &t = top[id];
+        if (t.task) {
+            const std::vector<lb_node> &run = runs[t.task_id];
+            size_t base = out.nodes.size();
+            // local node k (k >= 1) lands at base + k - 1; a leaf's first is already a triangle index
+            auto place = [&](lb_node v) {
+                if (v.count == 0) v.first = uint32_t(base + v.first - 1);
+                return v;
+            };
+            out.nodes[ni] = place(run[0]);
+            for (size_t k = 1; k < run.size(); k++) out.nodes.push_back(place(run[k]));
+        } else if (t.leaf) {
+            set(ni, t.bmin, uint32_t(t.start), t.bmax, uint32_t(t.end - t.start));
+        } else {
+            size_t left = out.nodes.size();
+            out.nodes.push_back(lb_node{});
+            out.nodes.push_back(lb_node{});
+            set(ni, t.bmin, uint32_t(left), t.bmax, 0);
+            stack.emplace_back(left + 1, t.right);
+            stack.emplace_back(left, t.left);
         }
-        size_t left = out.nodes.size();
-        out.nodes.push_back(lb_node{});
-        out.nodes.push_back(lb_node{});
-        set(ni, bmin, uint32_t(left), bmax, 0);
-        stack.emplace_back(left + 1, mid, end);
-        stack.emplace_back(left, start, mid);
     }
     out.tris.reserve(prims.size());
     for (auto &p : prims) out.tris.push_back(p.tri);
