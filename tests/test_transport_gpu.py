@@ -155,6 +155,53 @@ def test_l2_loss_to_a_perturbed_target(small):
     np.testing.assert_allclose(grad, want, rtol=0, atol=1e-4 * np.abs(want).max())
 
 
+def test_differentiation_workload(gpu):
+    """The differentiation workload as stated for the small map: three bounces; the parameters are the 16
+    box albedos (the ground's held fixed), one sky colour (zenith = horizon = ground) and the sun's scale;
+    the loss is L2 to a target baked at the parameters + N(0, 0.05) (seed 1). The adjoint's gradient is
+    checked against the float64 restatement's autograd gradient and against central differences
+    (h = 1e-3) of the float64 loss."""
+    import torch
+    tr = lb.Transport(scenes.small_map(seed=0, bounces=3), gpu)
+    assert tr.shape.bounces == 3 and tr.n_materials == 17
+    th0 = tr.theta0()
+    M = tr.n_materials
+
+    def full(phi):  # the reduced parameters into theta (numpy or torch)
+        cat = torch.cat if isinstance(phi, torch.Tensor) else np.concatenate
+        head = th0[:3] if not isinstance(phi, torch.Tensor) else torch.tensor(th0[:3], dtype=phi.dtype)
+        sky = phi[48:51]
+        return cat([head, phi[:48], sky, sky, sky, phi[51:52]])
+
+    phi0 = np.concatenate([th0[3:3 * M], th0[3 * M:3 * M + 3], th0[-1:]]).astype(np.float64)
+    target_phi = phi0 + np.random.default_rng(1).normal(0.0, 0.05, phi0.shape)
+    target = tr.forward(full(target_phi).astype(np.float32)).astype(np.float64)
+    y = tr.forward(full(phi0).astype(np.float32)).astype(np.float64)
+    g_full = tr.backward(2.0 * (y - target))
+    g_phi = np.concatenate([g_full[3:3 * M], g_full[3 * M:3 * M + 3] + g_full[3 * M + 3:3 * M + 6] +
+                            g_full[3 * M + 6:3 * M + 9], g_full[-1:]])
+    ref = T.TransportRef(_arrays(tr))
+    tgt = torch.from_numpy(target.reshape(-1, 3))
+
+    def loss64(phi):
+        return ((ref.forward(full(phi)) - tgt) ** 2).sum()
+
+    p = torch.tensor(phi0, requires_grad=True)
+    loss64(p).backward()
+    want = p.grad.numpy()
+    scale = np.abs(want).max()
+    np.testing.assert_allclose(g_phi, want, rtol=0, atol=1e-4 * scale)
+    h = 1e-3
+    for j in [0, 1, 2, 20, 47, 48, 49, 50, 51]:
+        e = np.zeros_like(phi0)
+        e[j] = h
+        with torch.no_grad():
+            fd = (loss64(torch.from_numpy(phi0 + e)) - loss64(torch.from_numpy(phi0 - e))).item() / (2 * h)
+        assert abs(fd - want[j]) <= 1e-5 * scale, (j, fd, want[j])
+        assert abs(fd - g_phi[j]) <= 1e-4 * scale, (j, fd, g_phi[j])
+    tr.close()
+
+
 def test_checkpoints_recompute_the_same_bits(small, gpu):
     scene, tr = small
     assert tr.shape.bounces == 2 and tr.shape.checkpoints == 2
