@@ -93,6 +93,8 @@ void build(lb_plan &p) {
     const lb::BakeSettings &b = h.bake;
     const lb::LightmapSettings &lm = h.lightmap;
     p.P = lb::prepare(p.scene);
+    auto mark = [&](const char *what) { p.build_phases += std::string(what) + " " + std::to_string(since(t0)) + " s; "; };
+    mark("layout and BVH");
     lb::Layout &layout = p.P.layout;
     p.aw = layout.width;
     p.ah = layout.height;
@@ -144,6 +146,7 @@ void build(lb_plan &p) {
     }
     p.n_all = off;
     if (p.dirty.empty()) p.n_dirty_texels = 0;
+    mark("upload and cache");
 
     // rasterise the dirty tiles (bake.rs:138-149)
     std::vector<lb_texel> tex(p.n_dirty_texels);
@@ -160,8 +163,9 @@ void build(lb_plan &p) {
         }
     p.n_cov = uint32_t(cov_idx.size());
     // at most one gathered texel a chart in each ds x ds block (bake.rs:286-297): the gather records' bound
-    p.max_gathered = 0;
-    for (size_t wi = 0; wi < p.dirty.size(); wi++) {
+    std::vector<uint64_t> pairs(p.dirty.size(), 0);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long wi = 0; wi < (long long)p.dirty.size(); wi++) {
         const DTile &t = p.tiles_all[wi];
         std::vector<uint64_t> keys;
         for (uint32_t y = 0; y < t.h; y++)
@@ -173,8 +177,11 @@ void build(lb_plan &p) {
                 keys.push_back((uint64_t((y / p.ds) * ((t.w + p.ds - 1) / p.ds) + x / p.ds) << 32) | chart);
             }
         std::sort(keys.begin(), keys.end());
-        p.max_gathered += uint64_t(std::unique(keys.begin(), keys.end()) - keys.begin());
+        pairs[wi] = uint64_t(std::unique(keys.begin(), keys.end()) - keys.begin());
     }
+    p.max_gathered = 0;
+    for (uint64_t n : pairs) p.max_gathered += n;
+    mark("raster");
 
     // cached tiles' light, the atlas owner map and the atlas the first bounce reads
     std::vector<uint8_t> known(p.n_all, 0), state(p.n_all, 0);
@@ -247,6 +254,7 @@ void build(lb_plan &p) {
         p.n_todo = uint32_t(probe_items.size());
     }
 
+    mark("atlas and volume");
     // device memory
     size_t N = p.n_dirty_texels ? p.n_dirty_texels : 1, A = p.n_all ? p.n_all : 1;
     std::vector<DTile> dirty_tiles(p.tiles_all.begin(), p.tiles_all.begin() + p.dirty.size());
@@ -330,6 +338,7 @@ void build(lb_plan &p) {
     p.blocks_direct = warp_blocks(p.g, LB_PASS_DIRECT);
     p.blocks_gather = warp_blocks(p.g, LB_PASS_GATHER);
     p.blocks_volume = warp_blocks(p.g, LB_PASS_VOLUME);
+    mark("device arrays");
     p.t_prepare = since(t0);
 }
 
@@ -635,6 +644,7 @@ lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_
                        std::to_string(p->n_todo) + " probes");
             p->opt.log("timing: build " + std::to_string(t_build) + " s, autotune " + std::to_string(t_tune) +
                        " s, capture " + std::to_string(t_capture) + " s");
+            p->opt.log("timing of the build, cumulative: " + p->build_phases);
         }
         return p.release();
     } catch (const std::exception &e) {

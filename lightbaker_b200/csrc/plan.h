@@ -100,6 +100,7 @@ struct lb_plan {
     uint64_t max_gathered = 0;  // a bound on the gathered texels (records are sized by it)
     lbplan::DBuf records, theta0;
     std::string tuned;  // what the autotuner picked
+    std::string build_phases;  // the host build's phases, seconds since its start
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     double t_prepare = 0;
