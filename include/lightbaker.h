@@ -96,6 +96,37 @@ lb_scene *lb_scene_upload(lb_gpu *gpu, const lb_node *nodes, size_t n_nodes, con
                           size_t n_tris, const float *materials /* 4 a material */, size_t n_materials,
                           const float *charts /* 8 a chart */, size_t n_charts);
 void lb_scene_free(lb_scene *scene);
+/* The triangles' exact vertices (9 floats a triangle: v0, v1, v2 of tris[i], in the uploaded order;
+ * lb_prepared_get_vertices gives them for a prepared scene), or NULL and 0 to drop them. No counterpart in
+ * the reference. With vertices every walk over this scene uses the watertight ray/triangle test (Woop,
+ * Benthin and Wald, JCGT 2013) in place of the shader's Moller-Trumbore, and widens each box's exit by
+ * 1 + 4e-7 so no box that holds a hit is culled: no ray passes between two triangles that share an
+ * edge. Hit/miss, faces and t then differ from the shader's only for rays through an edge or a vertex
+ * (within 1e-4 in barycentric terms), grazing a triangle, or ending within rounding of 1e-4 or tmax. */
+int lb_scene_set_vertices(lb_gpu *gpu, lb_scene *scene, const float *verts, size_t n_tris);
+
+/* One ray for lb_trace: origin, maximum distance, direction, and its key (the ray number the shader's
+ * opacity coin reads, trace.wgsl:69-72). */
+typedef struct lb_ray {
+    float o[3];
+    float tmax;
+    float d[3];
+    uint32_t key;
+} lb_ray;
+/* Its hit: t (tmax when none), the triangle (its index in the uploaded order; 0xffffffff: none) and the
+ * face (1: the ray met the back, the shader's det < 0). */
+typedef struct lb_hit {
+    float t;
+    uint32_t tri;
+    uint32_t back;
+    uint32_t pad;
+} lb_hit;
+/* trace() (trace.wgsl:83-130) for each of n rays in host memory, with the handle's BVH (lb_set_bvh) and
+ * the scene's triangle test: the nearest accepted hit, or with `any` the first accepted. seed: the bits
+ * of params.reach[3], which the opacity coin mixes in. Blocking; results in the caller's `out`. No
+ * counterpart in the reference (the shader's walk is internal to its passes); the passes' own rays
+ * (oracle item rays) traced here give their hit/miss masks one ray at a time. */
+int lb_trace(lb_gpu *gpu, lb_scene *scene, const lb_ray *rays, size_t n, int any, uint32_t seed, lb_hit *out);
 
 /* Gpu::run (gpu/mod.rs:140-196): runs `pass` over `n` items, reading `light` (4 floats an atlas
  * texel; may be empty), writing n * width float4 records into the caller's `out` (width 4 for
@@ -198,6 +229,8 @@ int lb_prepared_get_info(const lb_prepared *p, lb_prepared_info *out);
 /* Copies of the prepared arrays (caller-allocated, sized from the info). */
 int lb_prepared_get_bvh(const lb_prepared *p, lb_node *nodes, lb_tri *tris);
 int lb_prepared_get_materials(const lb_prepared *p, float *materials /* 4 a material */);
+/* The BVH's triangles' vertices as the scene holds them (n_tris * 9 floats), for lb_scene_set_vertices. */
+int lb_prepared_get_vertices(const lb_prepared *p, float *verts);
 int lb_prepared_get_charts(const lb_prepared *p, float *charts /* 8 a chart */);
 /* Tile t's rectangle (x, y, w, h in the atlas) and key. */
 int lb_prepared_get_tile(const lb_prepared *p, size_t t, uint32_t rect[4], int32_t key[2]);
@@ -222,6 +255,9 @@ typedef struct lb_bake_options {
     int trace_every_bounce;                     /* device bake: trace the gather rays again in every bounce
                                                  * (default 0: the first bounce records each ray's outcome
                                                  * and later bounces evaluate the records; same results) */
+    int watertight;                             /* the watertight triangle test (lb_scene_set_vertices) in
+                                                 * every pass; such tiles are cached apart (default 0: the
+                                                 * shader's test) */
 } lb_bake_options;
 
 typedef struct lb_bake lb_bake;

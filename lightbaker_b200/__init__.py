@@ -22,10 +22,10 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native as N
-from ._native import NODE, TEXEL, TRI, LightbakerError, Params
+from ._native import HIT, NODE, RAY, TEXEL, TRI, LightbakerError, Params
 
 __all__ = ["Pass", "Gpu", "SceneBuffers", "Prepared", "prepare", "bake", "Bake", "encode_scene", "blake3",
-           "rgb9e5", "rgb9e5_decode", "bc4_block", "Params", "NODE", "TRI", "TEXEL", "LightbakerError", "Transport",
+           "rgb9e5", "rgb9e5_decode", "bc4_block", "Params", "NODE", "TRI", "TEXEL", "RAY", "HIT", "LightbakerError", "Transport",
            "transport"]
 
 
@@ -46,6 +46,16 @@ class SceneBuffers:
     def __init__(self, handle: int, gpu: "Gpu"):
         self._h = handle
         self._gpu = gpu
+
+    def set_vertices(self, verts: np.ndarray | None) -> None:
+        """The triangles' exact vertices ((n_tris, 9) or (n_tris, 3, 3) float32, in the uploaded order;
+        `Prepared.verts`): every walk over this scene then uses the watertight triangle test. None: the
+        shader's test again (lb_scene_set_vertices)."""
+        if verts is None:
+            N.check(N.lib().lb_scene_set_vertices(self._gpu.handle, self._h, None, 0), "lb_scene_set_vertices")
+            return
+        v = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 9)
+        N.check(N.lib().lb_scene_set_vertices(self._gpu.handle, self._h, N.ptr(v), len(v)), "lb_scene_set_vertices")
 
     def close(self) -> None:
         if self._h:
@@ -114,6 +124,15 @@ class Gpu:
             nl = len(light_arr)
         N.check(N.lib().lb_run(self._h, scene._h, int(pass_), C.byref(params), N.ptr(texels), n,
                                N.ptr(light_arr), nl, N.ptr(out)), "GPU")
+        return out
+
+    def trace(self, scene: SceneBuffers, rays: np.ndarray, any_hit: bool = False, seed: int = 0) -> np.ndarray:
+        """trace() (trace.wgsl:83-130) for each ray of a RAY array: a HIT array (t = tmax and tri =
+        0xffffffff where none). seed: the bits of params.reach[3] (lb_trace)."""
+        rays = np.ascontiguousarray(rays, dtype=RAY)
+        out = np.zeros(len(rays), HIT)
+        N.check(N.lib().lb_trace(self._h, scene._h, N.ptr(rays), len(rays), int(bool(any_hit)),
+                                 int(seed) & 0xffffffff, N.ptr(out)), "lb_trace")
         return out
 
     @property
@@ -190,6 +209,9 @@ class Prepared:
         self.charts = np.zeros((info.n_charts, 8), np.float32)
         if info.n_charts:
             N.check(N.lib().lb_prepared_get_charts(self._h, N.ptr(self.charts)), "charts")
+        # each BVH triangle's vertices as the scene holds them (for the watertight test)
+        self.verts = np.zeros((info.n_tris, 9), np.float32)
+        N.check(N.lib().lb_prepared_get_vertices(self._h, N.ptr(self.verts)), "vertices")
         self.tiles = []
         for t in range(info.n_tiles):
             rect = (C.c_uint32 * 4)()
@@ -308,11 +330,12 @@ class Bake:
             pass
 
 
-def _options(cache, log, autotune=False, trace_every_bounce=False):
+def _options(cache, log, autotune=False, trace_every_bounce=False, watertight=False):
     opts = N.BakeOptions()
     opts.cache_dir = str(cache).encode() if cache else None
     opts.autotune = int(bool(autotune))
     opts.trace_every_bounce = int(bool(trace_every_bounce))
+    opts.watertight = int(bool(watertight))
     keep = None
     if log is not None:
         keep = N.LOG_CB(lambda ctx, line: log(line.decode("utf-8", "replace")))
@@ -320,9 +343,10 @@ def _options(cache, log, autotune=False, trace_every_bounce=False):
     return opts, keep
 
 
-def bake(scene: bytes, gpu: Gpu, cache=None, log=None) -> Bake:
-    """bake() (bake.rs:94-432): the whole bake with the passes on `gpu`."""
-    opts, keep = _options(cache, log)
+def bake(scene: bytes, gpu: Gpu, cache=None, log=None, watertight: bool = False) -> Bake:
+    """bake() (bake.rs:94-432): the whole bake with the passes on `gpu`; `watertight`: the watertight
+    triangle test instead of the shader's (lb_bake_options)."""
+    opts, keep = _options(cache, log, watertight=watertight)
     h = N.lib().lb_bake_run(gpu.handle, scene, len(scene), C.byref(opts))
     del keep
     if not h:
@@ -330,11 +354,12 @@ def bake(scene: bytes, gpu: Gpu, cache=None, log=None) -> Bake:
     return Bake(h)
 
 
-def bake_device(scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False, trace_every_bounce=False) -> Bake:
+def bake_device(scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False, trace_every_bounce=False,
+                watertight=False) -> Bake:
     """The device-resident bake: every dirty tile rebaked in one CUDA graph (same results as bake()).
     autotune: time the passes' ray order and grid on a sample of the texels first; trace_every_bounce:
     trace the gather rays in every bounce instead of evaluating the first bounce's records (lb_bake_options)."""
-    opts, keep = _options(cache, log, autotune, trace_every_bounce)
+    opts, keep = _options(cache, log, autotune, trace_every_bounce, watertight)
     h = N.lib().lb_bake_device(gpu.handle, scene, len(scene), C.byref(opts))
     del keep
     if not h:
@@ -346,8 +371,9 @@ class Plan:
     """A device bake in steps: the host work and the graph once (`Plan(scene, gpu)`), then `launch()`
     (the graph enqueued on gpu.stream; repeatable), `rays()`, `result()`."""
 
-    def __init__(self, scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False, trace_every_bounce=False):
-        self._opts, self._keep = _options(cache, log, autotune, trace_every_bounce)
+    def __init__(self, scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False, trace_every_bounce=False,
+                 watertight=False):
+        self._opts, self._keep = _options(cache, log, autotune, trace_every_bounce, watertight)
         self._h = N.lib().lb_plan_create(gpu.handle, scene, len(scene), C.byref(self._opts))
         if not self._h:
             raise LightbakerError(N.last_error())

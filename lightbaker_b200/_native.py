@@ -14,6 +14,8 @@ LIB_PATH = Path(__file__).resolve().parent / "liblightbaker_b200.so"
 NODE = np.dtype([("min", "<f4", 3), ("first", "<u4"), ("max", "<f4", 3), ("count", "<u4")])
 TRI = np.dtype([("v0", "<f4", 4), ("e1", "<f4", 4), ("e2", "<f4", 4)])
 TEXEL = np.dtype([("pos", "<f4", 4), ("normal", "<f4", 4), ("dx", "<f4", 4), ("dy", "<f4", 4)])
+RAY = np.dtype([("o", "<f4", 3), ("tmax", "<f4"), ("d", "<f4", 3), ("key", "<u4")])  # lb_ray
+HIT = np.dtype([("t", "<f4"), ("tri", "<u4"), ("back", "<u4"), ("pad", "<u4")])     # lb_hit
 assert NODE.itemsize == 32 and TRI.itemsize == 48 and TEXEL.itemsize == 64
 
 
@@ -77,7 +79,7 @@ class Tracer(C.Structure):
 
 class BakeOptions(C.Structure):
     _fields_ = [("cache_dir", C.c_char_p), ("log", LOG_CB), ("log_ctx", C.c_void_p), ("autotune", C.c_int),
-                ("trace_every_bounce", C.c_int)]
+                ("trace_every_bounce", C.c_int), ("watertight", C.c_int)]
 
 
 # every exported entry point: name -> (restype, argtypes)
@@ -88,6 +90,8 @@ SIGNATURES = {
     "lb_scene_upload": (C.c_void_p, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                      C.c_size_t, C.c_void_p, C.c_size_t]),
     "lb_scene_free": (None, [C.c_void_p]),
+    "lb_scene_set_vertices": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
+    "lb_trace": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_uint32, C.c_void_p]),
     "lb_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(Params), C.c_void_p, C.c_size_t, C.c_void_p,
                          C.c_size_t, C.c_void_p]),
     "lb_set_counting": (C.c_int, [C.c_void_p, C.c_int]),
@@ -115,6 +119,7 @@ SIGNATURES = {
     "lb_prepared_get_info": (C.c_int, [C.c_void_p, C.POINTER(PreparedInfo)]),
     "lb_prepared_get_bvh": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "lb_prepared_get_materials": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "lb_prepared_get_vertices": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lb_prepared_get_charts": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lb_prepared_get_tile": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]),
     "lb_prepared_rasterize": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p]),

@@ -80,10 +80,12 @@ PostArgs lb_plan_post_args(lb_plan &p) {
 
 namespace {
 
-int warp_blocks(lb_gpu *g, int pass) {
+int warp_blocks(const lb_plan &p, int pass) {
+    lbd::Scene S = lb_scene_view(p.dscene);
     WarpPass w{};
+    w.S = &S;
     w.pass = pass;
-    w.sms = g->sms;
+    w.sms = p.g->sms;
     return lb_warp_pass_blocks(w);
 }
 
@@ -105,6 +107,9 @@ void build(lb_plan &p) {
                                p.P.bvh.tris.size(), p.P.materials.data(), p.P.materials.size() / 4,
                                p.P.affines.data(), p.P.affines.size() / 8);
     if (!p.dscene) throw std::runtime_error(lb_last_error());
+    if (p.opt.watertight &&
+        lb_scene_set_vertices(p.g, p.dscene, p.P.bvh.verts.data(), p.P.bvh.tris.size()) != LB_OK)
+        throw std::runtime_error(lb_last_error());
 
     // the cache (bake.rs:123-136); without a cache directory nothing is read or written, so the tiles' and
     // chunks' hashes (only ever cache keys) are not computed
@@ -115,6 +120,7 @@ void build(lb_plan &p) {
     if (caching) {
         boxes.emplace(p.scene);
         global = lb::global_hash(p.scene);
+        if (p.opt.watertight) global = lb::watertight_hash(global);
     }
     float reach = b.gi_bounces > 0 ? std::fmax(b.gi_reach, b.ao_reach) : b.ao_reach;
     size_t nt = layout.tiles.size();
@@ -335,9 +341,9 @@ void build(lb_plan &p) {
     up(p.probe_items, probe_items.data(), probe_items.size() * 64);
     up(p.probe_slot, probe_slot.data(), probe_slot.size() * 4);
     ck(cudaStreamSynchronize(st), "upload");
-    p.blocks_direct = warp_blocks(p.g, LB_PASS_DIRECT);
-    p.blocks_gather = warp_blocks(p.g, LB_PASS_GATHER);
-    p.blocks_volume = warp_blocks(p.g, LB_PASS_VOLUME);
+    p.blocks_direct = warp_blocks(p, LB_PASS_DIRECT);
+    p.blocks_gather = warp_blocks(p, LB_PASS_GATHER);
+    p.blocks_volume = warp_blocks(p, LB_PASS_VOLUME);
     mark("device arrays");
     p.t_prepare = since(t0);
 }
@@ -380,6 +386,7 @@ void autotune(lb_plan &p) {
         for (int order : orders) {
             if (pass == LB_PASS_GATHER && sh.near) continue;
             WarpPass probe{};
+            probe.S = &S;
             probe.pass = pass;
             probe.sms = p.g->sms;
             probe.bvh = sh.bvh;
@@ -618,6 +625,7 @@ lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_
             void *ctx = opts->log_ctx;
             p->opt.log = [fn, ctx](const std::string &s) { fn(ctx, s.c_str()); };
         }
+        p->opt.watertight = opts && opts->watertight;
         p->autotune = opts && opts->autotune;
         p->reuse = !(opts && opts->trace_every_bounce);
         p->keep_records = keep_records;

@@ -294,6 +294,7 @@ Bake bake(const Scene &scene, Tracer &gpu, const Options &o) {
     Layout &layout = P.layout;
     size_t aw = layout.width, ah = layout.height;
     gpu.scene(P.bvh, P.materials, P.affines);
+    if (o.watertight) gpu.watertight(P.bvh);
     const lb_params &params = P.params;
     Vec3 sun = P.sun;
     uint32_t g = P.g;
@@ -307,6 +308,7 @@ Bake bake(const Scene &scene, Tracer &gpu, const Options &o) {
     Cache cache(o.cache);
     Boxes boxes(scene);
     Hash global = global_hash(scene);
+    if (o.watertight) global = watertight_hash(global);
     float reach = b.gi_bounces > 0 ? std::fmax(b.gi_reach, b.ao_reach) : b.ao_reach;
     size_t nt = layout.tiles.size();
     std::vector<Hash> hashes(nt);

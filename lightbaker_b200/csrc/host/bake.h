@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <functional>
 #include <optional>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -33,6 +34,9 @@ class Tracer {
     // out: n * width float4 records; returns the rays traced (every trace() call); throws std::runtime_error
     virtual uint64_t run(int pass, const lb_params &params, const std::vector<lb_texel> &items,
                      const std::vector<float> &light, std::vector<float> &out) = 0;
+    // the watertight triangle test over the scene's exact vertices for the passes that follow (beyond
+    // the reference); a tracer without one throws
+    virtual void watertight(const Bvh &) { throw std::runtime_error("this tracer has no watertight triangle test"); }
 };
 
 struct Stats {  // bake.rs:49-58
@@ -73,6 +77,7 @@ struct Bake {  // bake.rs:36-47
 struct Options {  // bake.rs:30-34
     std::string cache;  // empty: none
     std::function<void(const std::string &)> log;
+    bool watertight = false;  // beyond the reference: the watertight triangle test (Tracer::watertight)
 };
 
 // The inputs every pass needs, built once per bake.

@@ -17,6 +17,7 @@ constexpr size_t LEAF = 4;   // bvh.rs:10
 struct Prim {
     Vec3 min, max, centre;
     lb_tri tri;
+    uint32_t mesh, index;  // where its vertices are in the scene
 };
 
 // bvh.rs:109-111
@@ -190,6 +191,8 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
             q.max = a.max(b).max(c);
             q.centre = (a + b + c) / 3.0f;
             q.tri = lb_tri{{a.x, a.y, a.z, u2f(m.material)}, {e1.x, e1.y, e1.z, u2f(chart(mi, t))}, {e2.x, e2.y, e2.z, 0.0f}};
+            q.mesh = uint32_t(mi);
+            q.index = uint32_t(t);
             prims.push_back(q);
         }
     }
@@ -199,6 +202,7 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
         // one empty leaf, a box nothing reaches
         out.nodes[0] = lb_node{{FLT_MAX, FLT_MAX, FLT_MAX}, 0, {-FLT_MAX, -FLT_MAX, -FLT_MAX}, 0};
         out.tris.push_back(lb_tri{});
+        out.verts.assign(9, 0.0f);
         return out;
     }
     // The serial walk below (bvh.rs:62-104) pops a node, decides it a leaf or splits its primitives in
@@ -290,6 +294,16 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
     }
     out.tris.reserve(prims.size());
     for (auto &p : prims) out.tris.push_back(p.tri);
+    out.verts.resize(prims.size() * 9);
+    for (size_t i = 0; i < prims.size(); i++) {
+        const std::vector<Vec3> &p = scene.positions[prims[i].mesh];
+        for (int k = 0; k < 3; k++) {
+            Vec3 v = p[size_t(prims[i].index) * 3 + k];
+            out.verts[i * 9 + k * 3] = v.x;
+            out.verts[i * 9 + k * 3 + 1] = v.y;
+            out.verts[i * 9 + k * 3 + 2] = v.z;
+        }
+    }
     return out;
 }
 

@@ -13,6 +13,9 @@ namespace lb {
 struct Bvh {
     std::vector<lb_node> nodes;
     std::vector<lb_tri> tris;
+    // each triangle's vertices as the scene holds them (9 floats, in `tris` order): v0 = tris[i].v0
+    // exactly, while v0 + e1 and v0 + e2 may round; the watertight test reads these
+    std::vector<float> verts;
     // chart(mesh, triangle): the triangle's chart (0xffffffff: none)
     static Bvh build(const Scene &scene, const std::function<uint32_t(size_t, size_t)> &chart);
 };

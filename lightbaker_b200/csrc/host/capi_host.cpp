@@ -32,6 +32,10 @@ class GpuTracer : public lb::Tracer {
                              mats.size() / 4, charts.data(), charts.size() / 8);
         if (!s_) throw std::runtime_error(lb_last_error());
     }
+    void watertight(const lb::Bvh &bvh) override {
+        if (!s_ || lb_scene_set_vertices(g_, s_, bvh.verts.data(), bvh.tris.size()) != LB_OK)
+            throw std::runtime_error(lb_last_error());
+    }
     uint64_t run(int pass, const lb_params &params, const std::vector<lb_texel> &items, const std::vector<float> &light,
                  std::vector<float> &out) override {
         size_t width = pass == LB_PASS_VOLUME ? 4 : 1;
@@ -83,6 +87,7 @@ lb::Options options(const lb_bake_options *o) {
         void *ctx = o->log_ctx;
         opt.log = [fn, ctx](const std::string &s) { fn(ctx, s.c_str()); };
     }
+    if (o) opt.watertight = o->watertight != 0;
     return opt;
 }
 
@@ -139,6 +144,12 @@ int lb_prepared_get_bvh(const lb_prepared *p, lb_node *nodes, lb_tri *tris) {
     if (!p || !nodes || !tris) return LB_EINVAL;
     std::memcpy(nodes, p->prep.bvh.nodes.data(), p->prep.bvh.nodes.size() * sizeof(lb_node));
     std::memcpy(tris, p->prep.bvh.tris.data(), p->prep.bvh.tris.size() * sizeof(lb_tri));
+    return LB_OK;
+}
+
+int lb_prepared_get_vertices(const lb_prepared *p, float *verts) {
+    if (!p || !verts) return LB_EINVAL;
+    std::memcpy(verts, p->prep.bvh.verts.data(), p->prep.bvh.verts.size() * sizeof(float));
     return LB_OK;
 }
 

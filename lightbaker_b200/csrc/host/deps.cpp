@@ -32,6 +32,16 @@ Hash global_hash(const Scene &scene) {
     return out;
 }
 
+Hash watertight_hash(const Hash &global) {
+    Blake3 k;
+    k.update(global.data(), global.size());
+    static const char tag[] = "watertight triangle test";
+    k.update(tag, sizeof tag - 1);
+    Hash out;
+    k.finalize(out.data());
+    return out;
+}
+
 bool swept(const Aabb &zone, Vec3 sun, float top, const Aabb &b) {
     float tmax = sun.y > 1e-4f ? std::fmax((top - zone.min.y) / sun.y, 0.0f) : 0.0f;
     float lo = 0.0f, hi = tmax;

@@ -29,6 +29,9 @@ struct Boxes {  // deps.rs:33-57
 
 using Hash = std::array<uint8_t, 32>;
 Hash global_hash(const Scene &scene);  // deps.rs:59-68
+// global_hash for a bake with the watertight triangle test (beyond the reference): its tiles and chunks
+// are cached apart from the shader's
+Hash watertight_hash(const Hash &global);
 // deps.rs:70-96
 Hash hash_reach(const Scene &scene, const Boxes &boxes, const Hash &global, const Aabb &own, float reach,
                 const std::vector<uint8_t> &seed);

@@ -26,6 +26,12 @@ struct Scene {
     // the 8-wide BVH (host/bvh8.h): 5 uint4 a node, its triangle copy (e2.w: the reference index)
     const uint4 *nodes8 = nullptr;
     const float4 *tris8 = nullptr;
+    // the triangles' exact vertices (3 float4 a triangle, BVH2 order): set, the walks use the watertight
+    // triangle test and scale each box's exit distance by `grow` (1 + 4e-7, above the slab test's
+    // rounding: Ize, "Robust BVH Ray Traversal", JCGT 2(2), 2013), so a box holding a hit is not missed;
+    // 1 without vertices (the shader's tests, unchanged)
+    const float4 *verts = nullptr;
+    float grow = 1.0f;
 };
 
 constexpr int STACK8 = 96;  // node groups the 8-wide walk can hold (depth x 7 at most)
@@ -140,12 +146,86 @@ __device__ __forceinline__ bool stops(const Scene &S, uint32_t tri, float v0w, u
     return op >= 1.0f || rnd(tri * 9781u, ray, seed) < op;
 }
 
-// trace.wgsl:74-80
-__device__ __forceinline__ float box(float3 o, float3 inv, float4 mn, float4 mx, float tmax) {
+// ---- the triangle test ----
+__device__ __forceinline__ float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// The watertight test of Woop, Benthin and Wald ("Watertight Ray/Triangle Intersection", JCGT 2(1), 2013),
+// restated: the ray's largest axis kz, the other two in the order that keeps the frame's handedness,
+// the shear that takes d onto +z, then the three edge functions of the sheared vertices, each a
+// difference of two rounded products (recomputed in FP64 when one is exactly zero). An edge two
+// triangles share gives them edge functions that are exact negatives of each other, so a ray meets
+// at least one of them and never passes between. The shear keeps orientation, so det's sign is the
+// shader's det's sign. Returns (t, det) of a hit, t = -1 for a miss (every accepted t is above 1e-4).
+static __device__ __noinline__ float2 watertight(const float4 *verts, uint32_t ref, float3 o, float3 d) {
+    float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    float dz = comp(d, kz);
+    if (dz < 0.0f) {
+        int k = kx;
+        kx = ky;
+        ky = k;
+    }
+    float sx = comp(d, kx) / dz, sy = comp(d, ky) / dz, sz = 1.0f / dz;
+    const float4 *v = verts + 3 * size_t(ref);
+    float4 a4 = __ldg(v), b4 = __ldg(v + 1), c4 = __ldg(v + 2);
+    float3 A = sub(xyz(a4), o), B = sub(xyz(b4), o), C = sub(xyz(c4), o);
+    float Az = comp(A, kz), Bz = comp(B, kz), Cz = comp(C, kz);
+    float Ax = comp(A, kx) - sx * Az, Ay = comp(A, ky) - sy * Az;
+    float Bx = comp(B, kx) - sx * Bz, By = comp(B, ky) - sy * Bz;
+    float Cx = comp(C, kx) - sx * Cz, Cy = comp(C, ky) - sy * Cz;
+    float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        // products of two floats are exact in FP64: the edge functions' signs are exact
+        U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
+        V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+        W = float(double(Bx) * double(Ay) - double(By) * double(Ax));
+    }
+    float2 miss = make_float2(-1.0f, 0.0f);
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return miss;
+    float det = U + V + W;
+    if (det == 0.0f) return miss;
+    float T = U * (sz * Az) + V * (sz * Bz) + W * (sz * Cz);
+    return make_float2(T / det, det);
+}
+
+// Whether the ray meets triangle `ref` (v0, e1, e2: its record), with its t and face (back: the shader's
+// det < 0). WT false: Möller-Trumbore in the shader's arithmetic (trace.wgsl:105-121); true: the watertight
+// test over the scene's vertices. The caller applies the window (1e-4, nearest so far). Each walk is
+// built for both and picks once at its start, so the shader's test carries nothing of the other.
+template <bool WT>
+__device__ __forceinline__ bool tri_hit(const Scene &S, uint32_t ref, float4 v0, float4 e1, float4 e2, float3 o,
+                                        float3 d, float &t, bool &back) {
+    if (WT) {
+        float2 r = watertight(S.verts, ref, o, d);
+        t = r.x;
+        back = r.y < 0.0f;
+        return r.x >= 0.0f;
+    }
+    float3 p = cross3(d, xyz(e2));
+    float det = dot3(xyz(e1), p);
+    if (fabsf(det) < 1e-12f) return false;
+    float id = 1.0f / det;
+    float3 s = sub(o, xyz(v0));
+    float u = dot3(s, p) * id;
+    if (u < 0.0f || u > 1.0f) return false;
+    float3 q = cross3(s, xyz(e1));
+    float v = dot3(d, q) * id;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    t = dot3(xyz(e2), q) * id;
+    back = det < 0.0f;
+    return true;
+}
+
+// trace.wgsl:74-80; the watertight walks (WT) scale the exit distance by `grow`
+template <bool WT = false>
+__device__ __forceinline__ float box(float3 o, float3 inv, float4 mn, float4 mx, float tmax, float grow = 1.0f) {
     float ax = (mn.x - o.x) * inv.x, ay = (mn.y - o.y) * inv.y, az = (mn.z - o.z) * inv.z;
     float bx = (mx.x - o.x) * inv.x, by = (mx.y - o.y) * inv.y, bz = (mx.z - o.z) * inv.z;
     float lo = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
     float hi = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+    if (WT) hi = hi * grow;
     float l0 = fmaxf(lo, 0.0f);
     return (hi >= l0 && lo < tmax) ? l0 : FAR;
 }
@@ -155,9 +235,9 @@ __device__ __forceinline__ float box(float3 o, float3 inv, float4 mn, float4 mx,
 // carried into the next step instead of being read again; a popped node is read once. The root's box
 // is never tested (the shader starts at its children). An inner node whose children lie past the
 // array ends the walk (the reference's one-node BVH of an empty scene).
-template <bool COUNT>
-__device__ __forceinline__ Hit trace(const Scene &S, float3 o, float3 d, float tmax, bool any, uint32_t ray,
-                                     uint32_t seed, Count &c) {
+template <bool COUNT, bool WT>
+__device__ __forceinline__ Hit trace_t(const Scene &S, float3 o, float3 d, float tmax, bool any, uint32_t ray,
+                                       uint32_t seed, Count &c) {
     Hit hit{tmax, NONE, false};
     c.rays++;
     if (COUNT) c.nodes++;
@@ -174,19 +254,11 @@ __device__ __forceinline__ Hit trace(const Scene &S, float3 o, float3 d, float t
             for (uint32_t i = first; i < first + count; i++) {
                 if (COUNT) c.tris++;
                 float4 v0 = __ldg(&S.tris[3 * i]), e1 = __ldg(&S.tris[3 * i + 1]), e2 = __ldg(&S.tris[3 * i + 2]);
-                float3 p = cross3(d, xyz(e2));
-                float det = dot3(xyz(e1), p);
-                if (fabsf(det) < 1e-12f) continue;
-                float id = 1.0f / det;
-                float3 s = sub(o, xyz(v0));
-                float u = dot3(s, p) * id;
-                if (u < 0.0f || u > 1.0f) continue;
-                float3 q = cross3(s, xyz(e1));
-                float v = dot3(d, q) * id;
-                if (v < 0.0f || u + v > 1.0f) continue;
-                float t = dot3(xyz(e2), q) * id;
+                float t;
+                bool bk;
+                if (!tri_hit<WT>(S, i, v0, e1, e2, o, d, t, bk)) continue;
                 if (t > 1e-4f && t < hit.t && stops<COUNT>(S, i, v0.w, ray, seed, c)) {
-                    hit = Hit{t, i, det < 0.0f};
+                    hit = Hit{t, i, bk};
                     if (any) return hit;
                 }
             }
@@ -194,8 +266,8 @@ __device__ __forceinline__ Hit trace(const Scene &S, float3 o, float3 d, float t
             if (COUNT) c.nodes += 2;
             float4 alo = __ldg(&S.nodes[2 * first]), ahi = __ldg(&S.nodes[2 * first + 1]);
             float4 blo = __ldg(&S.nodes[2 * first + 2]), bhi = __ldg(&S.nodes[2 * first + 3]);
-            float ta = box(o, inv, alo, ahi, hit.t);
-            float tb = box(o, inv, blo, bhi, hit.t);
+            float ta = box<WT>(o, inv, alo, ahi, hit.t, S.grow);
+            float tb = box<WT>(o, inv, blo, bhi, hit.t, S.grow);
             bool a_near = ta <= tb;
             float tn = fminf(ta, tb), tf = fmaxf(ta, tb);
             if (tn < FAR) {
@@ -214,11 +286,17 @@ __device__ __forceinline__ Hit trace(const Scene &S, float3 o, float3 d, float t
     return hit;
 }
 
+template <bool COUNT, bool WT = false>
+__device__ __forceinline__ Hit trace(const Scene &S, float3 o, float3 d, float tmax, bool any, uint32_t ray,
+                                     uint32_t seed, Count &c) {
+    return trace_t<COUNT, WT>(S, o, d, tmax, any, ray, seed, c);
+}
+
 // trace() as a resumable walk: its state between nodes, so that a lane whose ray has ended can start
 // another while its warp's other lanes go on. step() does what one pass of trace()'s loop does (one
 // node: a leaf's triangles, or an inner node's two children, then a pop when there is nothing to
 // descend to), so a ray visits the same nodes in the same order and ends with the same hit.
-template <bool COUNT>
+template <bool COUNT, bool WT = false>
 struct Walk2 {
     float3 o, d, inv;
     uint32_t ray;
@@ -250,19 +328,11 @@ struct Walk2 {
             for (uint32_t i = first; i < first + count; i++) {
                 if (COUNT) c.tris++;
                 float4 v0 = __ldg(&S.tris[3 * i]), e1 = __ldg(&S.tris[3 * i + 1]), e2 = __ldg(&S.tris[3 * i + 2]);
-                float3 p = cross3(d, xyz(e2));
-                float det = dot3(xyz(e1), p);
-                if (fabsf(det) < 1e-12f) continue;
-                float id = 1.0f / det;
-                float3 s = sub(o, xyz(v0));
-                float u = dot3(s, p) * id;
-                if (u < 0.0f || u > 1.0f) continue;
-                float3 q = cross3(s, xyz(e1));
-                float v = dot3(d, q) * id;
-                if (v < 0.0f || u + v > 1.0f) continue;
-                float t = dot3(xyz(e2), q) * id;
+                float t;
+                bool bk;
+                if (!tri_hit<WT>(S, i, v0, e1, e2, o, d, t, bk)) continue;
                 if (t > 1e-4f && t < hit.t && stops<COUNT>(S, i, v0.w, ray, seed, c)) {
-                    hit = Hit{t, i, det < 0.0f};
+                    hit = Hit{t, i, bk};
                     if (any) {
                         done = true;
                         return;
@@ -273,8 +343,8 @@ struct Walk2 {
             if (COUNT) c.nodes += 2;
             float4 alo = __ldg(&S.nodes[2 * first]), ahi = __ldg(&S.nodes[2 * first + 1]);
             float4 blo = __ldg(&S.nodes[2 * first + 2]), bhi = __ldg(&S.nodes[2 * first + 3]);
-            float ta = box(o, inv, alo, ahi, hit.t);
-            float tb = box(o, inv, blo, bhi, hit.t);
+            float ta = box<WT>(o, inv, alo, ahi, hit.t, S.grow);
+            float tb = box<WT>(o, inv, blo, bhi, hit.t, S.grow);
             bool a_near = ta <= tb;
             float tn = fminf(ta, tb), tf = fmaxf(ta, tb);
             if (tn < FAR) {
@@ -316,18 +386,31 @@ __device__ __forceinline__ float box_front(float3 o, float3 n, float4 mn, float4
     return (x - o.x) * n.x + (y - o.y) * n.y + (z - o.z) * n.z;
 }
 
-// Warp-wide: the leaves within reach r of o on the n side (by a margin), into list, nearest first, with
-// their boxes' squared distances from o in dist2. Returns their count, or -1 when a level or the list would
-// overflow. All lanes return the same value.
+// A list entry: the leaf's node index, and in the top 4 bits which of its (at most 4) triangles the
+// list's rays must test.
+constexpr uint32_t LEAF_NODE = 0x0fffffffu;
+constexpr int LEAF_MASK_SHIFT = 28;
+
+// Warp-wide: the leaves within reach r of o on the n side (by a margin), into list (entries: node |
+// triangle bits << 28, every triangle of the leaf), nearest first, with their boxes' squared distances
+// from o in dist2. Returns their count, or -1 when a level or the list would overflow, a leaf holds more
+// than 4 triangles or node indices need more than 28 bits. All lanes return the same value.
+// (Dropping each leaf's triangles wholly behind o's plane from its bits was measured: testing them cost
+// more than the triangle tests it saved.)
 template <bool COUNT>
 __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float3 n, uint32_t *fa, uint32_t *fb,
                                         uint32_t *list, float *dist2, int lane, Count &c) {
     const unsigned FULLM = 0xffffffffu;
     float rr = r * 1.0001f + 1e-5f, r2 = rr * rr, margin = -(r * 1e-3f + 1e-4f);
+    if (S.n_nodes > LEAF_NODE) return -1;
     float4 rlo = __ldg(&S.nodes[0]), rhi = __ldg(&S.nodes[1]);
     uint32_t rfirst = __float_as_uint(rlo.w), rcount = __float_as_uint(rhi.w);
     if (rcount > 0u) {
-        if (lane == 0) list[0] = 0;
+        if (rcount > 4u) return -1;
+        if (lane == 0) {
+            list[0] = ((1u << rcount) - 1u) << LEAF_MASK_SHIFT;
+            dist2[0] = 0.0f;
+        }
         __syncwarp();
         return 1;
     }
@@ -339,8 +422,8 @@ __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float
         int nn = 0;
         for (int base = 0; base < nf; base += 32) {
             int i = base + lane;
-            bool leaf = false, inner = false;
-            uint32_t node = 0, first = 0;
+            bool leaf = false, inner = false, wide = false;
+            uint32_t node = 0, first = 0, tris = 0;
             if (i < nf) {
                 node = fa[i];
                 float4 lo = __ldg(&S.nodes[2 * node]), hi = __ldg(&S.nodes[2 * node + 1]);
@@ -348,14 +431,21 @@ __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float
                 if (box_dist2(o, lo, hi) <= r2 && box_front(o, n, lo, hi) >= margin) {
                     first = __float_as_uint(lo.w);
                     uint32_t count = __float_as_uint(hi.w);
-                    if (count > 0u) leaf = true;
-                    else if (first + 1u < S.n_nodes) inner = true;
+                    if (count > 4u) {
+                        wide = true;
+                    } else if (count > 0u) {
+                        leaf = true;
+                        tris = count;
+                    } else if (first + 1u < S.n_nodes) {
+                        inner = true;
+                    }
                 }
             }
+            if (__any_sync(FULLM, wide)) return -1;  // leaves of more than 4 triangles: the tree walk
             unsigned lm = __ballot_sync(FULLM, leaf), im = __ballot_sync(FULLM, inner);
             unsigned below = (1u << lane) - 1u;
             int lp = nl + __popc(lm & below), ip = nn + 2 * __popc(im & below);
-            if (leaf && lp < BALL_LEAVES) list[lp] = node;
+            if (leaf && lp < BALL_LEAVES) list[lp] = node | (((1u << tris) - 1u) << LEAF_MASK_SHIFT);
             if (inner && ip + 1 < BALL_FRONT) {
                 fb[ip] = first;
                 fb[ip + 1] = first + 1u;
@@ -373,7 +463,7 @@ __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float
     // nearest first: rank by distance (ties by index), then place; keys in fb
     float *key = (float *)fb;
     for (int i = lane; i < nl; i += 32) {
-        uint32_t node = list[i];
+        uint32_t node = list[i] & LEAF_NODE;
         key[i] = box_dist2(o, __ldg(&S.nodes[2 * node]), __ldg(&S.nodes[2 * node + 1]));
     }
     __syncwarp();
@@ -407,16 +497,15 @@ __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float
     return nl;
 }
 
-// trace() over a leaf list: the nearest accepted hit within tmax among the listed leaves' triangles,
-// with the walk's box test (culled by the nearest hit so far) and triangle test. The list is nearest
-// first from its centre (dist2: each box's squared distance from it), and the ray starts within `shift`
-// of that centre, so once a box lies farther than the nearest hit so far plus shift (by a relative
-// margin far above the rounding of t, |d| and the distance), neither it nor any later box can hold a
-// nearer hit and the walk ends: the same hit as the whole list.
-template <bool COUNT>
-__device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, const float *dist2, int nl, float3 o,
-                                          float3 d, float tmax, uint32_t ray, uint32_t seed, Count &c,
-                                          float shift = 0.0f) {
+// trace() over a leaf list: the nearest accepted hit within tmax among the listed leaves' triangles (an
+// entry's mask names the leaf's triangles the list keeps), with the walk's box test (culled by the nearest
+// hit so far) and triangle test. The list is nearest first from its centre (dist2: each box's squared
+// distance from it), and the ray starts within `shift` of that centre, so once a box lies farther than the
+// nearest hit so far plus shift (by a relative margin far above the rounding of t, |d| and the distance),
+// neither it nor any later box can hold a nearer hit and the walk ends: the same hit as the whole list.
+template <bool COUNT, bool WT>
+__device__ __forceinline__ Hit trace_list_t(const Scene &S, const uint32_t *list, const float *dist2, int nl, float3 o,
+                                            float3 d, float tmax, uint32_t ray, uint32_t seed, Count &c, float shift) {
     Hit hit{tmax, NONE, false};
     c.rays++;
     float3 dd = mk(fabsf(d.x) < 1e-12f ? 1e-12f : d.x, fabsf(d.y) < 1e-12f ? 1e-12f : d.y,
@@ -425,27 +514,20 @@ __device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, 
     float lim = (tmax + shift) * 1.0001f + 1e-5f, lim2 = lim * lim;
     for (int k = 0; k < nl; k++) {
         if (dist2[k] > lim2) break;
-        uint32_t node = list[k];
+        const uint32_t entry = list[k], node = entry & LEAF_NODE;
         float4 lo = __ldg(&S.nodes[2 * node]), hi = __ldg(&S.nodes[2 * node + 1]);
         if (COUNT) c.nodes++;
-        if (!(box(o, inv, lo, hi, hit.t) < FAR)) continue;
-        uint32_t first = __float_as_uint(lo.w), count = __float_as_uint(hi.w);
-        for (uint32_t i = first; i < first + count; i++) {
+        if (!(box<WT>(o, inv, lo, hi, hit.t, S.grow) < FAR)) continue;
+        const uint32_t first = __float_as_uint(lo.w);
+        for (uint32_t m = entry >> LEAF_MASK_SHIFT; m; m &= m - 1u) {
+            const uint32_t i = first + uint32_t(__ffs(int(m)) - 1);
             if (COUNT) c.tris++;
             float4 v0 = __ldg(&S.tris[3 * i]), e1 = __ldg(&S.tris[3 * i + 1]), e2 = __ldg(&S.tris[3 * i + 2]);
-            float3 p = cross3(d, xyz(e2));
-            float det = dot3(xyz(e1), p);
-            if (fabsf(det) < 1e-12f) continue;
-            float id = 1.0f / det;
-            float3 s3 = sub(o, xyz(v0));
-            float u = dot3(s3, p) * id;
-            if (u < 0.0f || u > 1.0f) continue;
-            float3 q = cross3(s3, xyz(e1));
-            float v = dot3(d, q) * id;
-            if (v < 0.0f || u + v > 1.0f) continue;
-            float t = dot3(xyz(e2), q) * id;
+            float t;
+            bool bk;
+            if (!tri_hit<WT>(S, i, v0, e1, e2, o, d, t, bk)) continue;
             if (t > 1e-4f && t < hit.t && stops<COUNT>(S, i, v0.w, ray, seed, c)) {
-                hit = Hit{t, i, det < 0.0f};
+                hit = Hit{t, i, bk};
                 lim = (t + shift) * 1.0001f + 1e-5f;
                 lim2 = lim * lim;
             }
@@ -453,15 +535,21 @@ __device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, 
     }
     return hit;
 }
+template <bool COUNT, bool WT = false>
+__device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, const float *dist2, int nl, float3 o,
+                                          float3 d, float tmax, uint32_t ray, uint32_t seed, Count &c,
+                                          float shift = 0.0f) {
+    return trace_list_t<COUNT, WT>(S, list, dist2, nl, o, d, tmax, ray, seed, c, shift);
+}
 
 // The same query over the 8-wide BVH: the nearest accepted hit within tmax (any: the first accepted),
 // the same triangle test in the same arithmetic, so every hit, its t and its face are the BVH2 walk's.
 // A node's eight child boxes are tested at once; its leaf slots' triangles first, then its hit inner
 // children nearest first (the rest pushed far to near with their entry distance, and skipped when
 // popped beyond the nearest hit so far).
-template <bool COUNT>
-__device__ __forceinline__ Hit trace8(const Scene &S, float3 o, float3 d, float tmax, bool any, uint32_t ray,
-                                      uint32_t seed, Count &c) {
+template <bool COUNT, bool WT>
+__device__ __forceinline__ Hit trace8_t(const Scene &S, float3 o, float3 d, float tmax, bool any, uint32_t ray,
+                                        uint32_t seed, Count &c) {
     Hit hit{tmax, NONE, false};
     c.rays++;
     float3 dd = mk(fabsf(d.x) < 1e-12f ? 1e-12f : d.x, fabsf(d.y) < 1e-12f ? 1e-12f : d.y,
@@ -496,7 +584,7 @@ __device__ __forceinline__ Hit trace8(const Scene &S, float3 o, float3 d, float 
             float4 mx = make_float4(px + __uint2float_rn(((s < 4 ? a3.z : a3.w) >> sh) & 0xffu) * sx,
                                     py + __uint2float_rn(((s < 4 ? a4.x : a4.y) >> sh) & 0xffu) * sy,
                                     pz + __uint2float_rn(((s < 4 ? a4.z : a4.w) >> sh) & 0xffu) * sz, 0.0f);
-            float t = box(o, inv, mn, mx, hit.t);
+            float t = box<WT>(o, inv, mn, mx, hit.t, S.grow);
             tc[s] = t;
             if (t < FAR) {
                 if (inner) innermask |= 1u << s;
@@ -512,20 +600,12 @@ __device__ __forceinline__ Hit trace8(const Scene &S, float3 o, float3 d, float 
                 if (COUNT) c.tris++;
                 const float4 *tp = S.tris8 + 3 * size_t(first + k);
                 float4 v0 = __ldg(tp), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
-                float3 p = cross3(d, xyz(e2));
-                float det = dot3(xyz(e1), p);
-                if (fabsf(det) < 1e-12f) continue;
-                float id = 1.0f / det;
-                float3 s3 = sub(o, xyz(v0));
-                float u = dot3(s3, p) * id;
-                if (u < 0.0f || u > 1.0f) continue;
-                float3 q = cross3(s3, xyz(e1));
-                float v = dot3(d, q) * id;
-                if (v < 0.0f || u + v > 1.0f) continue;
-                float t = dot3(xyz(e2), q) * id;
                 uint32_t orig = __float_as_uint(e2.w);
+                float t;
+                bool bk;
+                if (!tri_hit<WT>(S, orig, v0, e1, e2, o, d, t, bk)) continue;
                 if (t > 1e-4f && t < hit.t && stops<COUNT>(S, orig, v0.w, ray, seed, c)) {
-                    hit = Hit{t, orig, det < 0.0f};
+                    hit = Hit{t, orig, bk};
                     if (any) return hit;
                 }
             }
@@ -577,13 +657,13 @@ __device__ __forceinline__ Hit trace8(const Scene &S, float3 o, float3 d, float 
     }
     return hit;
 }
-
-// The walk a pass uses: BVH 2 the reference's tree, 8 the 8-wide one.
-template <int BVH, bool COUNT>
+// The walk a pass uses: BVH 2 the reference's tree, 8 the 8-wide one; WT the watertight triangle test
+// (the kernels are built for both and the launch picks by whether the scene has vertices).
+template <int BVH, bool COUNT, bool WT = false>
 __device__ __forceinline__ Hit walk(const Scene &S, float3 o, float3 d, float tmax, bool any, uint32_t ray,
                                     uint32_t seed, Count &c) {
-    if (BVH == 8) return trace8<COUNT>(S, o, d, tmax, any, ray, seed, c);
-    return trace<COUNT>(S, o, d, tmax, any, ray, seed, c);
+    if (BVH == 8) return trace8_t<COUNT, WT>(S, o, d, tmax, any, ray, seed, c);
+    return trace_t<COUNT, WT>(S, o, d, tmax, any, ray, seed, c);
 }
 
 // A gather ray's outcome, all a bounce needs to evaluate it again against another light atlas:

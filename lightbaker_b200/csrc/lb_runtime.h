@@ -39,6 +39,7 @@ struct lb_scene {
     uint32_t n_nodes = 0, n_tris = 0, n_mats = 0, n_charts = 0;
     void *nodes8 = nullptr, *tris8 = nullptr;  // the 8-wide BVH collapsed from the BVH2 (host/bvh8.h)
     uint32_t n_nodes8 = 0, n_tris8 = 0;
+    void *verts = nullptr;  // exact vertices (lb_scene_set_vertices): the watertight triangle test
 };
 
 void lb_set_error(const std::string &msg);

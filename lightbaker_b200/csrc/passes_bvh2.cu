@@ -11,14 +11,14 @@ namespace lbd {
 __device__ __forceinline__ float4 ld4(const float4 *p) { return __ldg(p); }
 
 // trace.wgsl:159-168
-template <bool COUNT>
+template <bool COUNT, bool WT>
 __device__ __forceinline__ bool inside(const Scene &S, const lb_params &P, uint32_t seed, float3 o, float3 n,
                                        uint32_t key, Count &c) {
     Frame f = frame(n);
     float back = 0.0f;
     for (uint32_t r = 0; r < 16u; r++) {
         float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
-        Hit h = trace<COUNT>(S, o, d, P.ground[3], false, key + r + 7000u, seed, c);
+        Hit h = trace<COUNT, WT>(S, o, d, P.ground[3], false, key + r + 7000u, seed, c);
         if (h.tri != NONE && h.back) back += 1.0f;
     }
     return back / 16.0f > __uint_as_float(P.atlas[3]);
@@ -47,7 +47,7 @@ __device__ __forceinline__ void flush(Count &c, unsigned long long *counters) {
 
 // trace.wgsl:170-243. `base` is the item index of items[0] in the whole list (the shader's
 // P.atlas.z + i), which keys the sample sequence.
-template <bool COUNT>
+template <bool COUNT, bool WT>
 __global__ void __launch_bounds__(128) direct_kernel(Scene S, lb_params P, const float4 *items, uint32_t n,
                                                      uint32_t base, float4 *out, unsigned long long *counters) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -66,11 +66,11 @@ __global__ void __launch_bounds__(128) direct_kernel(Scene S, lb_params P, const
         float3 at = pos;
         uint32_t pick = 0u;
         float span = 1.0f;
-        if (inside<COUNT>(S, P, seed, add(at, lift), nrm, key, c)) {
+        if (inside<COUNT, WT>(S, P, seed, add(at, lift), nrm, key, c)) {
             for (uint32_t q = 1u; q < 9u; q++) {
                 float2 cc = offset(q);
                 float3 p = add(add(pos, scl(dx, cc.x)), scl(dy, cc.y));
-                if (!inside<COUNT>(S, P, seed, add(p, lift), nrm, key + q * 31u, c)) {
+                if (!inside<COUNT, WT>(S, P, seed, add(p, lift), nrm, key + q * 31u, c)) {
                     at = p;
                     pick = q;
                     span = 0.4f;
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(128) direct_kernel(Scene S, lb_params P, const
             }
             if (pick == 0u) {
                 float3 p = add(pos, scl(nrm, PUSH));
-                if (!inside<COUNT>(S, P, seed, add(p, lift), nrm, key + 331u, c)) {
+                if (!inside<COUNT, WT>(S, P, seed, add(p, lift), nrm, key + 331u, c)) {
                     at = p;
                     pick = 9u;
                     span = 0.4f;
@@ -95,10 +95,10 @@ __global__ void __launch_bounds__(128) direct_kernel(Scene S, lb_params P, const
                 float cx = ((__uint2float_rn(s % g) + 0.5f) / fg - 0.5f) * span;
                 float cy = ((__uint2float_rn(s / g) + 0.5f) / fg - 0.5f) * span;
                 float3 o = add(add(add(at, scl(dx, cx)), scl(dy, cy)), lift);
-                if (trace<COUNT>(S, o, sun, FAR, true, key + s, seed, c).tri == NONE) hard |= 1u << (s & 31u);  // WGSL shifts modulo the bit width
+                if (trace<COUNT, WT>(S, o, sun, FAR, true, key + s, seed, c).tri == NONE) hard |= 1u << (s & 31u);  // WGSL shifts modulo the bit width
                 uint32_t k = (s + turn) % gg;
                 float3 d = sun_disc(P, sf, k, gg);
-                if (trace<COUNT>(S, o, d, FAR, true, key + s + 1000u, seed, c).tri == NONE) soft += 1.0f;
+                if (trace<COUNT, WT>(S, o, d, FAR, true, key + s + 1000u, seed, c).tri == NONE) soft += 1.0f;
             }
             soft /= fgg;
         }
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(128) direct_kernel(Scene S, lb_params P, const
         float occ = 0.0f, back = 0.0f;
         for (uint32_t r = 0u; r < rays; r++) {
             float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
-            Hit h = trace<COUNT>(S, o, d, P.reach[0], false, key + r + 2000u, seed, c);
+            Hit h = trace<COUNT, WT>(S, o, d, P.reach[0], false, key + r + 2000u, seed, c);
             if (h.tri == NONE) continue;
             float k = h.t / P.reach[0];
             occ += 1.0f - k * k;
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(128) direct_kernel(Scene S, lb_params P, const
 }
 
 // trace.wgsl:245-270
-template <bool COUNT>
+template <bool COUNT, bool WT>
 __global__ void __launch_bounds__(128) gather_kernel(Scene S, lb_params P, const float4 *items, uint32_t n,
                                                      uint32_t base, const float4 *light, uint32_t n_light,
                                                      float4 *out, unsigned long long *counters) {
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(128) gather_kernel(Scene S, lb_params P, const
             float jx = rnd(key + r, 19u, seed) - 0.5f, jy = rnd(key + r, 23u, seed) - 0.5f;
             float3 o = add(add(add(pos, scl(dx, jx)), scl(dy, jy)), scl(nrm, P.reach[2]));
             float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
-            Hit h = trace<COUNT>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c);
+            Hit h = trace<COUNT, WT>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c);
             if (h.tri == NONE) {
                 sum = add(sum, sky(P, d));
                 continue;
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(128) gather_kernel(Scene S, lb_params P, const
 }
 
 // trace.wgsl:272-324
-template <bool COUNT>
+template <bool COUNT, bool WT>
 __global__ void __launch_bounds__(128) volume_kernel(Scene S, lb_params P, const float4 *items, uint32_t n,
                                                      const float4 *light, uint32_t n_light, float4 *out,
                                                      unsigned long long *counters) {
@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(128) volume_kernel(Scene S, lb_params P, const
             float sa, ca;
             sincos32(a, &sa, &ca);
             float3 d = mk(rr * ca, z, rr * sa);
-            Hit h = trace<COUNT>(S, o, d, P.reach[1], false, key + r, seed, c);
+            Hit h = trace<COUNT, WT>(S, o, d, P.reach[1], false, key + r, seed, c);
             float3 l = sky(P, d);
             if (h.tri != NONE) {
                 if (h.back) back += 1.0f;
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(128) volume_kernel(Scene S, lb_params P, const
         float sun = 0.0f;
         for (uint32_t s = 0u; s < gg; s++) {
             float3 d = sun_disc(P, sf, s, gg);
-            if (trace<COUNT>(S, o, d, FAR, true, key + s + 9000u, seed, c).tri == NONE) sun += 1.0f;
+            if (trace<COUNT, WT>(S, o, d, FAR, true, key + s + 9000u, seed, c).tri == NONE) sun += 1.0f;
         }
         float3 a0 = scl(l0, w), ax = scl(l1x, w), ay = scl(l1y, w), az = scl(l1z, w);
         out[4 * i] = make_float4(a0.x, a0.y, a0.z, sun / __uint2float_rn(gg));
@@ -219,28 +219,38 @@ __global__ void __launch_bounds__(128) volume_kernel(Scene S, lb_params P, const
 
 }  // namespace lbd
 
+namespace {
+template <bool COUNT, bool WT>
+cudaError_t launch_bvh2(int pass, dim3 grid, int T, const lbd::Scene &S, const lb_params &P, const float4 *items,
+                        uint32_t n, uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
+                        unsigned long long *counters, cudaStream_t stream) {
+    switch (pass) {
+    case LB_PASS_DIRECT:
+        lbd::direct_kernel<COUNT, WT><<<grid, T, 0, stream>>>(S, P, items, n, base, out, counters);
+        break;
+    case LB_PASS_GATHER:
+        lbd::gather_kernel<COUNT, WT><<<grid, T, 0, stream>>>(S, P, items, n, base, light, n_light, out, counters);
+        break;
+    case LB_PASS_VOLUME:
+        lbd::volume_kernel<COUNT, WT><<<grid, T, 0, stream>>>(S, P, items, n, light, n_light, out, counters);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t lb_launch_pass_bvh2(int pass, const lbd::Scene &S, const lb_params &P, const float4 *items, uint32_t n,
                                 uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
                                 unsigned long long *counters, bool full_count, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     const int T = 128;
     dim3 grid((n + T - 1) / T);
-    bool count = full_count;
-    switch (pass) {
-    case LB_PASS_DIRECT:
-        if (count) lbd::direct_kernel<true><<<grid, T, 0, stream>>>(S, P, items, n, base, out, counters);
-        else lbd::direct_kernel<false><<<grid, T, 0, stream>>>(S, P, items, n, base, out, counters);
-        break;
-    case LB_PASS_GATHER:
-        if (count) lbd::gather_kernel<true><<<grid, T, 0, stream>>>(S, P, items, n, base, light, n_light, out, counters);
-        else lbd::gather_kernel<false><<<grid, T, 0, stream>>>(S, P, items, n, base, light, n_light, out, counters);
-        break;
-    case LB_PASS_VOLUME:
-        if (count) lbd::volume_kernel<true><<<grid, T, 0, stream>>>(S, P, items, n, light, n_light, out, counters);
-        else lbd::volume_kernel<false><<<grid, T, 0, stream>>>(S, P, items, n, light, n_light, out, counters);
-        break;
-    default:
-        return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+    const bool wt = S.verts != nullptr;  // the watertight kernels (lb_scene_set_vertices)
+    if (full_count)
+        return wt ? launch_bvh2<true, true>(pass, grid, T, S, P, items, n, base, light, n_light, out, counters, stream)
+                  : launch_bvh2<true, false>(pass, grid, T, S, P, items, n, base, light, n_light, out, counters, stream);
+    return wt ? launch_bvh2<false, true>(pass, grid, T, S, P, items, n, base, light, n_light, out, counters, stream)
+              : launch_bvh2<false, false>(pass, grid, T, S, P, items, n, base, light, n_light, out, counters, stream);
 }

@@ -95,7 +95,7 @@ __device__ __forceinline__ Item load_item(const float4 *tex, const uint32_t *idx
 
 // trace.wgsl:159-168 with lanes 0..15 each tracing one of the 16 rays; true on every lane when more than
 // insideShare of them meet back faces. The count of back faces is exact, as the shader's float sum of ones.
-template <int BVH, bool COUNT>
+template <int BVH, bool COUNT, bool WT>
 __device__ __forceinline__ bool inside_warp(const Scene &S, const lb_params &P, uint32_t seed, float3 o, float3 n,
                                             uint32_t key, int lane, Count &c) {
     bool back = false;
@@ -103,7 +103,7 @@ __device__ __forceinline__ bool inside_warp(const Scene &S, const lb_params &P, 
         Frame f = frame(n);
         uint32_t r = uint32_t(lane);
         float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
-        Hit h = walk<BVH, COUNT>(S, o, d, P.ground[3], false, key + r + 7000u, seed, c);
+        Hit h = walk<BVH, COUNT, WT>(S, o, d, P.ground[3], false, key + r + 7000u, seed, c);
         back = h.tri != NONE && h.back;
     }
     float nb = __uint2float_rn(__popc(__ballot_sync(FULL, back)));
@@ -112,7 +112,7 @@ __device__ __forceinline__ bool inside_warp(const Scene &S, const lb_params &P, 
 
 // The same test over the texel's leaf list (a list that holds every leaf the test's rays can meet: they
 // start within `shift` of its centre, head into the same hemisphere and reach no farther than the list).
-template <bool COUNT>
+template <bool COUNT, bool WT>
 __device__ __forceinline__ bool inside_list(const Scene &S, const lb_params &P, uint32_t seed, const uint32_t *list,
                                             const float *dist2, int nl, float3 o, float3 n, uint32_t key, int lane,
                                             Count &c, float shift) {
@@ -121,7 +121,7 @@ __device__ __forceinline__ bool inside_list(const Scene &S, const lb_params &P, 
         Frame f = frame(n);
         uint32_t r = uint32_t(lane);
         float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
-        Hit h = trace_list<COUNT>(S, list, dist2, nl, o, d, P.ground[3], key + r + 7000u, seed, c, shift);
+        Hit h = trace_list<COUNT, WT>(S, list, dist2, nl, o, d, P.ground[3], key + r + 7000u, seed, c, shift);
         back = h.tri != NONE && h.back;
     }
     float nb = __uint2float_rn(__popc(__ballot_sync(FULL, back)));
@@ -148,9 +148,10 @@ __device__ __forceinline__ void flush_counts(Count &c, unsigned long long *count
     }
 }
 
-// trace.wgsl:170-243. OCC: blocks of 256 threads an SM must hold (the compiler's register budget).
-template <int BVH, bool COUNT, int OCC = 1, int WALK = 0>
-__global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
+// trace.wgsl:170-243. OCC: blocks of 256 threads an SM must hold (1: the compiler's budget, capped at 128
+// registers so that two blocks still fit).
+template <int BVH, bool COUNT, int OCC = 1, int WALK = 0, bool WT = false>
+__global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
                                                    unsigned long long *counters, int group, int refill, int near) {
     __shared__ float s_term[WARPS][AO_CAP];
@@ -206,8 +207,8 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
         auto inside_at = [&](float3 o, uint32_t k) -> bool {
             float shift;
             if (listed_from(o, shift))
-                return inside_list<COUNT>(S, P, seed, s_list[wi], s_dist[wi], nl, o, nrm, k, lane, c, shift);
-            return inside_warp<BVH, COUNT>(S, P, seed, o, nrm, k, lane, c);
+                return inside_list<COUNT, WT>(S, P, seed, s_list[wi], s_dist[wi], nl, o, nrm, k, lane, c, shift);
+            return inside_warp<BVH, COUNT, WT>(S, P, seed, o, nrm, k, lane, c);
         };
         if (inside_at(c0, key)) {
             for (uint32_t q = 1u; q < 9u; q++) {
@@ -245,10 +246,10 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
                     float cy = ((__uint2float_rn(s / g) + 0.5f) / fg - 0.5f) * span;
                     float3 o = add(add(add(at, scl(dx, cx)), scl(dy, cy)), lift);
                     if (lane < 16) {
-                        escaped = walk<BVH, COUNT>(S, o, sun, FAR, true, key + s, seed, c).tri == NONE;
+                        escaped = walk<BVH, COUNT, WT>(S, o, sun, FAR, true, key + s, seed, c).tri == NONE;
                     } else {
                         float3 d = sun_disc(P, sf, (s + turn) % gg, gg);
-                        escaped = walk<BVH, COUNT>(S, o, d, FAR, true, key + s + 1000u, seed, c).tri == NONE;
+                        escaped = walk<BVH, COUNT, WT>(S, o, d, FAR, true, key + s + 1000u, seed, c).tri == NONE;
                     }
                 }
                 unsigned m = __ballot_sync(FULL, escaped);
@@ -282,7 +283,7 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
                 uint32_t r = ord.ray(r0 >> 5);
                 if (r < rays) {
                     float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
-                    Hit h = trace_list<COUNT>(S, s_list[w], s_dist[w], nl, o, d, P.reach[0], key + r + 2000u, seed, c,
+                    Hit h = trace_list<COUNT, WT>(S, s_list[w], s_dist[w], nl, o, d, P.reach[0], key + r + 2000u, seed, c,
                                               ao_shift);
                     float term = 0.0f;
                     bool hit = h.tri != NONE;
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
             __syncwarp();
         } else if (BVH == 2 && WALK == 2 && refill && rays <= AO_CAP) {
             // lane refill: a lane takes the item's next ray as soon as its own has ended
-            Walk2<COUNT> wk;
+            Walk2<COUNT, WT> wk;
             uint32_t seq = uint32_t(lane), next = 32, r = 0, myback = 0;
             bool have = seq < rays;
             if (have) {
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
             float term = 0.0f;
             if (r < rays) {
                 float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
-                Hit h = walk<BVH, COUNT>(S, o, d, P.reach[0], false, key + r + 2000u, seed, c);
+                Hit h = walk<BVH, COUNT, WT>(S, o, d, P.reach[0], false, key + r + 2000u, seed, c);
                 if (h.tri != NONE) {
                     hit = true;
                     float kk = h.t / P.reach[0];
@@ -383,7 +384,7 @@ __global__ void __launch_bounds__(256, OCC) direct_warp(Scene S, lb_params P, co
 }
 
 // trace.wgsl:245-270. rec (optional): each ray's outcome ([item][ray], gather_record) for later bounces.
-template <int BVH, bool COUNT, int OCC = 1, int WALK = 0>
+template <int BVH, bool COUNT, int OCC = 1, int WALK = 0, bool WT = false>
 __global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const float4 *pos_override, const uint32_t *n_dev, uint32_t n_host,
                                                    uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
@@ -412,7 +413,7 @@ __global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, co
         const bool refilling = BVH == 2 && WALK == 2 && refill && rays <= GI_CAP;
         if (refilling) {
             // lane refill: a lane takes the item's next ray as soon as its own has ended
-            Walk2<COUNT> wk;
+            Walk2<COUNT, WT> wk;
             uint32_t seq = uint32_t(lane), next = 32, r = 0, myback = 0;
             bool have = seq < rays;
             auto begin = [&](uint32_t rr) {
@@ -468,7 +469,7 @@ __global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, co
                 float jx = rnd(key + r, 19u, seed) - 0.5f, jy = rnd(key + r, 23u, seed) - 0.5f;
                 float3 o = add(add(add(pos, scl(dx, jx)), scl(dy, jy)), scl(nrm, P.reach[2]));
                 float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
-                Hit h = walk<BVH, COUNT>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c);
+                Hit h = walk<BVH, COUNT, WT>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c);
                 if (h.tri == NONE) {
                     term = sky(P, d);
                     on = true;
@@ -502,7 +503,7 @@ __global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, co
 }
 
 // trace.wgsl:272-324. `slot` (optional) scatters probe k's four records to 4 * slot[k].
-template <int BVH, bool COUNT>
+template <int BVH, bool COUNT, bool WT = false>
 __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const float4 *tex, uint32_t n, const float4 *light,
                                                    uint32_t n_light, float4 *out, const uint32_t *slot,
                                                    unsigned long long *counters) {
@@ -533,7 +534,7 @@ __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const f
                 float sa, ca;
                 sincos32(a, &sa, &ca);
                 float3 d = mk(rr * ca, z, rr * sa);
-                Hit h = walk<BVH, COUNT>(S, o, d, P.reach[1], false, key + r, seed, c);
+                Hit h = walk<BVH, COUNT, WT>(S, o, d, P.reach[1], false, key + r, seed, c);
                 float3 l = sky(P, d);
                 if (h.tri != NONE) {
                     bk = h.back;
@@ -560,7 +561,7 @@ __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const f
             bool esc = false;
             if (s < gg) {
                 float3 d = sun_disc(P, sf, s, gg);
-                esc = walk<BVH, COUNT>(S, o, d, FAR, true, key + s + 9000u, seed, c).tri == NONE;
+                esc = walk<BVH, COUNT, WT>(S, o, d, FAR, true, key + s + 9000u, seed, c).tri == NONE;
             }
             nsun += __popc(__ballot_sync(FULL, esc));
         }
@@ -589,60 +590,83 @@ static int walk_of(const WarpPass &w) {
     return (w.near && w.pass == LB_PASS_DIRECT) ? 1 : 0;
 }
 
-template <int BVH, bool COUNT, int OCC, int WALK> int blocks_walk(int pass) {
+template <int BVH, bool COUNT, int OCC, int WALK, bool WT> int blocks_walk(int pass) {
     const int T = 256;
     int per_sm = 0;
     cudaError_t e;
     switch (pass) {
     case LB_PASS_DIRECT:
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::direct_warp<BVH, COUNT, OCC, WALK>, T, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::direct_warp<BVH, COUNT, OCC, WALK, WT>, T, 0);
         break;
     case LB_PASS_GATHER:
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::gather_warp<BVH, COUNT, OCC, WALK>, T, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::gather_warp<BVH, COUNT, OCC, WALK, WT>, T, 0);
         break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::volume_warp<BVH, COUNT>, T, 0); break;
+    default:
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbd::volume_warp<BVH, COUNT, WT>, T, 0);
+        break;
     }
     return (e != cudaSuccess || per_sm < 1) ? 1 : per_sm;
 }
 
-template <int BVH, bool COUNT, int OCC, int WALK> void launch_walk(const WarpPass &w, int blocks, cudaStream_t stream) {
+template <int BVH, bool COUNT, int OCC, int WALK, bool WT>
+void launch_walk(const WarpPass &w, int blocks, cudaStream_t stream) {
     const int T = 256;
     switch (w.pass) {
     case LB_PASS_DIRECT:
-        lbd::direct_warp<BVH, COUNT, OCC, WALK><<<blocks, T, 0, stream>>>(
+        lbd::direct_warp<BVH, COUNT, OCC, WALK, WT><<<blocks, T, 0, stream>>>(
             *w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base, w.out, w.counters, w.group, w.refill, w.near);
         break;
     case LB_PASS_GATHER:
-        lbd::gather_warp<BVH, COUNT, OCC, WALK><<<blocks, T, 0, stream>>>(
+        lbd::gather_warp<BVH, COUNT, OCC, WALK, WT><<<blocks, T, 0, stream>>>(
             *w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host, w.base, w.light, w.n_light, w.out, w.counters, w.group,
             w.refill, w.rec);
         break;
     default:
-        lbd::volume_warp<BVH, COUNT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light, w.out,
-                                                               w.slot, w.counters);
+        lbd::volume_warp<BVH, COUNT, WT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light,
+                                                                   w.out, w.slot, w.counters);
         break;
     }
 }
 
+// the watertight kernels: the scene has vertices (lb_scene_set_vertices); a pass sized before its scene
+// is known is sized as the shader's test
+static bool watertight(const WarpPass &w) { return w.S != nullptr && w.S->verts != nullptr; }
+
 template <int BVH, bool COUNT, int OCC = 1> int blocks_for(const WarpPass &w) {
+    if (watertight(w)) {
+        switch (walk_of(w)) {
+        case 1: return blocks_walk<BVH, COUNT, 1, 1, true>(w.pass);
+        case 2: return blocks_walk<BVH, COUNT, 1, 2, true>(w.pass);
+        default: return blocks_walk<BVH, COUNT, 1, 0, true>(w.pass);
+        }
+    }
     switch (walk_of(w)) {
-    case 1: return blocks_walk<BVH, COUNT, OCC, 1>(w.pass);
-    case 2: return blocks_walk<BVH, COUNT, OCC, 2>(w.pass);
-    default: return blocks_walk<BVH, COUNT, OCC, 0>(w.pass);
+    case 1: return blocks_walk<BVH, COUNT, OCC, 1, false>(w.pass);
+    case 2: return blocks_walk<BVH, COUNT, OCC, 2, false>(w.pass);
+    default: return blocks_walk<BVH, COUNT, OCC, 0, false>(w.pass);
     }
 }
 
 template <int BVH, bool COUNT, int OCC = 1> void launch(const WarpPass &w, int blocks, cudaStream_t stream) {
+    if (watertight(w)) {
+        switch (walk_of(w)) {
+        case 1: launch_walk<BVH, COUNT, 1, 1, true>(w, blocks, stream); break;
+        case 2: launch_walk<BVH, COUNT, 1, 2, true>(w, blocks, stream); break;
+        default: launch_walk<BVH, COUNT, 1, 0, true>(w, blocks, stream); break;
+        }
+        return;
+    }
     switch (walk_of(w)) {
-    case 1: launch_walk<BVH, COUNT, OCC, 1>(w, blocks, stream); break;
-    case 2: launch_walk<BVH, COUNT, OCC, 2>(w, blocks, stream); break;
-    default: launch_walk<BVH, COUNT, OCC, 0>(w, blocks, stream); break;
+    case 1: launch_walk<BVH, COUNT, OCC, 1, false>(w, blocks, stream); break;
+    case 2: launch_walk<BVH, COUNT, OCC, 2, false>(w, blocks, stream); break;
+    default: launch_walk<BVH, COUNT, OCC, 0, false>(w, blocks, stream); break;
     }
 }
 
-// the register-capped variants exist for the BVH2 walk without counting (the product's passes)
+// the register-capped variants exist for the BVH2 walk without counting (the product's passes) with the
+// shader's triangle test
 static bool capped(const WarpPass &w) {
-    return w.bvh == 2 && !w.full_count && w.pass != LB_PASS_VOLUME && (w.occ == 3 || w.occ == 4);
+    return w.bvh == 2 && !w.full_count && w.pass != LB_PASS_VOLUME && (w.occ == 3 || w.occ == 4) && !watertight(w);
 }
 
 int lb_warp_pass_blocks(const WarpPass &w) {

@@ -189,6 +189,8 @@ lbd::Scene lb_scene_view(const lb_scene *s) {
                  s->n_nodes, s->n_tris, s->n_mats, s->n_charts};
     S.nodes8 = (const uint4 *)s->nodes8;
     S.tris8 = (const float4 *)s->tris8;
+    S.verts = (const float4 *)s->verts;
+    S.grow = s->verts ? 1.0000004f : 1.0f;
     return S;
 }
 
@@ -197,9 +199,37 @@ extern "C" {
 void lb_scene_free(lb_scene *s) {
     if (!s) return;
     cudaSetDevice(s->gpu->device);
-    for (void *p : {s->nodes, s->tris, s->mats, s->charts, s->nodes8, s->tris8})
+    for (void *p : {s->nodes, s->tris, s->mats, s->charts, s->nodes8, s->tris8, s->verts})
         if (p) cudaFree(p);
     delete s;
+}
+
+int lb_scene_set_vertices(lb_gpu *g, lb_scene *s, const float *verts, size_t n_tris) {
+    if (!g || !s || s->gpu != g || (verts && n_tris != s->n_tris) || (!verts && n_tris)) {
+        lb_set_error("lb_scene_set_vertices: bad arguments (one vertex triple for each uploaded triangle)");
+        return LB_EINVAL;
+    }
+    LB_CUDA(cudaSetDevice(g->device), "cudaSetDevice");
+    LB_CUDA(cudaStreamSynchronize(g->stream), "lb_scene_set_vertices");
+    if (s->verts) {
+        cudaFree(s->verts);
+        s->verts = nullptr;
+    }
+    if (!verts || n_tris == 0) return LB_OK;
+    std::vector<float> v4(n_tris * 12, 0.0f);
+    for (size_t i = 0; i < n_tris * 3; i++)
+        for (int k = 0; k < 3; k++) v4[i * 4 + k] = verts[i * 3 + k];
+    size_t bytes = v4.size() * sizeof(float);
+    void *p = nullptr;
+    LB_CUDA(cudaMalloc(&p, bytes), "lb_scene_set_vertices");
+    cudaError_t e = cudaMemcpy(p, v4.data(), bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(p);
+        return lb_cuda_fail(e, "lb_scene_set_vertices");
+    }
+    g->h2d += bytes;
+    s->verts = p;
+    return LB_OK;
 }
 
 int lb_run(lb_gpu *g, lb_scene *s, int pass, const lb_params *params, const lb_texel *items, size_t n,

@@ -47,6 +47,14 @@ def lib():
         l.or_trace.restype = C.c_int
         l.or_trace.argtypes = [C.c_int, vp, sz, vp, sz, vp, sz, vp, vp, vp, C.c_float, C.c_int, C.c_uint32,
                                C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.POINTER(C.c_int)]
+        l.or_run_ex.restype = C.c_int
+        l.or_run_ex.argtypes = l.or_run.argtypes + [vp]
+        l.or_trace_ex.restype = C.c_int
+        l.or_trace_ex.argtypes = l.or_trace.argtypes + [vp]
+        l.or_trace_rays.restype = C.c_int
+        l.or_trace_rays.argtypes = [C.c_int, vp, sz, vp, sz, vp, sz, vp, vp, sz, C.c_int, vp, vp, vp, vp, C.c_int]
+        l.or_rays_ambiguous.restype = C.c_int
+        l.or_rays_ambiguous.argtypes = [vp, sz, vp, sz, vp, sz, vp, vp, sz, C.c_double, vp, C.c_int]
         l.or_ray_ambiguous.restype = C.c_int
         l.or_ray_ambiguous.argtypes = [vp, sz, vp, sz, vp, sz, vp, vp, vp, C.c_float, C.c_uint32, C.c_double]
         l.or_item_rays.restype = sz
@@ -76,17 +84,21 @@ def _p(a):
 
 
 class Scene:
-    """The scene arrays the passes read (the same ones lb_scene_upload takes)."""
+    """The scene arrays the passes read (the same ones lb_scene_upload takes); with `verts` (9 floats a
+    triangle) the FP32 walk uses the watertight triangle test, as lb_scene_set_vertices switches the
+    kernels."""
 
-    def __init__(self, nodes, tris, materials, charts):
+    def __init__(self, nodes, tris, materials, charts, verts=None):
         self.nodes = np.ascontiguousarray(nodes)
         self.tris = np.ascontiguousarray(tris)
         self.materials = np.ascontiguousarray(materials, dtype=np.float32).reshape(-1, 4)
         self.charts = np.ascontiguousarray(charts, dtype=np.float32).reshape(-1, 8)
+        self.verts = None if verts is None else np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 9)
 
     @staticmethod
-    def of(prepared) -> "Scene":
-        return Scene(prepared.nodes, prepared.tris, prepared.materials, prepared.charts)
+    def of(prepared, watertight: bool = False) -> "Scene":
+        return Scene(prepared.nodes, prepared.tris, prepared.materials, prepared.charts,
+                     prepared.verts if watertight else None)
 
 
 def run(pass_: int, scene: Scene, params, items: np.ndarray, light=None, threads: int = 0):
@@ -101,10 +113,10 @@ def run(pass_: int, scene: Scene, params, items: np.ndarray, light=None, threads
         la = np.ascontiguousarray(light, dtype=np.float32).reshape(-1, 4)
         nl = len(la)
     cnt = Counters()
-    rc = lib().or_run(int(pass_), _p(scene.nodes), len(scene.nodes), _p(scene.tris), len(scene.tris),
-                      _p(scene.materials), len(scene.materials), _p(scene.charts) if len(scene.charts) else None,
-                      len(scene.charts), C.byref(params), _p(items), n, _p(la), nl, _p(out), int(threads),
-                      C.byref(cnt))
+    rc = lib().or_run_ex(int(pass_), _p(scene.nodes), len(scene.nodes), _p(scene.tris), len(scene.tris),
+                         _p(scene.materials), len(scene.materials), _p(scene.charts) if len(scene.charts) else None,
+                         len(scene.charts), C.byref(params), _p(items), n, _p(la), nl, _p(out), int(threads),
+                         C.byref(cnt), _p(scene.verts))
     if rc != 0:
         raise RuntimeError(f"oracle run failed: {rc}")
     return out, {"rays": cnt.rays, "nodes": cnt.nodes, "tris": cnt.tris, "mats": cnt.mats,
@@ -117,10 +129,43 @@ def trace(scene: Scene, params, o, d, tmax, any_hit, ray, precision=32):
     back = C.c_int()
     oa = (C.c_float * 3)(*o)
     da = (C.c_float * 3)(*d)
-    lib().or_trace(precision, _p(scene.nodes), len(scene.nodes), _p(scene.tris), len(scene.tris),
-                   _p(scene.materials), len(scene.materials), C.byref(params), oa, da, float(tmax), int(any_hit),
-                   int(ray) & 0xffffffff, C.byref(t), C.byref(tri), C.byref(back))
+    lib().or_trace_ex(precision, _p(scene.nodes), len(scene.nodes), _p(scene.tris), len(scene.tris),
+                      _p(scene.materials), len(scene.materials), C.byref(params), oa, da, float(tmax), int(any_hit),
+                      int(ray) & 0xffffffff, C.byref(t), C.byref(tri), C.byref(back), _p(scene.verts))
     return t.value, tri.value, bool(back.value)
+
+
+RAY = np.dtype([("o", "<f4", 3), ("tmax", "<f4"), ("d", "<f4", 3), ("key", "<u4")])
+
+
+def rays_of(r) -> np.ndarray:
+    """An item_rays dict as a RAY array (the layout of lb_ray)."""
+    out = np.zeros(len(r["d"]), RAY)
+    out["o"], out["d"], out["tmax"], out["key"] = r["o"], r["d"], r["tmax"], r["key"]
+    return out
+
+
+def trace_rays(scene: Scene, params, rays: np.ndarray, any_hit: bool, precision: int = 32, threads: int = 0):
+    """trace() of every ray of a RAY array: (t float64, tri uint32, back bool) arrays."""
+    rays = np.ascontiguousarray(rays, dtype=RAY)
+    n = len(rays)
+    t = np.zeros(n, np.float64)
+    tri = np.zeros(n, np.uint32)
+    back = np.zeros(n, np.int32)
+    lib().or_trace_rays(int(precision), _p(scene.nodes), len(scene.nodes), _p(scene.tris), len(scene.tris),
+                        _p(scene.materials), len(scene.materials), C.byref(params), _p(rays), n, int(bool(any_hit)),
+                        _p(scene.verts) if precision == 32 else None, _p(t), _p(tri), _p(back), int(threads))
+    return t, tri, back.astype(bool)
+
+
+def rays_ambiguous(scene: Scene, params, rays: np.ndarray, eps: float = 1e-4, threads: int = 0) -> np.ndarray:
+    """ray_ambiguous of every ray of a RAY array, as a bool array."""
+    rays = np.ascontiguousarray(rays, dtype=RAY)
+    out = np.zeros(len(rays), np.int32)
+    lib().or_rays_ambiguous(_p(scene.nodes), len(scene.nodes), _p(scene.tris), len(scene.tris), _p(scene.materials),
+                            len(scene.materials), C.byref(params), _p(rays), len(rays), float(eps), _p(out),
+                            int(threads))
+    return out.astype(bool)
 
 
 def ray_ambiguous(scene: Scene, params, o, d, tmax, ray, eps=1e-5) -> bool:

@@ -40,11 +40,32 @@ int or_run(int pass, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, s
            const lb_params *params, const lb_texel *items, size_t n, const float *light,
            size_t n_light, float *out, int threads, or_counters *counters);
 
+/* or_run with the watertight triangle test over `verts` (9 floats a triangle, in tris order; NULL: the
+ * shader's test), as lb_scene_set_vertices switches the kernels. */
+int or_run_ex(int pass, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+              const float *materials, size_t n_materials, const float *charts, size_t n_charts,
+              const lb_params *params, const lb_texel *items, size_t n, const float *light,
+              size_t n_light, float *out, int threads, or_counters *counters, const float *verts);
+
 /* One ray through the scene, in FP32 (precision 32) or FP64 (64); writes t, triangle
  * (0xffffffff: none), back face. `any`: the first accepted hit. */
 int or_trace(int precision, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
              const float *materials, size_t n_materials, const lb_params *params, const float o[3],
              const float d[3], float tmax, int any, uint32_t ray, double *t, uint32_t *tri, int *back);
+/* or_trace with the watertight test over `verts` for the FP32 walk (NULL: the shader's test). */
+int or_trace_ex(int precision, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+                const float *materials, size_t n_materials, const lb_params *params, const float o[3],
+                const float d[3], float tmax, int any, uint32_t ray, double *t, uint32_t *tri, int *back,
+                const float *verts);
+
+/* or_trace_ex over n rays (8 floats each, as lb_ray: o, tmax, d, key bits), in parallel. */
+int or_trace_rays(int precision, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+                  const float *materials, size_t n_materials, const lb_params *params, const float *rays, size_t n,
+                  int any, const float *verts, double *t, uint32_t *tri, int *back, int threads);
+/* or_ray_ambiguous over n rays (as or_trace_rays), in parallel: out[i] 1 where ambiguous. */
+int or_rays_ambiguous(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+                      const float *materials, size_t n_materials, const lb_params *params, const float *rays,
+                      size_t n, double eps, int *out, int threads);
 
 /* Is this ray within `eps` of deciding differently: does it pass, in FP64, within eps (barycentric)
  * of the edge of a triangle that stops it, or meet one within eps (relative) of 1e-4 or tmax? */

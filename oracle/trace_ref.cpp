@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -120,6 +121,8 @@ struct Ctx {
     const lb_params *P;
     uint32_t seed;
     or_counters *cnt;  // per thread
+    // exact vertices (9 floats a triangle): the FP32 walk uses the watertight test and widens box exits
+    const float *verts = nullptr;
 };
 
 // trace.wgsl:63-66 (mix(a, b, t) = a * (1 - t) + b * t)
@@ -140,15 +143,50 @@ inline bool stops(const Ctx &C, uint32_t tri, uint32_t ray) {
     return op >= 1.0f || rnd(tri * 9781u, ray, C.seed) < op;
 }
 
-// trace.wgsl:74-80
-template <class T> inline T box(V3<T> o, V3<T> inv, V3<T> mn, V3<T> mx, T tmax, T far) {
+// trace.wgsl:74-80; grow (1 for the shader) scales the exit distance for the watertight walk
+template <class T> inline T box(V3<T> o, V3<T> inv, V3<T> mn, V3<T> mx, T tmax, T far, T grow = T(1)) {
     V3<T> a = mulv(mn - o, inv);
     V3<T> b = mulv(mx - o, inv);
     T lo = vmax(vmax(vmin(a.x, b.x), vmin(a.y, b.y)), vmin(a.z, b.z));
     T hi = vmin(vmin(vmax(a.x, b.x), vmax(a.y, b.y)), vmax(a.z, b.z));
     T l0 = vmax(lo, T(0));
-    return (hi >= l0 && lo < tmax) ? l0 : far;
+    return (hi * grow >= l0 && lo < tmax) ? l0 : far;
 }
+
+// The watertight ray/triangle test (Woop, Benthin and Wald, "Watertight Ray/Triangle Intersection", JCGT
+// 2(1), 2013) in FP32: shear the ray's largest axis onto +z (the other two in the order that keeps the
+// frame's handedness), then three edge functions of the sheared vertices, each a difference of two
+// rounded products, recomputed in FP64 when one is exactly zero. Writes t and the face (det < 0: back).
+inline float axis(V3<float> v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+inline bool watertight(const float *verts, uint32_t i, V3<float> o, V3<float> d, float &t, bool &back) {
+    float ax = std::fabs(d.x), ay = std::fabs(d.y), az = std::fabs(d.z);
+    int kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    float dz = axis(d, kz);
+    if (dz < 0.0f) std::swap(kx, ky);
+    float sx = axis(d, kx) / dz, sy = axis(d, ky) / dz, sz = 1.0f / dz;
+    const float *v = verts + size_t(i) * 9;
+    V3<float> A = mk(v[0], v[1], v[2]) - o, B = mk(v[3], v[4], v[5]) - o, Cv = mk(v[6], v[7], v[8]) - o;
+    float Az = axis(A, kz), Bz = axis(B, kz), Cz = axis(Cv, kz);
+    float Ax = axis(A, kx) - sx * Az, Ay = axis(A, ky) - sy * Az;
+    float Bx = axis(B, kx) - sx * Bz, By = axis(B, ky) - sy * Bz;
+    float Cx = axis(Cv, kx) - sx * Cz, Cy = axis(Cv, ky) - sy * Cz;
+    float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
+        V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+        W = float(double(Bx) * double(Ay) - double(By) * double(Ax));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    float det = U + V + W;
+    if (det == 0.0f) return false;
+    float T = U * (sz * Az) + V * (sz * Bz) + W * (sz * Cz);
+    t = T / det;
+    back = det < 0.0f;
+    return true;
+}
+constexpr float WATERTIGHT_GROW = 1.0000004f;
 
 template <class T> struct Hit {
     T t;
@@ -175,6 +213,18 @@ template <class T> Hit<T> trace(const Ctx &C, V3<T> o, V3<T> d, T tmax, bool any
         if (node.count > 0u) {
             for (uint32_t i = node.first; i < node.first + node.count; i++) {
                 if (C.cnt) C.cnt->tris++;
+                if constexpr (std::is_same_v<T, float>) {
+                    if (C.verts) {
+                        float t;
+                        bool bk;
+                        if (!watertight(C.verts, i, o, d, t, bk)) continue;
+                        if (t > 1e-4f && t < hit.t && stops(C, i, ray)) {
+                            hit = Hit<T>{t, i, bk};
+                            if (any) return hit;
+                        }
+                        continue;
+                    }
+                }
                 const lb_tri &tr = C.tris[i];
                 V3<T> e1 = cvt<T>(f3(tr.e1)), e2 = cvt<T>(f3(tr.e2)), v0 = cvt<T>(f3(tr.v0));
                 V3<T> p = cross(d, e2);
@@ -197,8 +247,9 @@ template <class T> Hit<T> trace(const Ctx &C, V3<T> o, V3<T> d, T tmax, bool any
             const lb_node &a = C.nodes[node.first];
             const lb_node &b = C.nodes[node.first + 1u];
             if (C.cnt) C.cnt->nodes += 2;
-            T ta = box(o, inv, cvt<T>(f3(a.min)), cvt<T>(f3(a.max)), hit.t, far);
-            T tb = box(o, inv, cvt<T>(f3(b.min)), cvt<T>(f3(b.max)), hit.t, far);
+            const T grow = (std::is_same_v<T, float> && C.verts) ? T(WATERTIGHT_GROW) : T(1);
+            T ta = box(o, inv, cvt<T>(f3(a.min)), cvt<T>(f3(a.max)), hit.t, far, grow);
+            T tb = box(o, inv, cvt<T>(f3(b.min)), cvt<T>(f3(b.max)), hit.t, far, grow);
             uint32_t near = ta <= tb ? node.first : node.first + 1u;
             uint32_t farc = ta <= tb ? node.first + 1u : node.first;
             T tn = vmin(ta, tb), tf = vmax(ta, tb);
@@ -439,8 +490,17 @@ int or_run(int pass, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, s
            const float *materials, size_t n_materials, const float *charts, size_t n_charts,
            const lb_params *params, const lb_texel *items, size_t n, const float *light,
            size_t n_light, float *out, int threads, or_counters *counters) {
+    return or_run_ex(pass, nodes, n_nodes, tris, n_tris, materials, n_materials, charts, n_charts, params, items, n,
+                     light, n_light, out, threads, counters, nullptr);
+}
+
+int or_run_ex(int pass, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+              const float *materials, size_t n_materials, const float *charts, size_t n_charts,
+              const lb_params *params, const lb_texel *items, size_t n, const float *light,
+              size_t n_light, float *out, int threads, or_counters *counters, const float *verts) {
     if (pass < 0 || pass > 2 || !params || (n && (!items || !out)) || !nodes || n_nodes == 0) return LB_EINVAL;
     Ctx base = make_ctx(nodes, n_nodes, tris, n_tris, materials, n_materials, charts, n_charts, params, light, n_light);
+    base.verts = verts;
     size_t width = pass == LB_PASS_VOLUME ? 4 : 1;
     if (counters) std::memset(counters, 0, sizeof *counters);
 #pragma omp parallel num_threads(threads > 0 ? threads : omp_get_max_threads())
@@ -472,13 +532,58 @@ int or_run(int pass, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, s
 int or_trace(int precision, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
              const float *materials, size_t n_materials, const lb_params *params, const float o[3],
              const float d[3], float tmax, int any, uint32_t ray, double *t, uint32_t *tri, int *back) {
+    return or_trace_ex(precision, nodes, n_nodes, tris, n_tris, materials, n_materials, params, o, d, tmax, any, ray,
+                       t, tri, back, nullptr);
+}
+
+int or_trace_ex(int precision, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+                const float *materials, size_t n_materials, const lb_params *params, const float o[3],
+                const float d[3], float tmax, int any, uint32_t ray, double *t, uint32_t *tri, int *back,
+                const float *verts) {
     Ctx C = make_ctx(nodes, n_nodes, tris, n_tris, materials, n_materials, nullptr, 0, params, nullptr, 0);
+    C.verts = verts;
     if (precision == 64) {
         Hit<double> h = trace<double>(C, mk<double>(o[0], o[1], o[2]), mk<double>(d[0], d[1], d[2]), double(tmax), any != 0, ray);
         *t = h.t; *tri = h.tri; *back = h.back;
     } else {
         Hit<float> h = trace<float>(C, mk(o[0], o[1], o[2]), mk(d[0], d[1], d[2]), tmax, any != 0, ray);
         *t = h.t; *tri = h.tri; *back = h.back;
+    }
+    return LB_OK;
+}
+
+int or_trace_rays(int precision, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+                  const float *materials, size_t n_materials, const lb_params *params, const float *rays, size_t n,
+                  int any, const float *verts, double *t, uint32_t *tri, int *back, int threads) {
+    Ctx base = make_ctx(nodes, n_nodes, tris, n_tris, materials, n_materials, nullptr, 0, params, nullptr, 0);
+    base.verts = verts;
+#pragma omp parallel for schedule(dynamic, 256) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (long long i = 0; i < (long long)n; i++) {
+        const float *r = rays + size_t(i) * 8;
+        uint32_t key;
+        std::memcpy(&key, r + 7, 4);
+        if (precision == 64) {
+            Hit<double> h = trace<double>(base, mk<double>(r[0], r[1], r[2]), mk<double>(r[4], r[5], r[6]),
+                                          double(r[3]), any != 0, key);
+            t[i] = h.t; tri[i] = h.tri; back[i] = h.back;
+        } else {
+            Hit<float> h = trace<float>(base, mk(r[0], r[1], r[2]), mk(r[4], r[5], r[6]), r[3], any != 0, key);
+            t[i] = h.t; tri[i] = h.tri; back[i] = h.back;
+        }
+    }
+    return LB_OK;
+}
+
+int or_rays_ambiguous(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
+                      const float *materials, size_t n_materials, const lb_params *params, const float *rays,
+                      size_t n, double eps, int *out, int threads) {
+#pragma omp parallel for schedule(dynamic, 256) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (long long i = 0; i < (long long)n; i++) {
+        const float *r = rays + size_t(i) * 8;
+        uint32_t key;
+        std::memcpy(&key, r + 7, 4);
+        out[i] = or_ray_ambiguous(nodes, n_nodes, tris, n_tris, materials, n_materials, params, r, r + 4, r[3], key,
+                                  eps);
     }
     return LB_OK;
 }
