@@ -384,7 +384,6 @@ void autotune(lb_plan &p) {
         int best_order = 8, best_blocks = 0, best_bvh = 2, best_refill = 0, best_near = 0, best_occ = 0;
         for (const Shape &sh : shapes)
         for (int order : orders) {
-            if (pass == LB_PASS_GATHER && sh.near) continue;
             WarpPass probe{};
             probe.S = &S;
             probe.pass = pass;
@@ -443,6 +442,7 @@ void autotune(lb_plan &p) {
             p.blocks_gather = best_blocks;
             p.bvh_gather = best_bvh;
             p.refill_gather = best_refill;
+            p.near_gather = best_near;
             p.occ_gather = best_occ;
         }
         report += std::string(pass == LB_PASS_DIRECT ? "direct" : "gather") + ": bvh " + std::to_string(best_bvh) +
@@ -516,6 +516,7 @@ void capture(lb_plan &p) {
             gw.group = p.group_gather;
             gw.bvh = p.bvh_gather;
             gw.refill = p.refill_gather;
+            gw.near = p.near_gather;
             gw.occ = p.occ_gather;
             bool replay = p.reuse && b.gi_bounces > 1, record = replay || p.keep_records;
             if (replay && bounce > 0) {
@@ -633,7 +634,7 @@ lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_
         p->group_gather = g->group_gather;
         p->bvh_direct = p->bvh_gather = p->bvh_volume = g->bvh;
         p->refill_direct = p->refill_gather = g->refill;
-        p->near_direct = g->near;
+        p->near_direct = p->near_gather = g->near;
         // the gathers default to the 4-block register cap (fastest on B200 for the BVH2 gather walk)
         p->occ_direct = g->occ;
         p->occ_gather = g->occ ? g->occ : 4;

@@ -503,10 +503,18 @@ __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float
 // distance from it), and the ray starts within `shift` of that centre, so once a box lies farther than the
 // nearest hit so far plus shift (by a relative margin far above the rounding of t, |d| and the distance),
 // neither it nor any later box can hold a nearer hit and the walk ends: the same hit as the whole list.
-template <bool COUNT, bool WT>
+// TIES: set `tie` when another accepted triangle lies within NEAR_TIE of the returned t (coincident or
+// nearly coincident faces, a ray through a shared edge or vertex). Between such triangles the tree walk's
+// answer depends on the order it opens boxes in and on its box test culling one whose entry rounds past
+// the nearest hit it holds, so a caller that must match it walks the tree for such a ray. Without TIES
+// the nearest triangle found wins (the first in list order at an exact tie).
+__device__ __forceinline__ float near_tie(float t) { return t * 1.00001f + 1e-4f; }
+template <bool COUNT, bool WT, bool TIES>
 __device__ __forceinline__ Hit trace_list_t(const Scene &S, const uint32_t *list, const float *dist2, int nl, float3 o,
-                                            float3 d, float tmax, uint32_t ray, uint32_t seed, Count &c, float shift) {
+                                            float3 d, float tmax, uint32_t ray, uint32_t seed, Count &c, float shift,
+                                            bool &tie) {
     Hit hit{tmax, NONE, false};
+    float other = FAR;  // TIES: the nearest accepted t but the hit's
     c.rays++;
     float3 dd = mk(fabsf(d.x) < 1e-12f ? 1e-12f : d.x, fabsf(d.y) < 1e-12f ? 1e-12f : d.y,
                    fabsf(d.z) < 1e-12f ? 1e-12f : d.z);
@@ -517,7 +525,9 @@ __device__ __forceinline__ Hit trace_list_t(const Scene &S, const uint32_t *list
         const uint32_t entry = list[k], node = entry & LEAF_NODE;
         float4 lo = __ldg(&S.nodes[2 * node]), hi = __ldg(&S.nodes[2 * node + 1]);
         if (COUNT) c.nodes++;
-        if (!(box<WT>(o, inv, lo, hi, hit.t, S.grow) < FAR)) continue;
+        const bool found = hit.tri != NONE;
+        // TIES: boxes entered up to NEAR_TIE past the nearest hit open too, to see the triangles near it
+        if (!(box<WT>(o, inv, lo, hi, TIES && found ? near_tie(hit.t) : hit.t, S.grow) < FAR)) continue;
         const uint32_t first = __float_as_uint(lo.w);
         for (uint32_t m = entry >> LEAF_MASK_SHIFT; m; m &= m - 1u) {
             const uint32_t i = first + uint32_t(__ffs(int(m)) - 1);
@@ -527,19 +537,25 @@ __device__ __forceinline__ Hit trace_list_t(const Scene &S, const uint32_t *list
             bool bk;
             if (!tri_hit<WT>(S, i, v0, e1, e2, o, d, t, bk)) continue;
             if (t > 1e-4f && t < hit.t && stops<COUNT>(S, i, v0.w, ray, seed, c)) {
+                if (TIES && hit.tri != NONE) other = fminf(other, hit.t);
                 hit = Hit{t, i, bk};
                 lim = (t + shift) * 1.0001f + 1e-5f;
                 lim2 = lim * lim;
+            } else if (TIES && hit.tri != NONE && t > 1e-4f && t <= near_tie(hit.t) &&
+                       stops<COUNT>(S, i, v0.w, ray, seed, c)) {
+                other = fminf(other, t);
             }
         }
     }
+    tie = TIES && hit.tri != NONE && other <= near_tie(hit.t);
     return hit;
 }
 template <bool COUNT, bool WT = false>
 __device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, const float *dist2, int nl, float3 o,
                                           float3 d, float tmax, uint32_t ray, uint32_t seed, Count &c,
                                           float shift = 0.0f) {
-    return trace_list_t<COUNT, WT>(S, list, dist2, nl, o, d, tmax, ray, seed, c, shift);
+    bool tie;
+    return trace_list_t<COUNT, WT, false>(S, list, dist2, nl, o, d, tmax, ray, seed, c, shift, tie);
 }
 
 // The same query over the 8-wide BVH: the nearest accepted hit within tmax (any: the first accepted),

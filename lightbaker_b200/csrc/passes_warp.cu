@@ -383,14 +383,28 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
     flush_counts<COUNT>(c, counters);
 }
 
+// Gather rays that find a hit this close are resolved by the texel's leaf list (WALK 1); the others walk
+// the tree. A speed parameter only: either way a ray gets the tree walk's hit.
+constexpr float GATHER_NEAR = 2.0f;
+
 // trace.wgsl:245-270. rec (optional): each ray's outcome ([item][ray], gather_record) for later bounces.
+// WALK 1 (BVH2): the warp gathers the leaves within GATHER_NEAR (widened by the jitter's reach) of the
+// texel's lifted point, and every ray first walks that list with its length cut to GATHER_NEAR; a hit
+// there is the ray's nearest (any nearer triangle lies in the list too). The rays that found none, met a
+// tie (which the tree walk settles in its own order) or start behind the list's plane queue up and walk
+// the tree in full rounds of 32, so the long walks of rays that escape no longer hold up lanes whose rays
+// ended nearby.
 template <int BVH, bool COUNT, int OCC = 1, int WALK = 0, bool WT = false>
-__global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
-                                                   const float4 *pos_override, const uint32_t *n_dev, uint32_t n_host,
-                                                   uint32_t base, const float4 *light, uint32_t n_light, float4 *out,
-                                                   unsigned long long *counters, int group, int refill, uint2 *rec) {
+__global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) gather_warp(
+    Scene S, lb_params P, const float4 *tex, const uint32_t *idx, const float4 *pos_override, const uint32_t *n_dev,
+    uint32_t n_host, uint32_t base, const float4 *light, uint32_t n_light, float4 *out, unsigned long long *counters,
+    int group, int refill, uint2 *rec) {
+    constexpr int LW = (BVH == 2 && WALK == 1) ? WARPS : 1;  // the leaf lists' shared memory, when used
     __shared__ float3 s_term[WARPS][GI_CAP];
     __shared__ uint8_t s_on[WARPS][GI_CAP];
+    __shared__ uint32_t s_list[LW][BALL_LEAVES];
+    __shared__ float s_dist[LW][BALL_LEAVES];
+    __shared__ uint16_t s_pend[LW][GI_CAP];
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -411,7 +425,76 @@ __global__ void __launch_bounds__(256, OCC) gather_warp(Scene S, lb_params P, co
         const RayOrder ord(rays, GI_CAP, group, lane);
         const int w = threadIdx.x >> 5;
         const bool refilling = BVH == 2 && WALK == 2 && refill && rays <= GI_CAP;
-        if (refilling) {
+        const bool listing = BVH == 2 && WALK == 1 && ord.grouped;
+        // the ray's origin (jittered across the texel, lifted) and direction
+        auto ray_of = [&](uint32_t rr, float3 &oo, float3 &dd) {
+            float jx = rnd(key + rr, 19u, seed) - 0.5f, jy = rnd(key + rr, 23u, seed) - 0.5f;
+            oo = add(add(add(pos, scl(dx, jx)), scl(dy, jy)), scl(nrm, P.reach[2]));
+            dd = cosine(fract((__uint2float_rn(rr) + 0.5f) / frays + s1), fract(radical(rr) + s2), f);
+        };
+        // a ray's outcome into the item's terms (by ray index) and records
+        auto finish = [&](uint32_t rr, float3 oo, float3 dd, const Hit &h, uint32_t &backs) {
+            float3 term = mk(0.f, 0.f, 0.f);
+            bool on = true;
+            if (h.tri == NONE) term = sky(P, dd);
+            else if (h.back) {
+                on = false;
+                backs++;
+            } else term = bounced(S, P, light, n_light, oo, dd, h);
+            s_term[w][rr] = term;
+            s_on[w][rr] = on;
+            if (rec) rec[size_t(k) * rays + rr] = gather_record(S, P, n_light, oo, dd, h);
+        };
+        if (listing) {
+            const int lw = LW == 1 ? 0 : w;
+            const float3 c0 = add(pos, scl(nrm, P.reach[2]));
+            // every jittered origin lies within (|dx| + |dy|) / 2 of c0
+            const float far_ = (sqrtf(dot3(dx, dx)) + sqrtf(dot3(dy, dy))) * 0.5f * 1.001f + 1e-5f;
+            const float rnear = fminf(GATHER_NEAR, P.reach[1]), rball = rnear + far_;
+            // the ball query's scratch (two levels of nodes) is the item's term array, not yet written
+            static_assert(sizeof(s_term[0]) >= 2 * BALL_FRONT * sizeof(uint32_t), "scratch fits the terms");
+            uint32_t *scratch = reinterpret_cast<uint32_t *>(&s_term[w][0]);
+            const int nl = ball_leaves<COUNT>(S, c0, rball, nrm, scratch, scratch + BALL_FRONT, s_list[lw], s_dist[lw],
+                                              lane, c);
+            const float front = -(rball * 1e-3f + 1e-4f) * 0.5f;
+            const unsigned below = (1u << lane) - 1u;
+            uint32_t npend = 0, myback = 0;
+            for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
+                const uint32_t r = ord.ray(r0 >> 5);
+                float3 o, d;
+                ray_of(r, o, d);
+                bool done = false;
+                const float3 v = sub(o, c0);
+                if (nl >= 0 && dot3(v, nrm) >= front) {
+                    const float shift = sqrtf(dot3(v, v)) * 1.001f + 1e-6f;
+                    bool tie;
+                    Hit h = trace_list_t<COUNT, WT, true>(S, s_list[lw], s_dist[lw], nl, o, d, rnear, key + r + 4000u,
+                                                          seed, c, shift, tie);
+                    if (h.tri != NONE && !tie) {
+                        done = true;
+                        finish(r, o, d, h, myback);
+                    } else {
+                        c.rays--;  // the tree walk counts it
+                    }
+                }
+                const unsigned pm = __ballot_sync(FULL, !done);
+                if (!done) s_pend[lw][npend + __popc(pm & below)] = uint16_t(r);
+                npend += __popc(pm);
+            }
+            __syncwarp();
+            for (uint32_t b0 = 0; b0 < npend; b0 += 32) {
+                const uint32_t i = b0 + uint32_t(lane);
+                if (i < npend) {
+                    const uint32_t r = s_pend[lw][i];
+                    float3 o, d;
+                    ray_of(r, o, d);
+                    Hit h = walk<BVH, COUNT, WT>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c);
+                    finish(r, o, d, h, myback);
+                }
+            }
+            for (int ofs = 16; ofs > 0; ofs >>= 1) myback += __shfl_down_sync(FULL, myback, ofs);
+            nback = __shfl_sync(FULL, myback, 0);
+        } else if (refilling) {
             // lane refill: a lane takes the item's next ray as soon as its own has ended
             Walk2<COUNT, WT> wk;
             uint32_t seq = uint32_t(lane), next = 32, r = 0, myback = 0;
@@ -582,12 +665,11 @@ __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const f
 }  // namespace lbd
 
 // The walk a pass's occlusion or gather rays take (a template parameter, so that each kernel carries only
-// its own): 0 the tree walk, 1 leaf lists (BVH2 direct pass; the tree walk when a list overflows),
-// 2 lane refill (BVH2).
+// its own): 0 the tree walk, 1 leaf lists (BVH2; the tree walk when a list overflows), 2 lane refill (BVH2).
 static int walk_of(const WarpPass &w) {
     if (w.bvh != 2 || w.pass == LB_PASS_VOLUME) return 0;
     if (w.refill) return 2;
-    return (w.near && w.pass == LB_PASS_DIRECT) ? 1 : 0;
+    return w.near ? 1 : 0;
 }
 
 template <int BVH, bool COUNT, int OCC, int WALK, bool WT> int blocks_walk(int pass) {

@@ -93,7 +93,7 @@ struct lb_plan {
     int group_direct = 8, group_gather = 8;  // ray order for the warp passes
     int bvh_direct = 2, bvh_gather = 2, bvh_volume = 2;  // BVH width for the warp passes
     int refill_direct = 0, refill_gather = 0;          // lane refill for the warp passes
-    int near_direct = 1;                               // leaf lists for the occlusion rays
+    int near_direct = 1, near_gather = 1;              // leaf lists (direct: occlusion rays; gather: near hits)
     int occ_direct = 0, occ_gather = 0;                // register caps (WarpPass::occ)
     bool reuse = true;          // later bounces evaluate the first bounce's gather records
     bool keep_records = false;  // record the first bounce's gather rays whatever the bounce count

@@ -70,7 +70,8 @@ def test_passes_bit_exact(gpu, oracle_mod, name, limit, kernel, order, bvh, refi
     gc = gpu.counters()
     c, cc = oracle_mod.run(1, sc, P.params, gi, light)
     _compare(g, c, f"{name} gather")
-    for k in ("rays", "nodes", "tris", "mats") if bvh == 2 else ("rays",):
+    # (with leaf lists a gather ray that finds its hit nearby never walks the tree)
+    for k in ("rays", "nodes", "tris", "mats") if bvh == 2 and not (near and kernel == 1) else ("rays",):
         assert gc[k] == cc[k], f"gather {k}: gpu {gc[k]} oracle {cc[k]}"
     probes = np.zeros(500, lb.TEXEL)
     probes["pos"][:, :3] = rng.uniform(0, 1, size=(500, 3)) * np.array([P.nodes[0]["max"] - P.nodes[0]["min"]]) + \
