@@ -151,7 +151,9 @@ def scene_header(scene: bytes) -> dict:
 
 def probe_items(scene: bytes):
     import lightbaker_b200 as lb
-    v = scene_header(scene)["volume"]
+    v = scene_header(scene).get("volume")
+    if not v:  # a scene without an irradiance volume
+        return np.zeros(0, dtype=lb.TEXEL)
     nx, ny, nz = [max(int(round((v["max"][a] - v["min"][a]) / v["step"])) + 1, 2) for a in range(3)]
     k = np.arange(nx * ny * nz, dtype=np.uint32)
     items = np.zeros(len(k), dtype=lb.TEXEL)
@@ -192,6 +194,8 @@ def cpu_baseline(P, direct, gather, probes, light, budget_s: float, threads: int
     while time.perf_counter() < t_end:
         for pass_, items, chunk, key in ((0, direct, 2048, "direct"), (1, gather, 1024, "gather"),
                                          (2, probes, 256, "volume")):
+            if len(items) == 0:
+                continue
             start = int(rng.integers(0, max(1, len(items) - chunk)))
             sample = items[start:start + chunk]
             t0 = time.perf_counter()

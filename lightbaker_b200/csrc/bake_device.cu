@@ -154,39 +154,48 @@ void build(lb_plan &p) {
     if (p.dirty.empty()) p.n_dirty_texels = 0;
     mark("upload and cache");
 
-    // rasterise the dirty tiles (bake.rs:138-149)
-    std::vector<lb_texel> tex(p.n_dirty_texels);
+    // rasterise the dirty tiles (bake.rs:138-149) on the device: the host sets up each tile's triangles in
+    // the host rasteriser's order (raster.rs:48-67), the device writes the texels (raster.cu), lists the
+    // covered ones and counts the (block, chart) pairs that bound the gathered texels (bake.rs:286-297)
+    cudaStream_t st = p.g->stream;
+    std::vector<std::vector<RasterTri>> per_tile(p.dirty.size());
 #pragma omp parallel for schedule(dynamic, 1)
-    for (long long wi = 0; wi < (long long)p.dirty.size(); wi++) {
-        std::vector<lb_texel> v = lb::rasterize(p.scene, layout, layout.tiles[p.dirty[wi]]);
-        std::memcpy(&tex[p.tiles_all[wi].off], v.data(), v.size() * sizeof(lb_texel));
-    }
-    std::vector<uint32_t> cov_idx, cov_k(p.n_dirty_texels, 0xffffffffu);
-    for (uint32_t i = 0; i < p.n_dirty_texels; i++)
-        if (lb::covered(tex[i])) {
-            cov_k[i] = uint32_t(cov_idx.size());
-            cov_idx.push_back(i);
-        }
-    p.n_cov = uint32_t(cov_idx.size());
-    // at most one gathered texel a chart in each ds x ds block (bake.rs:286-297): the gather records' bound
-    std::vector<uint64_t> pairs(p.dirty.size(), 0);
-#pragma omp parallel for schedule(dynamic, 1)
-    for (long long wi = 0; wi < (long long)p.dirty.size(); wi++) {
-        const DTile &t = p.tiles_all[wi];
-        std::vector<uint64_t> keys;
-        for (uint32_t y = 0; y < t.h; y++)
-            for (uint32_t x = 0; x < t.w; x++) {
-                const lb_texel &tx = tex[t.off + y * t.w + x];
-                if (!lb::covered(tx)) continue;
-                uint32_t chart;
-                std::memcpy(&chart, &tx.normal[3], 4);
-                keys.push_back((uint64_t((y / p.ds) * ((t.w + p.ds - 1) / p.ds) + x / p.ds) << 32) | chart);
-            }
-        std::sort(keys.begin(), keys.end());
-        pairs[wi] = uint64_t(std::unique(keys.begin(), keys.end()) - keys.begin());
-    }
-    p.max_gathered = 0;
-    for (uint64_t n : pairs) p.max_gathered += n;
+    for (long long wi = 0; wi < (long long)p.dirty.size(); wi++)
+        per_tile[wi] = lb::raster_triangles(p.scene, layout, layout.tiles[p.dirty[wi]], uint32_t(wi));
+    std::vector<RasterTri> rtris;
+    for (auto &v : per_tile) rtris.insert(rtris.end(), v.begin(), v.end());
+    mark("raster set-up");
+    const size_t NT = p.n_dirty_texels ? p.n_dirty_texels : 1;
+    p.tiles_d.alloc(std::max<size_t>(1, p.tiles_all.size()) * sizeof(DTile));
+    p.tex.alloc(NT * 64);
+    p.cov_idx.alloc(NT * 4);
+    p.cov_k.alloc(NT * 4);
+    DBuf rt, raster_temp, raster_counts;
+    rt.alloc(std::max<size_t>(1, rtris.size()) * sizeof(RasterTri));
+    raster_counts.alloc(16);
+    const size_t raster_bytes = lb_raster_covered_temp(uint32_t(NT));
+    raster_temp.alloc(raster_bytes);
+    if (!p.tiles_all.empty())
+        ck(cudaMemcpyAsync(p.tiles_d.p, p.tiles_all.data(), p.tiles_all.size() * sizeof(DTile), cudaMemcpyHostToDevice,
+                           st),
+           "upload");
+    if (!rtris.empty())
+        ck(cudaMemcpyAsync(rt.p, rtris.data(), rtris.size() * sizeof(RasterTri), cudaMemcpyHostToDevice, st), "upload");
+    p.g->h2d += p.tiles_all.size() * sizeof(DTile) + rtris.size() * sizeof(RasterTri);
+    mark("raster allocations and upload");
+    unsigned long long *pairs_d = raster_counts.as<unsigned long long>();
+    uint32_t *ncov_d = reinterpret_cast<uint32_t *>(pairs_d + 1);
+    ck(lb_raster_tiles(rt.as<RasterTri>(), uint32_t(rtris.size()), p.tiles_d.as<DTile>(), uint32_t(p.dirty.size()),
+                       p.n_dirty_texels, p.ds, p.tex.as<float4>(), p.cov_k.as<uint32_t>(), pairs_d, p.g->sms, st),
+       "raster");
+    ck(lb_raster_covered(p.tex.as<float4>(), p.n_dirty_texels, raster_temp.p, raster_bytes, p.cov_idx.as<uint32_t>(),
+                         ncov_d, p.cov_k.as<uint32_t>(), p.g->sms, st),
+       "covered texels");
+    uint64_t counts[2] = {0, 0};
+    ck(cudaMemcpyAsync(counts, raster_counts.p, 16, cudaMemcpyDeviceToHost, st), "raster counts");
+    ck(cudaStreamSynchronize(st), "raster");
+    p.max_gathered = p.n_dirty_texels ? counts[0] : 0;
+    p.n_cov = p.n_dirty_texels ? uint32_t(counts[1] & 0xffffffffu) : 0;
     mark("raster");
 
     // cached tiles' light, the atlas owner map and the atlas the first bounce reads
@@ -263,12 +272,7 @@ void build(lb_plan &p) {
     mark("atlas and volume");
     // device memory
     size_t N = p.n_dirty_texels ? p.n_dirty_texels : 1, A = p.n_all ? p.n_all : 1;
-    std::vector<DTile> dirty_tiles(p.tiles_all.begin(), p.tiles_all.begin() + p.dirty.size());
-    p.tiles_d.alloc(std::max<size_t>(1, p.tiles_all.size()) * sizeof(DTile));
-    p.tex.alloc(N * 64);
-    p.cov_idx.alloc(std::max<size_t>(1, cov_idx.size()) * 4);
-    p.cov_k.alloc(N * 4);
-    p.direct_out.alloc(std::max<size_t>(1, cov_idx.size()) * 16);
+    p.direct_out.alloc(std::max<size_t>(1, size_t(p.n_cov)) * 16);
     p.chart.alloc(A * 4);
     for (DBuf *d : {&p.valid, &p.known_tmp, &p.gathered}) d->alloc(N);
     for (DBuf *d : {&p.state, &p.known}) d->alloc(A);
@@ -282,7 +286,7 @@ void build(lb_plan &p) {
     p.wr.alloc(wr.size() * 4);
     p.gath_idx.alloc(N * 4);
     p.gath_count.alloc(16);
-    p.gather_out.alloc(std::max<size_t>(1, cov_idx.size()) * 16);
+    p.gather_out.alloc(std::max<size_t>(1, size_t(p.n_cov)) * 16);
     p.select_bytes = lb_select_temp_bytes(uint32_t(N));
     p.select_temp.alloc(p.select_bytes);
     for (DBuf *d : {&p.s_ka, &p.s_kb}) d->alloc(N);
@@ -315,7 +319,7 @@ void build(lb_plan &p) {
     bool recording = (p.reuse && b.gi_bounces > 1) || (p.keep_records && b.gi_bounces > 0);
     p.records.alloc(recording ? p.max_gathered * p.P.params.counts[2] * 8 : 16);
 
-    cudaStream_t st = p.g->stream;
+    mark("allocations");
     auto up = [&](DBuf &d, const void *src, size_t bytes) {
         if (bytes) {
             ck(cudaMemcpyAsync(d.p, src, bytes, cudaMemcpyHostToDevice, st), "upload");
@@ -323,10 +327,6 @@ void build(lb_plan &p) {
         }
     };
     up(p.theta0, theta.data(), theta.size() * 4);
-    up(p.tiles_d, p.tiles_all.data(), p.tiles_all.size() * sizeof(DTile));
-    up(p.tex, tex.data(), tex.size() * 64);
-    up(p.cov_idx, cov_idx.data(), cov_idx.size() * 4);
-    up(p.cov_k, cov_k.data(), cov_k.size() * 4);
     up(p.known, known.data(), known.size());
     up(p.state, state.data(), state.size());
     up(p.field, field.data(), field.size() * 4);

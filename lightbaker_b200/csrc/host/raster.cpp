@@ -38,6 +38,66 @@ Vec2 nearest(Vec2 p, Vec2 a, Vec2 b, Vec2 c) {
 }
 }  // namespace
 
+namespace {
+// raster.rs:48-67: one chart triangle's set-up; false for a degenerate one
+struct Setup {
+    Vec2 ua, ub, uc;
+    float det;
+    Vec3 pa, pb, pc, n, dx, dy;
+    int32_t x0, y0, x1, y1;
+    void bary(Vec2 q, float &l1, float &l2, float &l3) const {
+        l1 = ((ub.y - uc.y) * (q.x - uc.x) + (uc.x - ub.x) * (q.y - uc.y)) / det;
+        l2 = ((uc.y - ua.y) * (q.x - uc.x) + (ua.x - uc.x) * (q.y - uc.y)) / det;
+        l3 = 1.0f - l1 - l2;
+    }
+    Vec3 at(Vec2 q) const {
+        float l1, l2, l3;
+        bary(q, l1, l2, l3);
+        return (pa * l1 + pb * l2) + pc * l3;
+    }
+};
+bool setup(const Layout &layout, const Chart &c, const std::vector<Vec3> &pos, size_t t, int32_t w, int32_t h,
+           Setup &s) {
+    s.pa = pos[t * 3];
+    s.pb = pos[t * 3 + 1];
+    s.pc = pos[t * 3 + 2];
+    s.ua = c.local(s.pa, layout.density, layout.padding);
+    s.ub = c.local(s.pb, layout.density, layout.padding);
+    s.uc = c.local(s.pc, layout.density, layout.padding);
+    s.det = (s.ub.y - s.uc.y) * (s.ua.x - s.uc.x) + (s.uc.x - s.ub.x) * (s.ua.y - s.uc.y);
+    if (std::fabs(s.det) < 1e-12f) return false;
+    s.n = face_normal(pos, t);
+    Vec3 o = s.at(Vec2(0, 0));
+    s.dx = s.at(Vec2(1, 0)) - o;
+    s.dy = s.at(Vec2(0, 1)) - o;
+    Vec2 lo = s.ua.min(s.ub).min(s.uc).floor().max(Vec2(0, 0));
+    Vec2 hi = s.ua.max(s.ub).max(s.uc).ceil().min(Vec2(float(w - 1), float(h - 1)));
+    s.x0 = as_i32(lo.x);
+    s.y0 = as_i32(lo.y);
+    s.x1 = as_i32(hi.x);
+    s.y1 = as_i32(hi.y);
+    return true;
+}
+}  // namespace
+
+std::vector<RasterTri> raster_triangles(const Scene &scene, const Layout &layout, const Tile &tile,
+                                        uint32_t tile_index) {
+    std::vector<RasterTri> out;
+    for (uint32_t ci : tile.charts) {
+        const Chart &c = layout.charts[ci];
+        const std::vector<Vec3> &pos = scene.positions[c.mesh];
+        for (uint32_t tt : c.tris) {
+            Setup s;
+            if (!setup(layout, c, pos, tt, int32_t(tile.w), int32_t(tile.h), s)) continue;
+            out.push_back(RasterTri{{s.ua.x, s.ua.y}, {s.ub.x, s.ub.y}, {s.uc.x, s.uc.y}, s.det,
+                                    {s.pa.x, s.pa.y, s.pa.z}, {s.pb.x, s.pb.y, s.pb.z}, {s.pc.x, s.pc.y, s.pc.z},
+                                    {s.n.x, s.n.y, s.n.z}, {s.dx.x, s.dx.y, s.dx.z}, {s.dy.x, s.dy.y, s.dy.z},
+                                    s.x0, s.y0, s.x1, s.y1, ci, tile_index, 0});
+        }
+    }
+    return out;
+}
+
 // raster.rs:39-100
 std::vector<lb_texel> rasterize(const Scene &scene, const Layout &layout, const Tile &tile) {
     int32_t w = int32_t(tile.w), h = int32_t(tile.h);
@@ -47,29 +107,13 @@ std::vector<lb_texel> rasterize(const Scene &scene, const Layout &layout, const 
             const Chart &c = layout.charts[ci];
             const std::vector<Vec3> &pos = scene.positions[c.mesh];
             for (uint32_t tt : c.tris) {
-                size_t t = tt;
-                Vec3 pa = pos[t * 3], pb = pos[t * 3 + 1], pc = pos[t * 3 + 2];
-                Vec2 ua = c.local(pa, layout.density, layout.padding), ub = c.local(pb, layout.density, layout.padding),
-                     uc = c.local(pc, layout.density, layout.padding);
-                float det = (ub.y - uc.y) * (ua.x - uc.x) + (uc.x - ub.x) * (ua.y - uc.y);
-                if (std::fabs(det) < 1e-12f) continue;
-                auto bary = [&](Vec2 q, float &l1, float &l2, float &l3) {
-                    l1 = ((ub.y - uc.y) * (q.x - uc.x) + (uc.x - ub.x) * (q.y - uc.y)) / det;
-                    l2 = ((uc.y - ua.y) * (q.x - uc.x) + (ua.x - uc.x) * (q.y - uc.y)) / det;
-                    l3 = 1.0f - l1 - l2;
-                };
-                auto at = [&](Vec2 q) {
-                    float l1, l2, l3;
-                    bary(q, l1, l2, l3);
-                    return (pa * l1 + pb * l2) + pc * l3;
-                };
-                Vec3 n = face_normal(pos, t);
-                Vec3 o = at(Vec2(0, 0));
-                Vec3 dx = at(Vec2(1, 0)) - o, dy = at(Vec2(0, 1)) - o;
-                Vec2 lo = ua.min(ub).min(uc).floor().max(Vec2(0, 0));
-                Vec2 hi = ua.max(ub).max(uc).ceil().min(Vec2(float(w - 1), float(h - 1)));
-                for (int32_t y = as_i32(lo.y); y <= as_i32(hi.y); y++)
-                    for (int32_t x = as_i32(lo.x); x <= as_i32(hi.x); x++) {
+                Setup s;
+                if (!setup(layout, c, pos, tt, w, h, s)) continue;
+                const Vec2 ua = s.ua, ub = s.ub, uc = s.uc;
+                const Vec3 pa = s.pa, pb = s.pb, pc = s.pc, n = s.n, dx = s.dx, dy = s.dy;
+                auto bary = [&](Vec2 q, float &l1, float &l2, float &l3) { s.bary(q, l1, l2, l3); };
+                for (int32_t y = s.y0; y <= s.y1; y++)
+                    for (int32_t x = s.x0; x <= s.x1; x++) {
                         Vec2 centre(float(x) + 0.5f, float(y) + 0.5f);
                         size_t i = size_t(y) * size_t(w) + size_t(x);
                         if (covered(out[i])) continue;

@@ -4,6 +4,8 @@
 
 #include <cstdint>
 
+#include "host/raster.h"
+
 // A tile in the device's texel arrays: its rectangle in the atlas and its first texel.
 struct DTile {
     uint32_t x, y, w, h;
@@ -66,3 +68,17 @@ cudaError_t lb_fallback(const PostArgs &a, const float4 *probes, float3 origin, 
 cudaError_t lb_composite(const CompositeArgs &c, float4 *scratch, uint8_t *has_b, cudaStream_t st);
 // the composite's block averages alone, before its dilations
 cudaError_t lb_composite_blocks(const CompositeArgs &c, cudaStream_t st);
+
+// The device rasteriser (raster.cu; raster.rs:39-114): the dirty tiles' texels (n_texels, the tiles in
+// `tiles`, concatenated) from their triangles (RasterTri, in the host rasteriser's order), written into
+// `tex` (64 bytes a texel, zero where uncovered); `scratch` holds n_texels claims; *pairs gets the number
+// of (ds x ds block, chart) pairs over the covered texels (a bound on the gathered texels).
+cudaError_t lb_raster_tiles(const RasterTri *tris, uint32_t n_tris, const DTile *tiles, uint32_t n_tiles,
+                            uint32_t n_texels, uint32_t ds, float4 *tex, uint32_t *scratch,
+                            unsigned long long *pairs, int sms, cudaStream_t st);
+// The covered texels' indices in order (idx, *count) and each texel's place among them (inverse;
+// 0xffffffff where not covered); temp: lb_raster_covered_temp(n_texels) bytes.
+size_t lb_raster_covered_temp(uint32_t n_texels);
+cudaError_t lb_raster_covered(const float4 *tex, uint32_t n_texels, void *temp, size_t temp_bytes, uint32_t *idx,
+                              uint32_t *count, uint32_t *inverse, int sms, cudaStream_t st);
+

@@ -332,4 +332,5 @@ def with_light(scene: bytes, albedo=None, zenith=None, horizon=None, ground=None
     return body + b"\0" * (pad(len(body)) - len(body)) + rest
 
 
-WORKLOADS = {"small_map": small_map, "map_100m": map_100m, "reference_test": reference_test}
+WORKLOADS = {"small_map": small_map, "map_100m": map_100m, "reference_test": reference_test,
+             "uneven_tiles": uneven_tiles, "stress_map": stress_map}

@@ -96,3 +96,22 @@ def test_device_bake_cache(gpu):
             shutil.rmtree(d2, ignore_errors=True)
     finally:
         shutil.rmtree(d, ignore_errors=True)
+
+
+@pytest.mark.parametrize("name", ["reference_test", "small_map", "map_100m"])
+def test_device_raster_equals_host(gpu, name):
+    """The device bake rasterises its tiles on the GPU (raster.cu): every texel record, covered or not,
+    equals the host rasteriser's (raster.rs:39-114) bit for bit, tile after tile in the plan's order."""
+    scene = scenes.WORKLOADS[name]()
+    P = lb.prepare(scene)
+    tr = lb.Transport(scene, gpu)
+    try:
+        dev = tr.export("texels").reshape(-1, 16).view(np.uint32)
+    finally:
+        tr.close()
+    host = np.concatenate([P.rasterize(t).reshape(-1) for t in range(len(P.tiles))])
+    host = host.view(np.float32).reshape(-1, 16).view(np.uint32)
+    assert dev.shape == host.shape
+    bad = np.nonzero((dev != host).any(axis=1))[0]
+    assert len(bad) == 0, f"{len(bad)} of {len(host)} texels differ, first {bad[:5]}"
+    assert (host.view(np.float32)[:, 3] > 0.5).sum() > 0
