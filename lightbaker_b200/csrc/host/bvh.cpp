@@ -14,8 +14,13 @@ namespace {
 constexpr size_t BINS = 16;  // bvh.rs:9
 constexpr size_t LEAF = 4;   // bvh.rs:10
 
+// A primitive as the build moves it (40 bytes: the passes over a node's primitives and the partition's
+// swaps touch only these); its triangle record and source are kept apart, by id.
 struct Prim {
     Vec3 min, max, centre;
+    uint32_t id;
+};
+struct Source {
     lb_tri tri;
     uint32_t mesh, index;  // where its vertices are in the scene
 };
@@ -35,6 +40,7 @@ float area(Vec3 mn, Vec3 mx) {
 // contiguous run of the primitives, and the runs' results are merged in run order: fmin and fmax keep
 // the first of equal values (so of -0 and +0 too), so the merge gives the serial fold's bits.
 constexpr size_t PARALLEL_BINS = 1 << 15;
+constexpr int MAX_PARTS = 64;  // runs a node's gathering is split into at most
 
 // the contiguous run [lo, hi) of n items that part k of parts takes
 inline void run_of(size_t n, int k, int parts, size_t &lo, size_t &hi) {
@@ -45,9 +51,14 @@ inline void run_of(size_t n, int k, int parts, size_t &lo, size_t &hi) {
 // bvh.rs:119-151: the axis and plane of the cheapest binned split, if one beats a leaf
 bool best_split(const Prim *p, size_t n, int &axis_out, float &at_out) {
     Vec3 cmin = Vec3::splat(INFINITY), cmax = Vec3::splat(-INFINITY), pmin = cmin, pmax = cmax;
-    const int parts = n >= PARALLEL_BINS ? std::max(1, std::min(omp_get_max_threads(), 64)) : 1;
+    const int parts = n >= PARALLEL_BINS ? std::max(1, std::min(omp_get_max_threads(), MAX_PARTS)) : 1;
     {
-        std::vector<Vec3> a(parts, Vec3::splat(INFINITY)), b(parts, Vec3::splat(-INFINITY)), c = a, d = b;
+        // fixed arrays: this runs once for every node of the tree, most of them small
+        Vec3 a[MAX_PARTS], b[MAX_PARTS], c[MAX_PARTS], d[MAX_PARTS];
+        for (int k = 0; k < parts; k++) {
+            a[k] = c[k] = Vec3::splat(INFINITY);
+            b[k] = d[k] = Vec3::splat(-INFINITY);
+        }
 #pragma omp parallel for schedule(static, 1) if (parts > 1)
         for (int k = 0; k < parts; k++) {
             size_t lo, hi;
@@ -76,8 +87,13 @@ bool best_split(const Prim *p, size_t n, int &axis_out, float &at_out) {
             bmax[b] = Vec3::splat(-INFINITY);
             bn[b] = 0;
         }
-        std::vector<Vec3> tmin(size_t(parts) * BINS, Vec3::splat(INFINITY)), tmax(size_t(parts) * BINS, Vec3::splat(-INFINITY));
-        std::vector<uint32_t> tn(size_t(parts) * BINS, 0);
+        Vec3 tmin[MAX_PARTS * BINS], tmax[MAX_PARTS * BINS];
+        uint32_t tn[MAX_PARTS * BINS];
+        for (size_t q = 0; q < size_t(parts) * BINS; q++) {
+            tmin[q] = Vec3::splat(INFINITY);
+            tmax[q] = Vec3::splat(-INFINITY);
+            tn[q] = 0;
+        }
 #pragma omp parallel for schedule(static, 1) if (parts > 1)
         for (int k = 0; k < parts; k++) {
             size_t lo, hi;
@@ -178,6 +194,7 @@ void build_subtree(std::vector<Prim> &prims, size_t start0, size_t end0, std::ve
 // bvh.rs:50-106
 Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)> &chart) {
     std::vector<Prim> prims;
+    std::vector<Source> sources;
     for (size_t mi = 0; mi < scene.header.meshes.size(); mi++) {
         const MeshInfo &m = scene.header.meshes[mi];
         if (!scene.header.materials[m.material].casts) continue;
@@ -190,9 +207,10 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
             q.min = a.min(b).min(c);
             q.max = a.max(b).max(c);
             q.centre = (a + b + c) / 3.0f;
-            q.tri = lb_tri{{a.x, a.y, a.z, u2f(m.material)}, {e1.x, e1.y, e1.z, u2f(chart(mi, t))}, {e2.x, e2.y, e2.z, 0.0f}};
-            q.mesh = uint32_t(mi);
-            q.index = uint32_t(t);
+            q.id = uint32_t(sources.size());
+            sources.push_back(Source{lb_tri{{a.x, a.y, a.z, u2f(m.material)}, {e1.x, e1.y, e1.z, u2f(chart(mi, t))},
+                                            {e2.x, e2.y, e2.z, 0.0f}},
+                                     uint32_t(mi), uint32_t(t)});
             prims.push_back(q);
         }
     }
@@ -293,12 +311,13 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
         }
     }
     out.tris.reserve(prims.size());
-    for (auto &p : prims) out.tris.push_back(p.tri);
+    for (auto &p : prims) out.tris.push_back(sources[p.id].tri);
     out.verts.resize(prims.size() * 9);
     for (size_t i = 0; i < prims.size(); i++) {
-        const std::vector<Vec3> &p = scene.positions[prims[i].mesh];
+        const Source &src = sources[prims[i].id];
+        const std::vector<Vec3> &p = scene.positions[src.mesh];
         for (int k = 0; k < 3; k++) {
-            Vec3 v = p[size_t(prims[i].index) * 3 + k];
+            Vec3 v = p[size_t(src.index) * 3 + k];
             out.verts[i * 9 + k * 3] = v.x;
             out.verts[i * 9 + k * 3 + 1] = v.y;
             out.verts[i * 9 + k * 3 + 2] = v.z;

@@ -7,6 +7,12 @@
 
 namespace lb {
 
+// std::fmin / std::fmax as the C library computes them (the non-NaN argument when one is NaN, the first
+// of two equal values, so +0 or -0 as given), written out so that the compiler inlines them: the BVH
+// build and the layout call them for every primitive of every node.
+inline float fmin_(float a, float b) { return (b < a || a != a) ? b : a; }
+inline float fmax_(float a, float b) { return (b > a || a != a) ? b : a; }
+
 struct Vec2 {
     float x = 0, y = 0;
     Vec2() = default;
@@ -18,8 +24,8 @@ struct Vec2 {
     float perp_dot(Vec2 o) const { return x * o.y - y * o.x; }
     float length_squared() const { return dot(*this); }
     float distance_squared(Vec2 o) const { return (*this - o).length_squared(); }
-    Vec2 min(Vec2 o) const { return {std::fmin(x, o.x), std::fmin(y, o.y)}; }
-    Vec2 max(Vec2 o) const { return {std::fmax(x, o.x), std::fmax(y, o.y)}; }
+    Vec2 min(Vec2 o) const { return {fmin_(x, o.x), fmin_(y, o.y)}; }
+    Vec2 max(Vec2 o) const { return {fmax_(x, o.x), fmax_(y, o.y)}; }
     Vec2 floor() const { return {std::floor(x), std::floor(y)}; }
     Vec2 ceil() const { return {std::ceil(x), std::ceil(y)}; }
 };
@@ -57,8 +63,8 @@ struct Vec3 {
         }
         return false;
     }
-    Vec3 min(Vec3 o) const { return {std::fmin(x, o.x), std::fmin(y, o.y), std::fmin(z, o.z)}; }
-    Vec3 max(Vec3 o) const { return {std::fmax(x, o.x), std::fmax(y, o.y), std::fmax(z, o.z)}; }
+    Vec3 min(Vec3 o) const { return {fmin_(x, o.x), fmin_(y, o.y), fmin_(z, o.z)}; }
+    Vec3 max(Vec3 o) const { return {fmax_(x, o.x), fmax_(y, o.y), fmax_(z, o.z)}; }
 };
 
 inline uint32_t f2u(float f) {
