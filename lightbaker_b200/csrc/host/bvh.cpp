@@ -237,7 +237,7 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
         int left = -1, right = -1;
         size_t task_id = 0;
     };
-    const size_t cut = std::max<size_t>(2048, prims.size() / 256);
+    const size_t cut = std::max<size_t>(2048, prims.size() / 32);
     std::vector<Top> top;
     std::vector<std::pair<size_t, size_t>> tasks;
     top.push_back(Top{0, prims.size()});
