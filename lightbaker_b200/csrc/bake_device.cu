@@ -198,17 +198,17 @@ void build(lb_plan &p) {
     p.n_cov = p.n_dirty_texels ? uint32_t(counts[1] & 0xffffffffu) : 0;
     mark("raster");
 
-    // cached tiles' light, the atlas owner map and the atlas the first bounce reads
-    std::vector<uint8_t> known(p.n_all, 0), state(p.n_all, 0);
-    std::vector<float> field(p.n_all, 0.0f), ao(p.n_all, 0.0f);
-    std::vector<float> dl(size_t(p.n_all) * 4, 0.0f), ind(size_t(p.n_all) * 4, 0.0f);
-    std::vector<uint32_t> owner(size_t(p.aw) * p.ah, 0xffffffffu);
-    std::vector<float> light(size_t(p.aw) * p.ah * 4, 0.0f);
+    // cached tiles' light and the atlas the first bounce reads (all zero when no tile comes from the cache:
+    // then cleared on the device instead); the atlas owner map is built on the device
+    const bool any_cached = p.dirty.size() < p.order.size();
+    const size_t n_cached = any_cached ? p.n_all : 0, n_atlas = any_cached ? size_t(p.aw) * p.ah : 0;
+    std::vector<uint8_t> known(n_cached, 0), state(n_cached, 0);
+    std::vector<float> field(n_cached, 0.0f), ao(n_cached, 0.0f);
+    std::vector<float> dl(n_cached * 4, 0.0f), ind(n_cached * 4, 0.0f);
+    std::vector<float> light(n_atlas * 4, 0.0f);
     for (size_t k = 0; k < p.order.size(); k++) {
         size_t ti = p.order[k];
         const DTile &t = p.tiles_all[k];
-        for (uint32_t y = 0; y < t.h; y++)
-            for (uint32_t x = 0; x < t.w; x++) owner[size_t(t.y + y) * p.aw + t.x + x] = t.off + y * t.w + x;
         if (!p.lights[ti]) continue;
         const lb::TileLight &l = *p.lights[ti];
         for (uint32_t i = 0; i < t.w * t.h; i++) {
@@ -300,7 +300,7 @@ void build(lb_plan &p) {
     p.probe_slot.alloc(std::max<size_t>(1, probe_slot.size()) * 4);
     p.pk_a.alloc(NP);
     p.pk_b.alloc(NP);
-    p.owner.alloc(owner.size() * 4);
+    p.owner.alloc(size_t(p.aw) * p.ah * 4);
     p.direct_atlas.alloc(size_t(p.aw) * p.ah * 8);
     p.validity.alloc(size_t(p.aw) * p.ah);
     p.indirect.alloc(size_t(p.iw) * p.ih * 16);
@@ -327,14 +327,23 @@ void build(lb_plan &p) {
         }
     };
     up(p.theta0, theta.data(), theta.size() * 4);
-    up(p.known, known.data(), known.size());
-    up(p.state, state.data(), state.size());
-    up(p.field, field.data(), field.size() * 4);
-    up(p.ao, ao.data(), ao.size() * 4);
-    up(p.dl, dl.data(), dl.size() * 4);
-    up(p.ind, ind.data(), ind.size() * 4);
-    up(p.owner, owner.data(), owner.size() * 4);
-    up(p.light, light.data(), light.size() * 4);
+    if (any_cached) {
+        up(p.known, known.data(), known.size());
+        up(p.state, state.data(), state.size());
+        up(p.field, field.data(), field.size() * 4);
+        up(p.ao, ao.data(), ao.size() * 4);
+        up(p.dl, dl.data(), dl.size() * 4);
+        up(p.ind, ind.data(), ind.size() * 4);
+        up(p.light, light.data(), light.size() * 4);
+    } else {
+        for (auto *d : {&p.known, &p.state}) ck(cudaMemsetAsync(d->p, 0, p.n_all, st), "clear");
+        for (auto *d : {&p.field, &p.ao}) ck(cudaMemsetAsync(d->p, 0, size_t(p.n_all) * 4, st), "clear");
+        for (auto *d : {&p.dl, &p.ind}) ck(cudaMemsetAsync(d->p, 0, size_t(p.n_all) * 16, st), "clear");
+        ck(cudaMemsetAsync(p.light.p, 0, size_t(p.aw) * p.ah * 16, st), "clear");
+    }
+    ck(lb_owner_map(p.tiles_d.as<DTile>(), uint32_t(p.tiles_all.size()), p.aw, p.ah, p.owner.as<uint32_t>(), p.g->sms,
+                    st),
+       "owner map");
     up(p.w1, w1.data(), w1.size() * 4);
     up(p.wr, wr.data(), wr.size() * 4);
     up(p.probes_init, probes_init.data(), probes_init.size() * 4);

@@ -81,4 +81,8 @@ cudaError_t lb_raster_tiles(const RasterTri *tris, uint32_t n_tris, const DTile 
 size_t lb_raster_covered_temp(uint32_t n_texels);
 cudaError_t lb_raster_covered(const float4 *tex, uint32_t n_texels, void *temp, size_t temp_bytes, uint32_t *idx,
                               uint32_t *count, uint32_t *inverse, int sms, cudaStream_t st);
+// The atlas owner map (aw x ah): each texel of a tile gets its place in the concatenated texel arrays,
+// the rest 0xffffffff.
+cudaError_t lb_owner_map(const DTile *tiles, uint32_t n_tiles, uint32_t aw, uint32_t ah, uint32_t *owner, int sms,
+                         cudaStream_t st);
 

@@ -166,6 +166,17 @@ struct CoveredFlag {
     __device__ __forceinline__ uint8_t operator()(uint32_t i) const { return tex[4 * size_t(i)].w > 0.5f ? 1 : 0; }
 };
 
+// the atlas owner map: each tile texel's place in the concatenated texel arrays
+__global__ void k_owner(const DTile *tiles, uint32_t n_tiles, uint32_t aw, uint32_t *owner) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    for (uint32_t k = 0; k < n_tiles; k++) {
+        const DTile tl = tiles[k];
+        const uint32_t n = tl.w * tl.h;
+        for (uint32_t r = tid; r < n; r += stride)
+            owner[size_t(tl.y + r / tl.w) * aw + tl.x + r % tl.w] = tl.off + r;
+    }
+}
+
 int grid_for(uint32_t n, int sms, int per_sm = 8) {
     int g = int((n + 255u) / 256u);
     int cap = (sms > 0 ? sms : 148) * per_sm;
@@ -215,5 +226,15 @@ cudaError_t lb_raster_covered(const float4 *tex, uint32_t n_texels, void *temp, 
     e = cub::DeviceSelect::Flagged(temp, temp_bytes, it, flags, idx, count, int(n_texels), st);
     if (e != cudaSuccess) return e;
     k_inverse_index<<<grid_for(n_texels, sms), 256, 0, st>>>(idx, count, inverse);
+    return cudaGetLastError();
+}
+
+cudaError_t lb_owner_map(const DTile *tiles, uint32_t n_tiles, uint32_t aw, uint32_t ah, uint32_t *owner, int sms,
+                         cudaStream_t st) {
+    using namespace lbd;
+    const uint32_t n = aw * ah;
+    if (n == 0) return cudaSuccess;
+    k_fill_u32<<<grid_for(n, sms), 256, 0, st>>>(owner, n, NOBODY);
+    if (n_tiles) k_owner<<<grid_for(n, sms), 256, 0, st>>>(tiles, n_tiles, aw, owner);
     return cudaGetLastError();
 }
