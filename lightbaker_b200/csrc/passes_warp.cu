@@ -154,9 +154,10 @@ template <int BVH, bool COUNT, int OCC = 1, int WALK = 0, bool WT = false>
 __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
                                                    unsigned long long *counters, int group, int refill, int near) {
+    // each occlusion ray's term by ray index (0 for a miss: adding it to the sum changes no bit, as the sum
+    // starts at +0 and every term is >= 0); before the rays, the ball query's scratch
     __shared__ float s_term[WARPS][AO_CAP];
-    __shared__ uint8_t s_hit[WARPS][AO_CAP];
-    __shared__ uint32_t s_front[WARPS][2][BALL_FRONT];
+    static_assert(sizeof(s_term[0]) >= 2 * BALL_FRONT * sizeof(uint32_t), "the ball query's scratch fits");
     __shared__ uint32_t s_list[WARPS][BALL_LEAVES];
     __shared__ float s_dist[WARPS][BALL_LEAVES];
     const int lane = threadIdx.x & 31;
@@ -196,7 +197,8 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
             for (uint32_t q = 1u; q <= 9u; q++) far_ = fmaxf(far_, sqrtf(dot3(sub(add(candidate(q), lift), c0),
                                                                               sub(add(candidate(q), lift), c0))));
             rball = P.reach[0] + far_ * 1.001f + 1e-5f;
-            nl = ball_leaves<COUNT>(S, c0, rball, nrm, s_front[wi][0], s_front[wi][1], s_list[wi], s_dist[wi], lane, c);
+            uint32_t *scratch = reinterpret_cast<uint32_t *>(&s_term[wi][0]);
+            nl = ball_leaves<COUNT>(S, c0, rball, nrm, scratch, scratch + BALL_FRONT, s_list[wi], s_dist[wi], lane, c);
         }
         const float front = -(rball * 1e-3f + 1e-4f) * 0.5f;
         auto listed_from = [&](float3 o, float &shift) -> bool {
@@ -272,9 +274,11 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
         if (pick != 0u && !listed_from(o, ao_shift)) {
             ao_shift = 0.0f;
             nl = -1;
-            if (listed)
-                nl = ball_leaves<COUNT>(S, o, P.reach[0], nrm, s_front[w][0], s_front[w][1], s_list[w], s_dist[w], lane,
+            if (listed) {
+                uint32_t *scratch = reinterpret_cast<uint32_t *>(&s_term[w][0]);
+                nl = ball_leaves<COUNT>(S, o, P.reach[0], nrm, scratch, scratch + BALL_FRONT, s_list[w], s_dist[w], lane,
                                         c);
+            }
         }
         if (pick == 0u) listed_from(o, ao_shift);
         if (nl >= 0) {
@@ -293,7 +297,6 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
                         if (h.back && h.t < P.ground[3]) myback++;
                     }
                     s_term[w][r] = term;
-                    s_hit[w][r] = hit;
                 }
             }
             for (int ofs = 16; ofs > 0; ofs >>= 1) myback += __shfl_down_sync(FULL, myback, ofs);
@@ -301,7 +304,7 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
             __syncwarp();
             for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
                 uint32_t rr = r0 + uint32_t(lane);
-                occ = ordered_add(occ, rr < rays ? s_term[w][rr] : 0.0f, rr < rays && s_hit[w][rr]);
+                occ = ordered_add(occ, rr < rays ? s_term[w][rr] : 0.0f, rr < rays);
             }
             __syncwarp();
         } else if (BVH == 2 && WALK == 2 && refill && rays <= AO_CAP) {
@@ -326,7 +329,6 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
                         if (wk.hit.back && wk.hit.t < P.ground[3]) myback++;
                     }
                     s_term[w][r] = term;
-                    s_hit[w][r] = hit;
                 }
                 unsigned fm = __ballot_sync(FULL, fin);
                 if (fin) {
@@ -346,7 +348,7 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
             __syncwarp();
             for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
                 uint32_t rr = r0 + uint32_t(lane);
-                occ = ordered_add(occ, rr < rays ? s_term[w][rr] : 0.0f, rr < rays && s_hit[w][rr]);
+                occ = ordered_add(occ, rr < rays ? s_term[w][rr] : 0.0f, rr < rays);
             }
             __syncwarp();
         } else
@@ -366,7 +368,6 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
             }
             if (ord.grouped) {
                 s_term[w][r] = term;
-                s_hit[w][r] = hit;
             } else {
                 occ = ordered_add(occ, term, hit);
             }
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
         }
         if (nl < 0 && !(BVH == 2 && WALK == 2 && refill && rays <= AO_CAP) && ord.grouped) {
             __syncwarp();
-            for (uint32_t r0 = 0; r0 < rays; r0 += 32) occ = ordered_add(occ, s_term[w][r0 + lane], s_hit[w][r0 + lane]);
+            for (uint32_t r0 = 0; r0 < rays; r0 += 32) occ = ordered_add(occ, s_term[w][r0 + lane], true);
             __syncwarp();
         }
         if (lane == 0)
