@@ -104,6 +104,12 @@ void lb_scene_free(lb_scene *scene);
  * edge. Hit/miss, faces and t then differ from the shader's only for rays through an edge or a vertex
  * (within 1e-4 in barycentric terms), grazing a triangle, or ending within rounding of 1e-4 or tmax. */
 int lb_scene_set_vertices(lb_gpu *gpu, lb_scene *scene, const float *verts, size_t n_tris);
+/* The scene's 8-wide BVH (lb_set_bvh 8), which lb_scene_upload builds on the device from the BVH2: node
+ * and triangle counts, and with non-NULL buffers the nodes (20 words each) and triangles (e2.w: the
+ * triangle's index in the uploaded array). Equal byte for byte to lb_bvh8_collapse of the same BVH2.
+ * No counterpart in the reference, whose walk uses the BVH2 only. */
+int lb_scene_get_bvh8(lb_gpu *gpu, const lb_scene *scene, uint32_t *nodes8, lb_tri *tris8, uint64_t *n_nodes8,
+                      uint64_t *n_tris8);
 
 /* One ray for lb_trace: origin, maximum distance, direction, and its key (the ray number the shader's
  * opacity coin reads, trace.wgsl:69-72). */
@@ -361,6 +367,10 @@ int lb_scene_encode(const char *header_json, const float *const *positions, cons
  * leaf, every box inside its parent's slot): LB_OK, its node count and depth; for tests and tools. */
 int lb_bvh8_check(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris, uint64_t *n_nodes8,
                   uint64_t *depth);
+/* The same collapse on the host: counts, and with non-NULL buffers the nodes and triangles, as
+ * lb_scene_get_bvh8 returns them; for tests of the device build. */
+int lb_bvh8_collapse(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris, uint32_t *nodes8,
+                     lb_tri *tris8, uint64_t *n_nodes8, uint64_t *n_tris8);
 /* blake3 of a byte string (the hash the cache is keyed by), 32 bytes. */
 void lb_blake3(const uint8_t *data, size_t len, uint8_t out[32]);
 /* encode.rs: RGB9E5 and BC4 blocks, for format tests. */

@@ -57,6 +57,18 @@ class SceneBuffers:
         v = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 9)
         N.check(N.lib().lb_scene_set_vertices(self._gpu.handle, self._h, N.ptr(v), len(v)), "lb_scene_set_vertices")
 
+    def bvh8(self) -> tuple[np.ndarray, np.ndarray]:
+        """The 8-wide BVH built on the device at upload (lb_scene_get_bvh8): nodes as (n, 20) uint32 words
+        and triangles as (m, 12) uint32 words (e2.w: the triangle's index in the uploaded array)."""
+        nn, nt = C.c_uint64(), C.c_uint64()
+        lib = N.lib()
+        N.check(lib.lb_scene_get_bvh8(self._gpu.handle, self._h, None, None, C.byref(nn), C.byref(nt)), "lb_scene_get_bvh8")
+        nodes = np.zeros((nn.value, 20), np.uint32)
+        tris = np.zeros((nt.value, 12), np.uint32)
+        N.check(lib.lb_scene_get_bvh8(self._gpu.handle, self._h, N.ptr(nodes), N.ptr(tris), None, None),
+                "lb_scene_get_bvh8")
+        return nodes, tris
+
     def close(self) -> None:
         if self._h:
             N.lib().lb_scene_free(self._h)
@@ -428,6 +440,21 @@ def encode_scene(header: dict, positions: list) -> bytes:
         return C.string_at(p, n.value)
     finally:
         N.lib().lb_free(p)
+
+
+def bvh8_collapse(nodes: np.ndarray, tris: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """The host's collapse of a BVH2 into the 8-wide BVH (lb_bvh8_collapse), in SceneBuffers.bvh8's form."""
+    nodes = np.ascontiguousarray(nodes)
+    tris = np.ascontiguousarray(tris)
+    nn, nt = C.c_uint64(), C.c_uint64()
+    lib = N.lib()
+    N.check(lib.lb_bvh8_collapse(N.ptr(nodes), len(nodes), N.ptr(tris), len(tris), None, None, C.byref(nn),
+                                 C.byref(nt)), "lb_bvh8_collapse")
+    n8 = np.zeros((nn.value, 20), np.uint32)
+    t8 = np.zeros((nt.value, 12), np.uint32)
+    N.check(lib.lb_bvh8_collapse(N.ptr(nodes), len(nodes), N.ptr(tris), len(tris), N.ptr(n8), N.ptr(t8), None, None),
+            "lb_bvh8_collapse")
+    return n8, t8
 
 
 def blake3(data: bytes) -> bytes:

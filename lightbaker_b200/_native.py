@@ -91,6 +91,8 @@ SIGNATURES = {
                                      C.c_size_t, C.c_void_p, C.c_size_t]),
     "lb_scene_free": (None, [C.c_void_p]),
     "lb_scene_set_vertices": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
+    "lb_scene_get_bvh8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64),
+                                    C.POINTER(C.c_uint64)]),
     "lb_trace": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_uint32, C.c_void_p]),
     "lb_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(Params), C.c_void_p, C.c_size_t, C.c_void_p,
                          C.c_size_t, C.c_void_p]),
@@ -157,6 +159,8 @@ SIGNATURES = {
                                   C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t)]),
     "lb_bvh8_check": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64),
                                 C.POINTER(C.c_uint64)]),
+    "lb_bvh8_collapse": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,
+                                   C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "lb_blake3": (None, [C.c_char_p, C.c_size_t, C.c_void_p]),
     "lb_rgb9e5": (C.c_uint32, [C.POINTER(C.c_float)]),
     "lb_rgb9e5_decode": (None, [C.c_uint32, C.POINTER(C.c_float)]),

@@ -380,6 +380,21 @@ int lb_bvh8_check(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size
         LB_EINVAL);
 }
 
+int lb_bvh8_collapse(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris, uint32_t *nodes8,
+                     lb_tri *tris8, uint64_t *n_nodes8, uint64_t *n_tris8) {
+    if (!nodes || !n_nodes || !tris) return LB_EINVAL;
+    return guard(
+        [&]() -> int {
+            lb::Bvh8 b = lb::Bvh8::collapse(nodes, n_nodes, tris, n_tris);
+            if (n_nodes8) *n_nodes8 = b.n_nodes();
+            if (n_tris8) *n_tris8 = b.tris.size();
+            if (nodes8) std::memcpy(nodes8, b.nodes.data(), b.nodes.size() * 4);
+            if (tris8) std::memcpy(tris8, b.tris.data(), b.tris.size() * sizeof(lb_tri));
+            return LB_OK;
+        },
+        LB_EINVAL);
+}
+
 void lb_blake3(const uint8_t *data, size_t len, uint8_t out[32]) { lb::blake3_hash(data, len, out); }
 uint32_t lb_rgb9e5(const float c[3]) { return lb::rgb9e5(c); }
 void lb_rgb9e5_decode(uint32_t p, float out[3]) { lb::rgb9e5_decode(p, out); }

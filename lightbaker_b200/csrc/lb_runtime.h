@@ -37,7 +37,7 @@ struct lb_scene {
     lb_gpu *gpu = nullptr;
     void *nodes = nullptr, *tris = nullptr, *mats = nullptr, *charts = nullptr;
     uint32_t n_nodes = 0, n_tris = 0, n_mats = 0, n_charts = 0;
-    void *nodes8 = nullptr, *tris8 = nullptr;  // the 8-wide BVH collapsed from the BVH2 (host/bvh8.h)
+    void *nodes8 = nullptr, *tris8 = nullptr;  // the 8-wide BVH collapsed from the BVH2 (bvh8_build.cu)
     uint32_t n_nodes8 = 0, n_tris8 = 0;
     void *verts = nullptr;  // exact vertices (lb_scene_set_vertices): the watertight triangle test
 };
@@ -50,6 +50,8 @@ struct Scene;
 lbd::Scene lb_scene_view(const lb_scene *s);
 int lb_cuda_fail(cudaError_t e, const char *what);
 int lb_buffer_reserve(lb_buffer &b, size_t bytes);
+// the scene's 8-wide BVH, built on the device from its BVH2 (bvh8_build.cu)
+int lb_bvh8_build(lb_gpu *g, lb_scene *s);
 void lb_buffer_free(lb_buffer &b);
 int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const float4 *items, uint32_t n, uint32_t base,
                   const float4 *light, uint32_t n_light, float4 *out);

@@ -11,8 +11,8 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
-#include "host/bvh8.h"
 #include "lb_device.cuh"
 #include "lb_kernels.h"
 #include "lb_runtime.h"
@@ -127,6 +127,13 @@ lb_scene *lb_scene_upload(lb_gpu *g, const lb_node *nodes, size_t n_nodes, const
         lb_set_error("lb_scene_upload: more than 2^31 nodes or triangles");
         return nullptr;
     }
+    // every leaf inside the triangle array (an inner node whose children lie past the node array is the
+    // reference's empty BVH: every walk and the 8-wide build treat it as having no children)
+    for (size_t i = 0; i < n_nodes; i++)
+        if (nodes[i].count > 0 && uint64_t(nodes[i].first) + nodes[i].count > n_tris) {
+            lb_set_error("lb_scene_upload: a BVH leaf reaches past the triangle array");
+            return nullptr;
+        }
     cudaSetDevice(g->device);
     lb_scene *s = new lb_scene();
     s->gpu = g;
@@ -158,24 +165,8 @@ lb_scene *lb_scene_upload(lb_gpu *g, const lb_node *nodes, size_t n_nodes, const
     s->n_tris = uint32_t(n_tris);
     s->n_mats = uint32_t(n_materials);
     s->n_charts = uint32_t(n_charts);
-    // the 8-wide BVH over the same triangles
-    try {
-        lb::Bvh8 b8 = lb::Bvh8::collapse(nodes, n_nodes, n_tris ? tris : &zero_tri, n_tris ? n_tris : 1);
-        size_t nb = b8.nodes.size() * 4, tb = b8.tris.size() * sizeof(lb_tri);
-        cudaError_t e = cudaMalloc(&s->nodes8, nb);
-        if (e == cudaSuccess) e = cudaMemcpy(s->nodes8, b8.nodes.data(), nb, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMalloc(&s->tris8, tb);
-        if (e == cudaSuccess) e = cudaMemcpy(s->tris8, b8.tris.data(), tb, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) {
-            lb_cuda_fail(e, "lb_scene_upload (8-wide BVH)");
-            lb_scene_free(s);
-            return nullptr;
-        }
-        g->h2d += nb + tb;
-        s->n_nodes8 = uint32_t(b8.n_nodes());
-        s->n_tris8 = uint32_t(b8.tris.size());
-    } catch (const std::exception &ex) {
-        lb_set_error(std::string("lb_scene_upload: ") + ex.what());
+    // the 8-wide BVH over the same triangles, collapsed on the device from the BVH2 just uploaded
+    if (lb_bvh8_build(g, s) != LB_OK) {
         lb_scene_free(s);
         return nullptr;
     }
@@ -229,6 +220,23 @@ int lb_scene_set_vertices(lb_gpu *g, lb_scene *s, const float *verts, size_t n_t
     }
     g->h2d += bytes;
     s->verts = p;
+    return LB_OK;
+}
+
+int lb_scene_get_bvh8(lb_gpu *g, const lb_scene *s, uint32_t *nodes8, lb_tri *tris8, uint64_t *n_nodes8,
+                      uint64_t *n_tris8) {
+    if (!g || !s || s->gpu != g || !s->nodes8 || !s->tris8) {
+        lb_set_error("lb_scene_get_bvh8: bad arguments");
+        return LB_EINVAL;
+    }
+    if (n_nodes8) *n_nodes8 = s->n_nodes8;
+    if (n_tris8) *n_tris8 = s->n_tris8;
+    LB_CUDA(cudaSetDevice(g->device), "cudaSetDevice");
+    LB_CUDA(cudaStreamSynchronize(g->stream), "lb_scene_get_bvh8");
+    const size_t nb = size_t(s->n_nodes8) * 80, tb = size_t(s->n_tris8) * sizeof(lb_tri);
+    if (nodes8) LB_CUDA(cudaMemcpy(nodes8, s->nodes8, nb, cudaMemcpyDeviceToHost), "lb_scene_get_bvh8");
+    if (tris8) LB_CUDA(cudaMemcpy(tris8, s->tris8, tb, cudaMemcpyDeviceToHost), "lb_scene_get_bvh8");
+    g->d2h += (nodes8 ? nb : 0) + (tris8 ? tb : 0);
     return LB_OK;
 }
 

@@ -73,3 +73,20 @@ def test_bvh8_empty_and_big_leaves():
     nodes[0]["min"], nodes[0]["max"] = v.min(0), v.max(0)
     nodes[0]["first"], nodes[0]["count"] = 0, 70
     N.check(N.lib().lb_bvh8_check(N.ptr(nodes), 1, N.ptr(tris), 70, None, None), "big leaf")
+
+
+@pytest.mark.parametrize("name", ["reference_test", "small_map"])
+def test_bvh8_collapse_export(name):
+    """lb_bvh8_collapse (the host collapse the device build is checked against): the node count of
+    lb_bvh8_check, every triangle once (e2.w a permutation of the BVH2's triangle indices, the triangle
+    otherwise unchanged), and the root's inner children numbered from 1."""
+    P = lb.prepare(scenes.WORKLOADS[name]())
+    n8 = C.c_uint64()
+    N.check(N.lib().lb_bvh8_check(N.ptr(P.nodes), len(P.nodes), N.ptr(P.tris), len(P.tris), C.byref(n8), None), "bvh8")
+    nodes, tris = lb.bvh8_collapse(P.nodes, P.tris)
+    assert len(nodes) == n8.value and len(tris) == len(P.tris)
+    orig = tris[:, 11]
+    assert np.array_equal(np.sort(orig), np.arange(len(P.tris)))
+    src = P.tris.view(np.uint32).reshape(-1, 12)[orig]
+    assert np.array_equal(tris[:, :11], src[:, :11])
+    assert nodes[0, 4] == 1 and (nodes[0, 3] >> 24) != 0
