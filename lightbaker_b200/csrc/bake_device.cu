@@ -686,7 +686,12 @@ lb_plan *lb_plan_create(lb_gpu *g, const uint8_t *scene, size_t len, const lb_ba
 
 int lb_plan_launch(lb_plan *p) {
     if (!p) return LB_EINVAL;
-    cudaError_t e = cudaGraphLaunch(p->exec, p->g->stream);
+    cudaError_t e = cudaSuccess;
+    for (cudaEvent_t &ev : p->ev)
+        if (!ev && e == cudaSuccess) e = cudaEventCreate(&ev);
+    if (e == cudaSuccess) e = cudaEventRecord(p->ev[0], p->g->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(p->exec, p->g->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(p->ev[1], p->g->stream);
     if (e != cudaSuccess) return lb_cuda_fail(e, "lb_plan_launch");
     return LB_OK;
 }
@@ -709,8 +714,11 @@ const char *lb_plan_tuning(const lb_plan *p) { return p ? p->tuned.c_str() : "";
 
 void lb_plan_free(lb_plan *p) {
     if (p) {
+        auto t0 = std::chrono::steady_clock::now();
         cudaStreamSynchronize(p->g->stream);
+        auto log = p->opt.log;
         delete p;
+        if (log) log("timing: plan freed in " + std::to_string(since(t0)) + " s");
     }
 }
 
@@ -722,20 +730,38 @@ const lb::Scene &lb_plan_scene(const lb_plan &p) { return p.scene; }
 lb::Bake lb_plan_collect(lb_plan &p) {
     const lb::SceneHeader &h = p.scene.header;
     auto t0 = std::chrono::steady_clock::now();
+    ck(cudaStreamSynchronize(p.g->stream), "bake");
+    const double t_wait = since(t0);
+    float graph_ms = 0.0f;
+    if (p.ev[0] && p.ev[1]) ck(cudaEventElapsedTime(&graph_ms, p.ev[0], p.ev[1]), "graph time");
     lb::Bake out;
     size_t A = size_t(p.aw) * p.ah;
-    std::vector<float> dir = down<float>(p, p.direct_atlas, A * 2);
-    std::vector<uint8_t> val = down<uint8_t>(p, p.validity, A);
-    std::vector<float> ind = down<float>(p, p.indirect, size_t(p.iw) * p.ih * 4);
-    std::vector<float> probes;
-    if (p.has_volume) probes = down<float>(p, p.probes, size_t(p.n_probes) * 16);
+    // the atlases and probes through the handle's pinned staging buffer (kept between bakes)
+    const size_t n_ind = size_t(p.iw) * p.ih, n_pr = p.has_volume ? size_t(p.n_probes) * 16 : 0;
+    auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t o_val = up(A * 8), o_ind = o_val + up(A), o_pr = o_ind + up(n_ind * 16), total = o_pr + n_pr * 4;
+    if (lb_host_stage_reserve(p.g, total) != LB_OK) throw std::runtime_error(lb_last_error());
+    char *stage = (char *)p.g->stage;
+    auto fetch = [&](size_t off, const DBuf &d, size_t bytes) {
+        if (!bytes) return;
+        ck(cudaMemcpyAsync(stage + off, d.p, bytes, cudaMemcpyDeviceToHost, p.g->stream), "download");
+        p.g->d2h += bytes;
+    };
+    fetch(0, p.direct_atlas, A * 8);
+    fetch(o_val, p.validity, A);
+    fetch(o_ind, p.indirect, n_ind * 16);
+    if (p.has_volume) fetch(o_pr, p.probes, n_pr * 4);
     uint64_t rays[3];
     if (lb_plan_rays(&p, rays) != LB_OK) throw std::runtime_error(lb_last_error());
+    const double t_down = since(t0);
+    const float *ind = (const float *)(stage + o_ind), *probes = (const float *)(stage + o_pr);
     out.direct.resize(A);
-    std::memcpy(out.direct.data(), dir.data(), A * 8);
-    out.validity = std::move(val);
-    out.indirect.resize(size_t(p.iw) * p.ih);
-    for (size_t i = 0; i < out.indirect.size(); i++) out.indirect[i] = {ind[i * 4], ind[i * 4 + 1], ind[i * 4 + 2]};
+    std::memcpy(out.direct.data(), stage, A * 8);
+    out.validity.assign((const uint8_t *)stage + o_val, (const uint8_t *)stage + o_val + A);
+    out.indirect.resize(n_ind);
+    auto *oi = out.indirect.data();
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)n_ind; i++) oi[i] = {ind[i * 4], ind[i * 4 + 1], ind[i * 4 + 2]};
     out.iw = p.iw;
     out.ih = p.ih;
     if (p.has_volume) {
@@ -744,7 +770,7 @@ lb::Bake lb_plan_collect(lb_plan &p) {
         v.step = h.volume->step;
         v.size = p.vsize;
         v.probes.resize(p.n_probes);
-        std::memcpy(v.probes.data(), probes.data(), probes.size() * 4);
+        std::memcpy(v.probes.data(), probes, n_pr * 4);
         v.chunks = p.n_chunks;
         v.chunks_baked = p.chunk_keys.size();
         out.volume = std::move(v);
@@ -794,5 +820,9 @@ lb::Bake lb_plan_collect(lb_plan &p) {
     s.rays_volume = rays[2];
     s.t_layout = p.t_prepare;
     s.t_composite = since(t0);
+    if (p.opt.log)
+        p.opt.log("timing of the collection, cumulative: device " + std::to_string(t_wait) + " s (graph " +
+                  std::to_string(graph_ms * 1e-3) + " s on the device); downloads " +
+                  std::to_string(t_down) + " s; results and cache " + std::to_string(s.t_composite) + " s");
     return out;
 }

@@ -30,6 +30,8 @@ struct lb_gpu {
     lb_counters last = {};
     uint64_t h2d = 0, d2h = 0;  // bytes copied by this handle
     lb_buffer items, out, light, scratch;
+    void *stage = nullptr;  // pinned host memory for downloads (lb_host_stage_reserve), kept between calls
+    size_t stage_cap = 0;
 };
 
 // The scene's buffers (gpu/mod.rs:65-71).
@@ -50,6 +52,7 @@ struct Scene;
 lbd::Scene lb_scene_view(const lb_scene *s);
 int lb_cuda_fail(cudaError_t e, const char *what);
 int lb_buffer_reserve(lb_buffer &b, size_t bytes);
+int lb_host_stage_reserve(lb_gpu *g, size_t bytes);
 // the scene's 8-wide BVH, built on the device from its BVH2 (bvh8_build.cu)
 int lb_bvh8_build(lb_gpu *g, lb_scene *s);
 void lb_buffer_free(lb_buffer &b);

@@ -103,9 +103,12 @@ struct lb_plan {
     std::string build_phases;  // the host build's phases, seconds since its start
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};  // around the last lb_plan_launch: the graph's device time
     double t_prepare = 0;
     lb::Stats stats;
     ~lb_plan() {
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (dscene) lb_scene_free(dscene);

@@ -49,6 +49,23 @@ int lb_buffer_reserve(lb_buffer &b, size_t bytes) {
     return LB_OK;
 }
 
+int lb_host_stage_reserve(lb_gpu *g, size_t bytes) {
+    if (bytes <= g->stage_cap) return LB_OK;
+    cudaError_t e = cudaStreamSynchronize(g->stream);  // no copy into the old buffer is in flight
+    if (e != cudaSuccess) return lb_cuda_fail(e, "lb_host_stage_reserve");
+    if (g->stage) cudaFreeHost(g->stage);
+    g->stage = nullptr;
+    g->stage_cap = 0;
+    size_t want = bytes + bytes / 4;
+    e = cudaHostAlloc(&g->stage, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        g->stage = nullptr;
+        return lb_cuda_fail(e, "cudaHostAlloc");
+    }
+    g->stage_cap = want;
+    return LB_OK;
+}
+
 void lb_buffer_free(lb_buffer &b) {
     if (b.ptr) cudaFree(b.ptr);
     b.ptr = nullptr;
@@ -113,6 +130,7 @@ void lb_gpu_close(lb_gpu *g) {
     lb_buffer_free(g->scratch);
     if (g->counters) cudaFree(g->counters);
     if (g->host_counters) cudaFreeHost(g->host_counters);
+    if (g->stage) cudaFreeHost(g->stage);
     cudaStreamDestroy(g->stream);
     delete g;
 }
