@@ -80,12 +80,18 @@ PostArgs lb_plan_post_args(lb_plan &p) {
 
 namespace {
 
+// full occupancy for the kernel the pass launches with the plan's shape (walk, BVH, register cap)
 int warp_blocks(const lb_plan &p, int pass) {
     lbd::Scene S = lb_scene_view(p.dscene);
     WarpPass w{};
     w.S = &S;
     w.pass = pass;
     w.sms = p.g->sms;
+    const bool direct = pass == LB_PASS_DIRECT;
+    w.bvh = direct ? p.bvh_direct : p.bvh_gather;
+    w.refill = direct ? p.refill_direct : p.refill_gather;
+    w.near = direct ? p.near_direct : p.near_gather;
+    w.occ = direct ? p.occ_direct : p.occ_gather;
     return lb_warp_pass_blocks(w);
 }
 
@@ -398,6 +404,8 @@ void autotune(lb_plan &p) {
             probe.pass = pass;
             probe.sms = p.g->sms;
             probe.bvh = sh.bvh;
+            probe.refill = sh.refill;
+            probe.near = sh.near;
             probe.occ = sh.occ;
             int full = lb_warp_pass_blocks(probe);
             int per_sm = std::max(1, full / std::max(1, p.g->sms));
