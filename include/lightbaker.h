@@ -74,7 +74,7 @@ enum lb_status {
     LB_ENODEV = -2,    /* no CUDA device ("no GPU adapter", gpu/mod.rs:83) */
     LB_ECUDA = -3,     /* a CUDA call failed */
     LB_ENOMEM = -4,    /* device memory */
-    LB_ETIMEOUT = -5,  /* a bounded device wait ran out (persistent kernels) */
+    /* -5 is not used: no kernel waits on another, and upload refuses a BVH2 a walk could loop in */
     LB_EIO = -6,       /* file or format error */
     LB_ESCRATCH = -7   /* request larger than a fixed scratch area */
 };
@@ -91,11 +91,18 @@ lb_gpu *lb_gpu_open(int device, char *name, size_t cap);
 void lb_gpu_close(lb_gpu *gpu);
 
 /* Gpu::scene (gpu/mod.rs:129-136): uploads the BVH, the materials (albedo rgb, opacity) and the
- * charts' affine rows (two float4 a chart). Empty charts: a one-chart dummy, as the reference. */
+ * charts' affine rows (two float4 a chart). Empty charts: a one-chart dummy, as the reference. The
+ * BVH must pass lb_bvh_check, or nothing is uploaded (NULL, the reason in lb_last_error). */
 lb_scene *lb_scene_upload(lb_gpu *gpu, const lb_node *nodes, size_t n_nodes, const lb_tri *tris,
                           size_t n_tris, const float *materials /* 4 a material */, size_t n_materials,
                           const float *charts /* 8 a chart */, size_t n_charts);
 void lb_scene_free(lb_scene *scene);
+/* The checks lb_scene_upload makes of a BVH2 before anything reaches the device, on the host only:
+ * every leaf inside the triangle array, and the nodes form a tree whose children follow their parent
+ * as the reference allocates them (bvh.rs:93-101: an inner node's children at first > its own index,
+ * no node with two parents; an inner node whose children lie past the array has none, the reference's
+ * empty BVH). A cyclic or shared child would let a walk loop without end. LB_OK or LB_EINVAL. */
+int lb_bvh_check(const lb_node *nodes, size_t n_nodes, size_t n_tris);
 /* The triangles' exact vertices (9 floats a triangle: v0, v1, v2 of tris[i], in the uploaded order;
  * lb_prepared_get_vertices gives them for a prepared scene), or NULL and 0 to drop them. No counterpart in
  * the reference. With vertices every walk over this scene uses the watertight ray/triangle test (Woop,
@@ -205,9 +212,12 @@ int lb_fill(lb_gpu *gpu, uint32_t w, uint32_t h, const uint32_t *chart, float *v
  * other work is in flight. No counterpart in the reference. The fill's ping-pong copy lives in a
  * fixed 4.25 MiB device array that every GPU loading the library holds until exit; tiles of more
  * than 512 x 512 texels are rejected (LB_ESCRATCH). Arrays are device pointers as for lb_fill;
- * enqueued on `stream` (a cudaStream_t, NULL: the default stream) on the current device. The first
- * call on a device looks the array's address up (cudaGetSymbolAddress): make it before any stream
- * capture. Calls share the array: calls that overlap on the GPU race. Nothing in it needs clearing:
+ * enqueued on `stream` (a cudaStream_t, NULL: the default stream) in the calling thread's current
+ * CUDA context (the device's primary context unless the application made its own current). Each
+ * context holds its own copy of the array at its own address: the first call in a context looks that
+ * address up (cudaGetSymbolAddress) and caches it under the context's unique id, so make that first
+ * call before any stream capture; made during a capture it is refused (LB_EINVAL) with nothing
+ * launched. Calls share the array: calls that overlap on the GPU race. Nothing in it needs clearing:
  * each ring writes every texel of the copy it reads next. */
 int lb_fill_fixed(void *stream, uint32_t w, uint32_t h, const uint32_t *chart, float *values, int channels,
                   uint8_t *valid, int rings);
@@ -240,6 +250,18 @@ int lb_prepared_get_vertices(const lb_prepared *p, float *verts);
 int lb_prepared_get_charts(const lb_prepared *p, float *charts /* 8 a chart */);
 /* Tile t's rectangle (x, y, w, h in the atlas) and key. */
 int lb_prepared_get_tile(const lb_prepared *p, size_t t, uint32_t rect[4], int32_t key[2]);
+/* Tile t's charts, in the layout's order (layout.rs:45-54 `Tile::charts`): the count, and with a
+ * buffer the first `cap` chart indices. */
+size_t lb_prepared_get_tile_charts(const lb_prepared *p, size_t t, uint32_t *charts, size_t cap);
+/* Chart c of the layout (layout.rs:20-40 `Chart`): its plane (normal, axes u and v, the extent min/max
+ * on them), tile key, quarter turn, size and corner in its tile; the count of its triangles, and with
+ * a buffer the first `cap` of them (indices into its mesh, in mesh order). */
+typedef struct lb_chart_frame {
+    uint32_t mesh, turned, x, y, w, h;
+    int32_t tile[2];
+    float normal[3], u[3], v[3], min[2], max[2];
+} lb_chart_frame;
+size_t lb_prepared_get_chart(const lb_prepared *p, size_t c, lb_chart_frame *frame, uint32_t *tris, size_t cap);
 /* raster.rs:39-100: tile t's texels (w * h records, row by row). */
 int lb_prepared_rasterize(const lb_prepared *p, size_t t, lb_texel *out);
 
@@ -354,8 +376,10 @@ int lb_transport_backward_async(lb_transport *t, const float *d_g_indirect, floa
 int lb_transport_bake_indirect(lb_transport *t, float *indirect);
 /* A copy of one of the transport's fixed arrays, for tests ("records", "gathered_index", "texels", "sample_points",
  * "chart", "gathered", "known", "known_bounce", "state", "direct_light", "fixed_indirect", "owner",
- * "light_flags", "tiles", "smooth_weights", "shape"): its size in bytes when out is NULL, else the
- * bytes copied (0 on error). */
+ * "light_flags", "tiles", "smooth_weights", "shape"; and the bake's arrays as it left them: "direct_records"
+ * (the direct pass's record of each covered texel), "valid", "field", "ao", "direct" and "indirect_light"
+ * (float4 a texel), "gather_out" (the last bounce's gather results), "light" (the last light atlas),
+ * "probes"): its size in bytes when out is NULL, else the bytes copied (0 on error). */
 size_t lb_transport_export(lb_transport *t, const char *name, void *out, size_t cap);
 void lb_transport_free(lb_transport *t);
 

@@ -231,6 +231,29 @@ class Prepared:
             N.check(N.lib().lb_prepared_get_tile(self._h, t, rect, key), "tile")
             self.tiles.append({"x": rect[0], "y": rect[1], "w": rect[2], "h": rect[3], "key": (key[0], key[1])})
 
+    def layout(self) -> dict:
+        """The layout as data (layout.rs:20-66): per tile its charts in order; per chart its frame (mesh,
+        turned, corner and size in its tile, tile key, normal, axes u and v, extent min/max) and its
+        triangles (indices into its mesh)."""
+        L = N.lib()
+        tiles = []
+        for t in range(len(self.tiles)):
+            n = L.lb_prepared_get_tile_charts(self._h, t, None, 0)
+            a = np.zeros(n, np.uint32)
+            L.lb_prepared_get_tile_charts(self._h, t, N.ptr(a), n)
+            tiles.append(a)
+        charts = []
+        for c in range(self.info.n_charts):
+            f = N.ChartFrame()
+            n = L.lb_prepared_get_chart(self._h, c, C.byref(f), None, 0)
+            tris = np.zeros(n, np.uint32)
+            L.lb_prepared_get_chart(self._h, c, None, N.ptr(tris), n)
+            charts.append({"mesh": f.mesh, "turned": bool(f.turned), "x": f.x, "y": f.y, "w": f.w, "h": f.h,
+                           "tile": (f.tile[0], f.tile[1]), "normal": np.array(f.normal, np.float32),
+                           "u": np.array(f.u, np.float32), "v": np.array(f.v, np.float32),
+                           "min": np.array(f.min, np.float32), "max": np.array(f.max, np.float32), "tris": tris})
+        return {"tile_charts": tiles, "charts": charts}
+
     def rasterize(self, t: int) -> np.ndarray:
         """raster.rs:39-100: tile t's texels, (h, w) records."""
         tile = self.tiles[t]

@@ -47,6 +47,14 @@ class PreparedInfo(C.Structure):
                 ("params", Params)]
 
 
+class ChartFrame(C.Structure):
+    """lb_chart_frame: a chart of the layout (layout.rs:20-40)."""
+
+    _fields_ = [("mesh", C.c_uint32), ("turned", C.c_uint32), ("x", C.c_uint32), ("y", C.c_uint32),
+                ("w", C.c_uint32), ("h", C.c_uint32), ("tile", C.c_int32 * 2), ("normal", C.c_float * 3),
+                ("u", C.c_float * 3), ("v", C.c_float * 3), ("min", C.c_float * 2), ("max", C.c_float * 2)]
+
+
 class BakeInfo(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("indirect_width", C.c_uint32),
                 ("indirect_height", C.c_uint32), ("has_volume", C.c_uint32), ("volume_size", C.c_uint32 * 3),
@@ -90,6 +98,7 @@ SIGNATURES = {
     "lb_scene_upload": (C.c_void_p, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                      C.c_size_t, C.c_void_p, C.c_size_t]),
     "lb_scene_free": (None, [C.c_void_p]),
+    "lb_bvh_check": (C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t]),
     "lb_scene_set_vertices": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
     "lb_scene_get_bvh8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64),
                                     C.POINTER(C.c_uint64)]),
@@ -125,6 +134,8 @@ SIGNATURES = {
     "lb_prepared_get_charts": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lb_prepared_get_tile": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]),
     "lb_prepared_rasterize": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p]),
+    "lb_prepared_get_tile_charts": (C.c_size_t, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t]),
+    "lb_prepared_get_chart": (C.c_size_t, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t]),
     "lb_bake_run": (C.c_void_p, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(BakeOptions)]),
     "lb_bake_run_with": (C.c_void_p, [C.POINTER(Tracer), C.c_char_p, C.c_size_t, C.POINTER(BakeOptions)]),
     "lb_bake_free": (None, [C.c_void_p]),

@@ -181,6 +181,41 @@ int lb_prepared_get_tile(const lb_prepared *p, size_t t, uint32_t rect[4], int32
     return LB_OK;
 }
 
+size_t lb_prepared_get_tile_charts(const lb_prepared *p, size_t t, uint32_t *charts, size_t cap) {
+    if (!p || t >= p->prep.layout.tiles.size()) return 0;
+    const std::vector<uint32_t> &c = p->prep.layout.tiles[t].charts;
+    if (charts) std::memcpy(charts, c.data(), std::min(cap, c.size()) * 4);
+    return c.size();
+}
+
+size_t lb_prepared_get_chart(const lb_prepared *p, size_t c, lb_chart_frame *frame, uint32_t *tris, size_t cap) {
+    if (!p || c >= p->prep.layout.charts.size()) return 0;
+    const lb::Chart &C = p->prep.layout.charts[c];
+    if (frame) {
+        frame->mesh = C.mesh;
+        frame->turned = C.turned ? 1u : 0u;
+        frame->x = C.x;
+        frame->y = C.y;
+        frame->w = C.w;
+        frame->h = C.h;
+        const lb::Vec3 *axes[3] = {&C.normal, &C.u, &C.v};
+        float *dst[3] = {frame->normal, frame->u, frame->v};
+        for (int a = 0; a < 3; a++) {
+            dst[a][0] = axes[a]->x;
+            dst[a][1] = axes[a]->y;
+            dst[a][2] = axes[a]->z;
+        }
+        frame->min[0] = C.min.x;
+        frame->min[1] = C.min.y;
+        frame->max[0] = C.max.x;
+        frame->max[1] = C.max.y;
+        frame->tile[0] = C.tile.first;
+        frame->tile[1] = C.tile.second;
+    }
+    if (tris) std::memcpy(tris, C.tris.data(), std::min(cap, C.tris.size()) * 4);
+    return C.tris.size();
+}
+
 int lb_prepared_rasterize(const lb_prepared *p, size_t t, lb_texel *out) {
     if (!p || !out || t >= p->prep.layout.tiles.size()) return LB_EINVAL;
     std::vector<lb_texel> v = lb::rasterize(p->scene, p->prep.layout, p->prep.layout.tiles[t]);

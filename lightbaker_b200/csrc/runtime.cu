@@ -135,6 +135,35 @@ void lb_gpu_close(lb_gpu *g) {
     delete g;
 }
 
+int lb_bvh_check(const lb_node *nodes, size_t n_nodes, size_t n_tris) {
+    if (!nodes || n_nodes == 0) {
+        lb_set_error("lb_bvh_check: no nodes");
+        return LB_EINVAL;
+    }
+    // every leaf inside the triangle array (an inner node whose children lie past the node array is the
+    // reference's empty BVH: every walk and the 8-wide build treat it as having no children)
+    for (size_t i = 0; i < n_nodes; i++)
+        if (nodes[i].count > 0 && uint64_t(nodes[i].first) + nodes[i].count > n_tris) {
+            lb_set_error("lb_bvh_check: BVH leaf " + std::to_string(i) + " reaches past the triangle array");
+            return LB_EINVAL;
+        }
+    // A tree whose children come after their parent, as the reference allocates them (bvh.rs:93-101): each inner
+    // node's children lie above its own index and no node has two parents. Every walk then visits each node at
+    // most once a ray and ends; a cyclic or shared child would make a walk loop or repeat without bound.
+    std::vector<uint8_t> parent(n_nodes, 0);
+    for (size_t i = 0; i < n_nodes; i++) {
+        if (nodes[i].count > 0 || uint64_t(nodes[i].first) + 1 >= n_nodes) continue;
+        uint32_t c = nodes[i].first;
+        if (c <= i || parent[c] || parent[c + 1]) {
+            lb_set_error("lb_bvh_check: BVH node " + std::to_string(i) +
+                         " is not a tree node (its children must follow it and have no other parent)");
+            return LB_EINVAL;
+        }
+        parent[c] = parent[c + 1] = 1;
+    }
+    return LB_OK;
+}
+
 lb_scene *lb_scene_upload(lb_gpu *g, const lb_node *nodes, size_t n_nodes, const lb_tri *tris, size_t n_tris,
                           const float *materials, size_t n_materials, const float *charts, size_t n_charts) {
     if (!g || !nodes || n_nodes == 0 || (n_tris && !tris) || (n_materials && !materials) || (n_charts && !charts)) {
@@ -145,13 +174,7 @@ lb_scene *lb_scene_upload(lb_gpu *g, const lb_node *nodes, size_t n_nodes, const
         lb_set_error("lb_scene_upload: more than 2^31 nodes or triangles");
         return nullptr;
     }
-    // every leaf inside the triangle array (an inner node whose children lie past the node array is the
-    // reference's empty BVH: every walk and the 8-wide build treat it as having no children)
-    for (size_t i = 0; i < n_nodes; i++)
-        if (nodes[i].count > 0 && uint64_t(nodes[i].first) + nodes[i].count > n_tris) {
-            lb_set_error("lb_scene_upload: a BVH leaf reaches past the triangle array");
-            return nullptr;
-        }
+    if (lb_bvh_check(nodes, n_nodes, n_tris) != LB_OK) return nullptr;
     cudaSetDevice(g->device);
     lb_scene *s = new lb_scene();
     s->gpu = g;

@@ -1,0 +1,59 @@
+"""The oracle's whole bake (oracle/bake_ref.py + bake_ref.cpp: the reference's bake.rs, raster.rs and
+volume.rs restated independently of the product) against the product's host pipeline (csrc/host, the
+drop-in bake) running the same oracle tracer, on the CPU: the Params, the charts' affines, every
+tile's texels, and the finished atlases and volume must be the same bits."""
+import numpy as np
+import pytest
+
+import lightbaker_b200 as lb
+import oracle
+from lightbaker_b200 import scenes
+from oracle.bake_ref import OracleBake, chart_affines, make_params, raster_tile, read_scene
+
+
+def bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint32) if a.dtype == np.float32 else a
+
+
+def assert_same(name, a, b):
+    d = np.nonzero(bits(a) != bits(b))
+    assert len(d[0]) == 0, f"{name}: {len(d[0])} values differ, first at {[x[:3] for x in d]}"
+
+
+@pytest.mark.parametrize("name", ["reference_test", "small_map", "map_100m"])
+def test_params_affines_and_raster(name):
+    s = scenes.WORKLOADS[name]()
+    P = lb.prepare(s)
+    header, positions = read_scene(s)
+    p = make_params(header, int(P.info.atlas_width), int(P.info.atlas_height))
+    assert bytes(memoryview(p)) == bytes(memoryview(P.params))
+    lm = header["lightmap"]
+    layout = P.layout()
+    assert_same("affines", chart_affines(layout, P.tiles, np.float32(lm["texelsPerMeter"]), int(lm["padding"])),
+                P.charts)
+    tiles = range(len(P.tiles)) if name != "map_100m" else range(0, len(P.tiles), 7)
+    for t in tiles:
+        mine = raster_tile(layout, P.tiles[t], t, positions, np.float32(lm["texelsPerMeter"]), int(lm["padding"]))
+        assert_same(f"tile {t} texels", mine.view(np.uint32), P.rasterize(t).reshape(-1).view(np.uint32))
+        if name == "reference_test":
+            assert (mine["pos"][:, 3] > 0.5).any()
+
+
+@pytest.mark.parametrize("name", ["reference_test", "small_map"])
+def test_oracle_bake_equals_host_pipeline(name):
+    s = scenes.WORKLOADS[name]()
+    P = lb.prepare(s)
+    ob = OracleBake(s, P)
+    t, keep = oracle.tracer()
+    hb = lb.bake_with(s, t)
+    assert_same("direct atlas", ob.direct, hb.direct)
+    assert_same("validity", ob.validity, hb.validity)
+    assert_same("indirect atlas", ob.indirect, hb.indirect)
+    assert_same("volume", ob.volume, hb.volume)
+    assert (ob.rays["direct"], ob.rays["gather"], ob.rays["volume"]) == (
+        hb.stats.rays_direct, hb.stats.rays_gather, hb.stats.rays_volume)
+    # every validity code the bake writes is exercised on the small map (offset, pushed, filled, volume)
+    if name == "small_map":
+        counts = np.bincount(ob.validity.reshape(-1), minlength=6)
+        assert (counts[1:] > 0).all(), counts
