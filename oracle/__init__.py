@@ -34,7 +34,8 @@ def lib():
     global _lib
     if _lib is None:
         if not LIB.exists() or LIB.stat().st_mtime < max(
-                p.stat().st_mtime for p in (HERE / "trace_ref.cpp", HERE / "filter_ref.cpp", HERE / "oracle.h")):
+                p.stat().st_mtime for p in (HERE / "trace_ref.cpp", HERE / "filter_ref.cpp", HERE / "bake_ref.cpp",
+                                            HERE / "bvh_ref.cpp", HERE / "oracle.h")):
             import importlib.util
             spec = importlib.util.spec_from_file_location("oracle_build", HERE / "build.py")
             m = importlib.util.module_from_spec(spec)

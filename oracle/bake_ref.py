@@ -201,6 +201,36 @@ def volume_probes(vs: dict, tile_size: float):
     return (nx, ny, nz), np.array([it[0] for it in items], np.int64), arr
 
 
+def build_bvh(scene: bytes, layout: dict):
+    """bvh.rs:50-104 over the scene (oracle/bvh_ref.cpp), each triangle's chart taken from the layout:
+    (nodes, tris) as raw records (32 and 48 bytes)."""
+    l = lib()
+    if not getattr(l, "_bvh_declared", False):
+        vp, sz = C.c_void_p, C.c_size_t
+        l.or_bvh_build.restype = sz
+        l.or_bvh_build.argtypes = [vp, vp, sz, vp, vp, vp, vp, sz, vp, C.POINTER(sz)]
+        l._bvh_declared = True
+    header, positions = read_scene(scene)
+    meshes = header["meshes"]
+    first = np.zeros(len(meshes) + 1, np.uint32)
+    for i, m in enumerate(meshes):
+        first[i + 1] = first[i] + int(m["triangles"])
+    pos = np.ascontiguousarray(np.concatenate([p.reshape(-1, 9) for p in positions]) if positions
+                               else np.zeros((0, 9), np.float32), np.float32)
+    mat = np.array([int(m["material"]) for m in meshes], np.uint32)
+    casts = np.array([1 if m.get("casts", True) else 0 for m in header["materials"]], np.uint8)
+    chart = np.full(int(first[-1]), 0xFFFFFFFF, np.uint32)
+    for ci, c in enumerate(layout["charts"]):
+        chart[int(first[c["mesh"]]) + c["tris"].astype(np.int64)] = ci
+    n = max(1, int(first[-1]))
+    nodes = np.zeros((2 * n + 1, 8), np.uint32)
+    tris = np.zeros((n, 12), np.uint32)
+    nt = C.c_size_t()
+    nn = l.or_bvh_build(_p(pos), _p(first), len(meshes), _p(mat), _p(casts), _p(chart), _p(nodes), len(nodes),
+                        _p(tris), C.byref(nt))
+    return nodes[:nn], tris[:nt.value]
+
+
 class OracleBake:
     """A whole bake (no cache) on the CPU. Attributes: `direct` (h, w, 2), `validity` (h, w), `indirect`
     (ih, iw, 3), `volume` (probes, 4, 4) or None; per tile `texels` (raster, before any move), `known`,

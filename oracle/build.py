@@ -1,6 +1,6 @@
 """ORACLE build recipe — test infrastructure only.
 
-Compiles the CPU restatement (trace_ref.cpp, filter_ref.cpp, bake_ref.cpp) into oracle/liboracle.so with g++
+Compiles the CPU restatement (trace_ref.cpp, filter_ref.cpp, bake_ref.cpp, bvh_ref.cpp) into oracle/liboracle.so with g++
 -O2 -ffp-contract=off -fopenmp: no fused multiply-add, so every float operation rounds in the order the
 shader's source gives it. The reference itself (Rust + wgpu) cannot be built here: there is no Rust
 toolchain and no graphics stack, so there is no oracle/_ref.
@@ -16,7 +16,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "liboracle.so"
-SRCS = [HERE / "trace_ref.cpp", HERE / "filter_ref.cpp", HERE / "bake_ref.cpp"]
+SRCS = [HERE / "trace_ref.cpp", HERE / "filter_ref.cpp", HERE / "bake_ref.cpp", HERE / "bvh_ref.cpp"]
 DEPS = SRCS + [HERE / "oracle.h", HERE.parent / "include" / "lightbaker.h"]
 
 

@@ -11,6 +11,7 @@
  *                   :303-322 (bounce filters), :337-359 (volume fallback), :364-421 (composite),
  *                   :435-445 (write_light), volume.rs:86-147 (inside fill, irradiance)
  *   transport_ref.py  the bounce transport in float64 and its gradient (torch autograd)
+ *   bvh_ref.cpp     crates/lightbaker/src/bvh.rs:50-162 (the binned SAH build, serial)
  *   bake_ref.py     a whole bake driven from these pieces (the layout and BVH as the product lays them
  *                   out; everything after, including the Params, restated)
  *
@@ -164,6 +165,16 @@ void or_composite(uint32_t aw, uint32_t ah, uint32_t ds, size_t n_tiles, const u
                   const uint8_t *const *known, const uint8_t *const *state, const float *const *field,
                   const float *const *ao, const float *const *indirect, float *direct_out, uint8_t *validity,
                   float *indirect_out);
+
+/* ---- bvh_ref.cpp: the reference's BVH build (bvh.rs:50-162) ---- */
+
+/* Bvh::build over every mesh's triangles (pos: 9 floats a triangle, meshes concatenated, mesh m's at
+ * [mesh_first[m], mesh_first[m + 1])), skipping meshes whose material does not cast; tri_chart: each
+ * triangle's chart (0xffffffff: none). Writes the nodes (when cap_nodes holds them all) and the triangles
+ * (tris_out holds every triangle of the scene) and returns the node count. */
+size_t or_bvh_build(const float *pos, const uint32_t *mesh_first, size_t n_meshes, const uint32_t *mesh_material,
+                    const uint8_t *material_casts, const uint32_t *tri_chart, lb_node *nodes_out, size_t cap_nodes,
+                    lb_tri *tris_out, size_t *n_tris_out);
 
 #ifdef __cplusplus
 }

@@ -57,3 +57,16 @@ def test_oracle_bake_equals_host_pipeline(name):
     if name == "small_map":
         counts = np.bincount(ob.validity.reshape(-1), minlength=6)
         assert (counts[1:] > 0).all(), counts
+
+
+@pytest.mark.parametrize("name", ["reference_test", "small_map", "map_100m", "uneven_tiles"])
+def test_bvh_equals_oracle_build(name):
+    """bvh.rs:50-162 restated independently (oracle/bvh_ref.cpp, serial): the product's parallel build gives
+    the same nodes and triangles byte for byte."""
+    from oracle.bake_ref import build_bvh
+    s = scenes.WORKLOADS[name]() if name != "uneven_tiles" else scenes.uneven_tiles(seed=1, tiles=4,
+                                                                                     tri_range=(2_000, 40_000))
+    P = lb.prepare(s)
+    nodes, tris = build_bvh(s, P.layout())
+    assert_same("nodes", nodes.reshape(-1), P.nodes.view(np.uint32).reshape(-1))
+    assert_same("triangles", tris.reshape(-1), P.tris.view(np.uint32).reshape(-1))
