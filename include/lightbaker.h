@@ -316,6 +316,10 @@ int lb_bake_get_charts(const lb_bake *b, float *out);
 int lb_bake_get_tri_charts(const lb_bake *b, uint32_t *out);
 /* output::write (output.rs:95-154): the .lbake file. *out is malloc'd; free with lb_free. */
 int lb_bake_write(const lb_bake *b, uint8_t **out, size_t *len);
+/* 1 when the bake's file encodings (BC5 of `direct`, RGB9E5 of `indirect`, the probes' bytes) were made
+ * on the device by lb_bake_device, which lb_bake_write then uses as they are (the same bytes the host's
+ * encoders give); 0 when lb_bake_write encodes on the host. */
+int lb_bake_device_encoded(const lb_bake *b);
 void lb_free(void *p);
 
 /* ---- the device-resident bake (the batched mode) ---- */
@@ -399,6 +403,11 @@ int lb_bvh8_collapse(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, s
 void lb_blake3(const uint8_t *data, size_t len, uint8_t out[32]);
 /* encode.rs: RGB9E5 and BC4 blocks, for format tests. */
 uint32_t lb_rgb9e5(const float c[3]);
+/* lb_rgb9e5 on the device over n float4 texels (rgb; w ignored) in device memory, into n words there,
+ * enqueued on the handle's stream: the encoder the device-resident bake runs on its indirect atlas
+ * (encode.cu), equal to lb_rgb9e5 bit for bit. No counterpart in the reference (encode.rs:53-70 runs on
+ * the CPU). */
+int lb_rgb9e5_device(lb_gpu *gpu, const float *rgba, size_t n, uint32_t *out);
 void lb_rgb9e5_decode(uint32_t p, float out[3]);
 void lb_bc4_block(const uint8_t v[16], uint8_t out[8]);
 

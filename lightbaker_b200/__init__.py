@@ -343,6 +343,11 @@ class Bake:
                            info.seconds, info.rays_direct, info.rays_gather, info.rays_volume, info.t_layout,
                            info.t_direct, info.t_bounces, info.t_volume, info.t_composite)
 
+    @property
+    def device_encoded(self) -> bool:
+        """Whether the file's encodings (BC5, RGB9E5, probe bytes) were made on the device."""
+        return bool(N.lib().lb_bake_device_encoded(self._h))
+
     def write(self) -> bytes:
         """The .lbake file (output.rs:95-154)."""
         p = C.POINTER(C.c_uint8)()

@@ -174,6 +174,8 @@ SIGNATURES = {
                                    C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "lb_blake3": (None, [C.c_char_p, C.c_size_t, C.c_void_p]),
     "lb_rgb9e5": (C.c_uint32, [C.POINTER(C.c_float)]),
+    "lb_rgb9e5_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+    "lb_bake_device_encoded": (C.c_int, [C.c_void_p]),
     "lb_rgb9e5_decode": (None, [C.c_uint32, C.POINTER(C.c_float)]),
     "lb_bc4_block": (None, [C.c_void_p, C.c_void_p]),
 }

@@ -27,6 +27,7 @@
 #include "host/deps.h"
 #include "host/handles.h"
 #include "host/raster.h"
+#include "lb_deps.h"
 #include "lb_device.cuh"
 #include "lb_kernels.h"
 #include "lb_post.h"
@@ -95,6 +96,117 @@ int warp_blocks(const lb_plan &p, int pass) {
     return lb_warp_pass_blocks(w);
 }
 
+// A probe's position in the volume grid (volume.rs:36-37): x fastest, then z, then y.
+lb::Vec3 probe_at(const lb::VolumeSettings &v, const std::array<uint32_t, 3> &size, size_t k) {
+    size_t nx = size[0], nz = size[2];
+    return lb::Vec3(v.min[0] + float(k % nx) * v.step, v.min[1] + float(k / (nx * nz)) * v.step,
+                    v.min[2] + float((k / nx) % nz) * v.step);
+}
+
+// The volume's grid and its chunks, the probes of each ground-plan tile (volume.rs:34-41).
+void volume_grid(const lb::VolumeSettings &v, float tile_size, std::array<uint32_t, 3> &size,
+                 std::map<lb::TileKey, std::vector<uint32_t>> &chunks) {
+    auto n = [&](int a) { return uint32_t(std::round((v.max[a] - v.min[a]) / v.step)) + 1; };
+    size = {std::max(n(0), 2u), std::max(n(1), 2u), std::max(n(2), 2u)};
+    chunks.clear();
+    size_t np = size_t(size[0]) * size[1] * size[2];
+    for (size_t k = 0; k < np; k++) chunks[lb::tile_of(probe_at(v, size, k), tile_size)].push_back(uint32_t(k));
+}
+
+// A chunk's seed (volume.rs:49-55): its key, then the volume's settings as JSON.
+std::vector<uint8_t> chunk_seed(const lb::TileKey &key, const std::string &vjson) {
+    std::vector<uint8_t> seed(8);
+    std::memcpy(seed.data(), &key.first, 4);
+    std::memcpy(seed.data() + 4, &key.second, 4);
+    seed.insert(seed.end(), vjson.begin(), vjson.end());
+    return seed;
+}
+
+// Every tile's and chunk's dependency hash (deps.rs:70-96, bake.rs:127-130, volume.rs:42-57), all on the
+// device at once (deps.cu): the casting triangles concatenated here, the seeds hashed here.
+void dependency_hashes(lb_gpu *g, const lb::Scene &scene, const lb::Layout &layout, const lb::Hash &global,
+                       const std::map<lb::TileKey, std::vector<uint32_t>> *chunks, const std::array<uint32_t, 3> &vsize,
+                       std::vector<lb::Hash> &tile_hashes, std::vector<lb::Hash> &chunk_hashes) {
+    const lb::SceneHeader &h = scene.header;
+    const lb::BakeSettings &b = h.bake;
+    DepsInput in;
+    std::vector<size_t> first(h.meshes.size() + 1, 0);
+    for (size_t mi = 0; mi < h.meshes.size(); mi++) {
+        bool casts = h.materials[h.meshes[mi].material].casts;
+        first[mi + 1] = first[mi] + (casts ? scene.positions[mi].size() / 3 : 0);
+    }
+    std::vector<float> pos(first.back() * 9);
+    in.tri_mesh.resize(first.back());
+    in.mesh_start.push_back(0);
+    std::vector<uint32_t> mesh_of(h.meshes.size(), 0);
+    for (size_t mi = 0; mi < h.meshes.size(); mi++) {
+        if (!h.materials[h.meshes[mi].material].casts) continue;
+        mesh_of[mi] = uint32_t(in.mesh_id.size());
+        in.mesh_id.push_back(uint32_t(mi));
+        in.mesh_mat.push_back(h.meshes[mi].material);
+        in.mesh_start.push_back(uint32_t(first[mi + 1]));
+    }
+    float top = -INFINITY;
+#pragma omp parallel for schedule(dynamic, 16) reduction(max : top)
+    for (long long mi = 0; mi < (long long)h.meshes.size(); mi++) {
+        const std::vector<lb::Vec3> &P = scene.positions[mi];
+        // the top of every triangle's box, casting or not (deps.rs:53)
+        for (size_t t = 0; t + 2 < P.size(); t += 3)
+            for (int k = 0; k < 3; k++) top = std::fmax(top, P[t + k].y);
+        if (!h.materials[h.meshes[mi].material].casts) continue;
+        float *dst = pos.data() + first[mi] * 9;
+        for (size_t v = 0; v < P.size(); v++) {
+            dst[v * 3] = P[v].x;
+            dst[v * 3 + 1] = P[v].y;
+            dst[v * 3 + 2] = P[v].z;
+        }
+        for (size_t t = first[mi]; t < first[mi + 1]; t++) in.tri_mesh[t] = mesh_of[mi];
+    }
+    in.pos = pos.data();
+    in.n_tris = uint32_t(first.back());
+    in.top = top;
+    lb::Vec3 sun = lb::Vec3(h.sun.direction[0], h.sun.direction[1], h.sun.direction[2]).normalize();
+    in.sun[0] = sun.x;
+    in.sun[1] = sun.y;
+    in.sun[2] = sun.z;
+    // the queries: every tile (its surfaces' box, bake.rs:127-130), then every chunk (its probes' box)
+    const size_t nt = layout.tiles.size(), nc = chunks ? chunks->size() : 0;
+    std::vector<DepsQuery> qs(nt + nc);
+    const float reach = b.gi_bounces > 0 ? std::fmax(b.gi_reach, b.ao_reach) : b.ao_reach;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long ti = 0; ti < (long long)nt; ti++) {
+        const lb::Tile &t = layout.tiles[ti];
+        lb::Aabb own = lb::tile_box(scene, layout, t.charts);
+        DepsQuery &q = qs[ti];
+        q.min[0] = own.min.x, q.min[1] = own.min.y, q.min[2] = own.min.z;
+        q.max[0] = own.max.x, q.max[1] = own.max.y, q.max[2] = own.max.z;
+        q.reach = reach;
+        std::vector<uint8_t> seed = lb::tile_seed(scene, layout, t.key, t.charts);
+        q.prefix.assign(global.begin(), global.end());
+        q.prefix.insert(q.prefix.end(), seed.begin(), seed.end());
+    }
+    if (chunks) {
+        const lb::VolumeSettings &v = *h.volume;
+        std::string vjson = lb::to_json(v).dump();
+        size_t c = nt;
+        for (auto &kv : *chunks) {
+            lb::Aabb own;
+            for (uint32_t k : kv.second) own.add(probe_at(v, vsize, k));
+            DepsQuery &q = qs[c++];
+            q.min[0] = own.min.x, q.min[1] = own.min.y, q.min[2] = own.min.z;
+            q.max[0] = own.max.x, q.max[1] = own.max.y, q.max[2] = own.max.z;
+            q.reach = b.gi_reach;
+            std::vector<uint8_t> seed = chunk_seed(kv.first, vjson);
+            q.prefix.assign(global.begin(), global.end());
+            q.prefix.insert(q.prefix.end(), seed.begin(), seed.end());
+        }
+    }
+    std::vector<std::array<uint8_t, 32>> out;
+    lb_hash_reach_device(g, in, qs, out);
+    tile_hashes.assign(out.begin(), out.begin() + nt);
+    chunk_hashes.assign(out.begin() + nt, out.end());
+}
+
 void build(lb_plan &p) {
     auto t0 = std::chrono::steady_clock::now();
     const lb::SceneHeader &h = p.scene.header;
@@ -121,23 +233,21 @@ void build(lb_plan &p) {
     // chunks' hashes (only ever cache keys) are not computed
     lb::Cache cache(p.opt.cache);
     const bool caching = !p.opt.cache.empty();
-    std::optional<lb::Boxes> boxes;
-    lb::Hash global{};
-    if (caching) {
-        boxes.emplace(p.scene);
-        global = lb::global_hash(p.scene);
-        if (p.opt.watertight) global = lb::watertight_hash(global);
-    }
-    float reach = b.gi_bounces > 0 ? std::fmax(b.gi_reach, b.ao_reach) : b.ao_reach;
+    if (h.volume) volume_grid(*h.volume, lm.tile_size, p.vsize, p.chunks);
     size_t nt = layout.tiles.size();
     p.hashes.resize(nt);
     p.lights.resize(nt);
+    std::vector<lb::Hash> chunk_hashes;
     if (caching) {
+        // every tile's and chunk's hash at once on the device
+        lb::Hash global = lb::global_hash(p.scene);
+        if (p.opt.watertight) global = lb::watertight_hash(global);
+        dependency_hashes(p.g, p.scene, layout, global, h.volume ? &p.chunks : nullptr, p.vsize, p.hashes,
+                          chunk_hashes);
+        mark("dependency hashes");
 #pragma omp parallel for schedule(dynamic, 1)
         for (long long ti = 0; ti < (long long)nt; ti++) {
             const lb::Tile &t = layout.tiles[ti];
-            p.hashes[ti] = lb::hash_reach(p.scene, *boxes, global, lb::tile_box(p.scene, layout, t.charts), reach,
-                                          lb::tile_seed(p.scene, layout, t.key, t.charts));
             if (auto bytes = cache.get("tile", p.hashes[ti]))
                 p.lights[ti] = lb::TileLight::unpack(*bytes, size_t(t.w) * t.h);
         }
@@ -238,26 +348,14 @@ void build(lb_plan &p) {
     if (h.volume) {
         const lb::VolumeSettings &v = *h.volume;
         p.has_volume = true;
-        auto n = [&](int a) { return uint32_t(std::round((v.max[a] - v.min[a]) / v.step)) + 1; };
-        p.vsize = {std::max(n(0), 2u), std::max(n(1), 2u), std::max(n(2), 2u)};
-        size_t nx = p.vsize[0], nz = p.vsize[2];
         p.n_probes = p.vsize[0] * p.vsize[1] * p.vsize[2];
-        auto at = [&](size_t k) {
-            return lb::Vec3(v.min[0] + float(k % nx) * v.step, v.min[1] + float(k / (nx * nz)) * v.step,
-                            v.min[2] + float((k / nx) % nz) * v.step);
-        };
-        for (size_t k = 0; k < p.n_probes; k++) p.chunks[lb::tile_of(at(k), lm.tile_size)].push_back(uint32_t(k));
+        auto at = [&](size_t k) { return probe_at(v, p.vsize, k); };
         probes_init.assign(size_t(p.n_probes) * 16, 0.0f);
-        std::string vjson = lb::to_json(v).dump();
+        size_t ci = 0;
         for (auto &kv : p.chunks) {
-            lb::Aabb bx;
-            for (uint32_t k : kv.second) bx.add(at(k));
-            std::vector<uint8_t> seed(8);
-            std::memcpy(seed.data(), &kv.first.first, 4);
-            std::memcpy(seed.data() + 4, &kv.first.second, 4);
-            seed.insert(seed.end(), vjson.begin(), vjson.end());
             lb::Hash hash{};
-            if (caching) hash = lb::hash_reach(p.scene, *boxes, global, bx, b.gi_reach, seed);
+            if (caching) hash = chunk_hashes[ci];
+            ci++;
             auto got = caching ? cache.get("probes", hash) : std::nullopt;
             if (got && got->size() == kv.second.size() * 64) {
                 for (size_t i = 0; i < kv.second.size(); i++)
@@ -313,6 +411,10 @@ void build(lb_plan &p) {
     p.indirect_b.alloc(size_t(p.iw) * p.ih * 16);
     p.has.alloc(size_t(p.iw) * p.ih);
     p.has_b.alloc(size_t(p.iw) * p.ih);
+    p.enc_bc5.alloc(size_t(p.aw) * p.ah);
+    p.enc_rgb.alloc(size_t(p.iw) * p.ih * 4);
+    p.enc_vol.alloc(NP * 16);
+    p.enc_scale.alloc(4);
     p.counters.alloc(12 * 8);
     // the first bounce's gather records, which the later bounces evaluate instead of tracing again (their
     // rays are the first bounce's: the keys depend on the gathered texel, not the bounce), and theta at the
@@ -597,6 +699,16 @@ void capture(lb_plan &p) {
         c.indirect = p.indirect.as<float4>();
         c.has = p.has.as<uint8_t>();
         ck(lb_composite(c, p.indirect_b.as<float4>(), p.has_b.as<uint8_t>(), st), "composite");
+        // the file's encodings, from the atlases just written (the file then needs only its compression);
+        // BC5 takes whole 4 x 4 blocks (an atlas of another size is left to the host's writer, which refuses it)
+        if (p.aw % 4 == 0 && p.ah % 4 == 0) {
+            ck(lb_encode_bc5(p.direct_atlas.as<float2>(), p.aw, p.ah, p.enc_bc5.as<uint8_t>(), st), "BC5");
+            ck(lb_encode_rgb9e5(p.indirect.as<float4>(), p.iw * p.ih, p.enc_rgb.as<uint32_t>(), st), "RGB9E5");
+            if (p.has_volume)
+                ck(lb_encode_volume(p.probes.as<float4>(), p.n_probes, p.enc_scale.as<unsigned int>(),
+                                    p.enc_vol.as<uint8_t>(), st),
+                   "volume bytes");
+        }
     } catch (...) {
         cudaGraph_t g;
         cudaStreamEndCapture(st, &g);
@@ -747,7 +859,9 @@ lb::Bake lb_plan_collect(lb_plan &p) {
     // the atlases and probes through the handle's pinned staging buffer (kept between bakes)
     const size_t n_ind = size_t(p.iw) * p.ih, n_pr = p.has_volume ? size_t(p.n_probes) * 16 : 0;
     auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
-    const size_t o_val = up(A * 8), o_ind = o_val + up(A), o_pr = o_ind + up(n_ind * 16), total = o_pr + n_pr * 4;
+    const size_t o_val = up(A * 8), o_ind = o_val + up(A), o_pr = o_ind + up(n_ind * 16), o_bc5 = o_pr + up(n_pr * 4),
+                 o_rgb = o_bc5 + up(A), o_vb = o_rgb + up(n_ind * 4), o_sc = o_vb + up(p.has_volume ? size_t(p.n_probes) * 16 : 0),
+                 total = o_sc + 4;
     if (lb_host_stage_reserve(p.g, total) != LB_OK) throw std::runtime_error(lb_last_error());
     char *stage = (char *)p.g->stage;
     auto fetch = [&](size_t off, const DBuf &d, size_t bytes) {
@@ -759,6 +873,12 @@ lb::Bake lb_plan_collect(lb_plan &p) {
     fetch(o_val, p.validity, A);
     fetch(o_ind, p.indirect, n_ind * 16);
     if (p.has_volume) fetch(o_pr, p.probes, n_pr * 4);
+    fetch(o_bc5, p.enc_bc5, A);
+    fetch(o_rgb, p.enc_rgb, n_ind * 4);
+    if (p.has_volume) {
+        fetch(o_vb, p.enc_vol, size_t(p.n_probes) * 16);
+        fetch(o_sc, p.enc_scale, 4);
+    }
     uint64_t rays[3];
     if (lb_plan_rays(&p, rays) != LB_OK) throw std::runtime_error(lb_last_error());
     const double t_down = since(t0);
@@ -772,6 +892,17 @@ lb::Bake lb_plan_collect(lb_plan &p) {
     for (long long i = 0; i < (long long)n_ind; i++) oi[i] = {ind[i * 4], ind[i * 4 + 1], ind[i * 4 + 2]};
     out.iw = p.iw;
     out.ih = p.ih;
+    if (p.aw % 4 == 0 && p.ah % 4 == 0) {
+        lb::Encoded enc;
+        enc.bc5.assign((const uint8_t *)stage + o_bc5, (const uint8_t *)stage + o_bc5 + A);
+        enc.rgb9e5.resize(n_ind);
+        std::memcpy(enc.rgb9e5.data(), stage + o_rgb, n_ind * 4);
+        if (p.has_volume) {
+            enc.volume.assign((const uint8_t *)stage + o_vb, (const uint8_t *)stage + o_vb + size_t(p.n_probes) * 16);
+            std::memcpy(&enc.volume_scale, stage + o_sc, 4);
+        }
+        out.encoded = std::move(enc);
+    }
     if (p.has_volume) {
         lb::Volume v;
         v.origin = h.volume->min;

@@ -126,7 +126,11 @@ cudaError_t fill_rings(uint32_t w, uint32_t h, const uint32_t *chart, float *v, 
     float *vw = v, *vn = sv;
     uint8_t *kw = valid, *kn = sk;
     for (int r = 0; r < rings; r++) {
-        k_tile_fill<N><<<grid, 256, 0, st>>>(w, h, chart, kw, vw, kn, vn);
+        // cudaLaunchKernel returns this launch's own status: an error the host application left in the thread
+        // before this call is neither consumed nor reported as this call's
+        void *args[] = {&w, &h, (void *)&chart, &kw, &vw, &kn, &vn};
+        cudaError_t e = cudaLaunchKernel((const void *)k_tile_fill<N>, grid, dim3(256), args, 0, st);
+        if (e != cudaSuccess) return e;
         float *t = vw;
         vw = vn;
         vn = t;
@@ -139,7 +143,7 @@ cudaError_t fill_rings(uint32_t w, uint32_t h, const uint32_t *chart, float *v, 
         if (e == cudaSuccess) e = cudaMemcpyAsync(valid, kw, n, cudaMemcpyDeviceToDevice, st);
         if (e != cudaSuccess) return e;
     }
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 }  // namespace lbd
@@ -234,9 +238,51 @@ constexpr size_t FIXED_VALUES = size_t(FIXED_TEXELS) * 4 * sizeof(float);
 static __device__ __align__(256) unsigned char lb_fill_scratch[FIXED_VALUES + FIXED_TEXELS];
 
 namespace {
-// the array's device address, looked up once per device (host code may not take it by name)
+// The array's device address belongs to a CUDA context: each context that loads the library's module has its
+// own copy of the array at its own address. Host code may not take it by name, so it is looked up with
+// cudaGetSymbolAddress and cached under the context's unique id (cuCtxGetId: never reused within a process, so
+// a context destroyed by cudaDeviceReset or by the application, and one created later, never share an entry).
+typedef int (*ctx_get_current_fn)(void **);
+typedef int (*ctx_get_id_fn)(void *, unsigned long long *);
+struct FixedEntry {
+    unsigned long long ctx_id;
+    void *ptr;
+};
 std::mutex g_fixed_mutex;
-void *g_fixed_ptr[128] = {nullptr};
+FixedEntry g_fixed[64];
+int g_fixed_n = 0, g_fixed_next = 0;
+ctx_get_current_fn g_ctx_current = nullptr;
+ctx_get_id_fn g_ctx_id = nullptr;
+
+// The unique id of the calling thread's current context (creating the device's primary context when none is
+// current, as any runtime call would). Driver entry points are taken through the runtime, so the library does
+// not link libcuda.
+cudaError_t current_context_id(unsigned long long *id) {
+    if (!g_ctx_current || !g_ctx_id) {
+        cudaDriverEntryPointQueryResult q1, q2;
+        cudaError_t e = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void **)&g_ctx_current, 12000,
+                                                         cudaEnableDefault, &q1);
+        if (e == cudaSuccess)
+            e = cudaGetDriverEntryPointByVersion("cuCtxGetId", (void **)&g_ctx_id, 12000, cudaEnableDefault, &q2);
+        if (e != cudaSuccess) return e;
+        if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !g_ctx_current || !g_ctx_id) {
+            g_ctx_current = nullptr;
+            g_ctx_id = nullptr;
+            return cudaErrorSymbolNotFound;
+        }
+    }
+    void *ctx = nullptr;
+    if (g_ctx_current(&ctx) != 0) return cudaErrorDeviceUninitialized;
+    if (!ctx) {
+        // no context is current yet: make the runtime bind the device's primary context (no allocation)
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaSetDevice(dev);
+        if (e != cudaSuccess) return e;
+        if (g_ctx_current(&ctx) != 0 || !ctx) return cudaErrorDeviceUninitialized;
+    }
+    return g_ctx_id(ctx, id) == 0 ? cudaSuccess : cudaErrorDeviceUninitialized;
+}
 }  // namespace
 
 extern "C" int lb_fill_fixed(void *stream, uint32_t w, uint32_t h, const uint32_t *chart, float *values, int channels,
@@ -250,26 +296,34 @@ extern "C" int lb_fill_fixed(void *stream, uint32_t w, uint32_t h, const uint32_
                      std::to_string(FIXED_TEXELS) + " (512 x 512); use lb_fill");
         return LB_ESCRATCH;
     }
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return lb_cuda_fail(e, "lb_fill_fixed");
-    if (dev < 0 || dev >= 128) {
-        lb_set_error("lb_fill_fixed: device index out of range");
-        return LB_EINVAL;
-    }
-    void *base;
+    void *base = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_fixed_mutex);
-        if (!g_fixed_ptr[dev]) {
-            void *p = nullptr;
-            e = cudaGetSymbolAddress(&p, lb_fill_scratch);
+        unsigned long long id = 0;
+        cudaError_t e = current_context_id(&id);
+        if (e != cudaSuccess) return lb_cuda_fail(e, "lb_fill_fixed: current context");
+        for (int k = 0; k < g_fixed_n; k++)
+            if (g_fixed[k].ctx_id == id) base = g_fixed[k].ptr;
+        if (!base) {
+            // The first call in a context looks the address up, which may load the library's module into the
+            // context: not allowed while the caller's stream is being captured into a graph.
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            e = cudaStreamIsCapturing((cudaStream_t)stream, &cs);
+            if (e != cudaSuccess) return lb_cuda_fail(e, "lb_fill_fixed: cudaStreamIsCapturing");
+            if (cs != cudaStreamCaptureStatusNone) {
+                lb_set_error("lb_fill_fixed: the first call in a CUDA context must come before any stream capture "
+                             "(it looks up the fixed scratch's address); call it once outside the capture");
+                return LB_EINVAL;
+            }
+            e = cudaGetSymbolAddress(&base, lb_fill_scratch);
             if (e != cudaSuccess) return lb_cuda_fail(e, "lb_fill_fixed: cudaGetSymbolAddress");
-            g_fixed_ptr[dev] = p;
+            g_fixed[g_fixed_next] = {id, base};  // a ring of 64 contexts: the oldest entry goes first
+            g_fixed_next = (g_fixed_next + 1) % 64;
+            if (g_fixed_n < 64) g_fixed_n++;
         }
-        base = g_fixed_ptr[dev];
     }
     float *sv = (float *)base;
     uint8_t *sk = (uint8_t *)base + FIXED_VALUES;
-    e = lb_fill_with_scratch(w, h, chart, values, channels, valid, rings, sv, sk, (cudaStream_t)stream);
+    cudaError_t e = lb_fill_with_scratch(w, h, chart, values, channels, valid, rings, sv, sk, (cudaStream_t)stream);
     return e == cudaSuccess ? LB_OK : lb_cuda_fail(e, "lb_fill_fixed");
 }

@@ -64,6 +64,15 @@ struct Volume {  // volume.rs:22-31
     void irradiance(Vec3 p, Vec3 n, float e[3], float &sun) const;  // volume.rs:125-147
 };
 
+// The file's encodings of a bake's atlases and probes, when the device made them (encode.cu): the BC5
+// blocks of `direct`, the RGB9E5 words of `indirect`, the probes' bytes and their scale.
+struct Encoded {
+    std::vector<uint8_t> bc5;
+    std::vector<uint32_t> rgb9e5;
+    std::vector<uint8_t> volume;
+    float volume_scale = 1.0f;
+};
+
 struct Bake {  // bake.rs:36-47
     Layout layout;
     std::vector<std::array<float, 2>> direct;
@@ -72,6 +81,7 @@ struct Bake {  // bake.rs:36-47
     std::vector<uint8_t> validity;
     std::optional<Volume> volume;
     Stats stats;
+    std::optional<Encoded> encoded;  // beyond the reference: set by the device-resident bake
 };
 
 struct Options {  // bake.rs:30-34

@@ -354,6 +354,8 @@ int lb_bake_get_volume(const lb_bake *b, float *out) {
     return LB_OK;
 }
 
+int lb_bake_device_encoded(const lb_bake *b) { return b && b->bake.encoded ? 1 : 0; }
+
 int lb_bake_write(const lb_bake *b, uint8_t **out, size_t *len) {
     if (!b || !out || !len) return LB_EINVAL;
     return guard(

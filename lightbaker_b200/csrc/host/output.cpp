@@ -64,13 +64,26 @@ Json jf3(const std::array<float, 3> &v) {
 std::vector<uint8_t> write_bake(const Scene &scene, const Bake &bake) {
     const Layout &l = bake.layout;
     size_t w = l.width, h = l.height;
-    std::vector<uint8_t> rg(w * h * 2);
-    for (size_t i = 0; i < w * h; i++) {
-        rg[i * 2] = qbyte(bake.direct[i][0]);
-        rg[i * 2 + 1] = qbyte(bake.direct[i][1]);
+    // the encodings: the device's when it made them (the same bits), else encoded here
+    const Encoded *enc = bake.encoded ? &*bake.encoded : nullptr;
+    std::vector<uint8_t> blocks;
+    if (enc) {
+        blocks = enc->bc5;
+    } else {
+        std::vector<uint8_t> rg(w * h * 2);
+        for (size_t i = 0; i < w * h; i++) {
+            rg[i * 2] = qbyte(bake.direct[i][0]);
+            rg[i * 2 + 1] = qbyte(bake.direct[i][1]);
+        }
+        blocks = bc5(rg.data(), w, h);
     }
-    std::vector<uint32_t> packed(bake.indirect.size());
-    for (size_t i = 0; i < packed.size(); i++) packed[i] = rgb9e5(bake.indirect[i].data());
+    std::vector<uint32_t> packed;
+    if (enc) {
+        packed = enc->rgb9e5;
+    } else {
+        packed.resize(bake.indirect.size());
+        for (size_t i = 0; i < packed.size(); i++) packed[i] = rgb9e5(bake.indirect[i].data());
+    }
     std::vector<float> charts;
     std::vector<uint32_t> ct = l.chart_tile();
     for (size_t c = 0; c < l.charts.size(); c++)
@@ -78,7 +91,7 @@ std::vector<uint8_t> write_bake(const Scene &scene, const Bake &bake) {
     std::vector<uint32_t> tri;
     for (auto &m : l.tri_chart) tri.insert(tri.end(), m.begin(), m.end());
     std::vector<std::pair<std::string, std::vector<uint8_t>>> chunks;
-    chunks.emplace_back("direct", ktx2(FORMAT_BC5, uint32_t(w), uint32_t(h), bc5(rg.data(), w, h)));
+    chunks.emplace_back("direct", ktx2(FORMAT_BC5, uint32_t(w), uint32_t(h), blocks));
     chunks.emplace_back("indirect", ktx2(FORMAT_RGB9E5, bake.iw, bake.ih, bytes_of(packed)));
     auto cb = bytes_of(charts);
     chunks.emplace_back("charts", deflate_raw(cb.data(), cb.size()));
@@ -86,7 +99,10 @@ std::vector<uint8_t> write_bake(const Scene &scene, const Bake &bake) {
     chunks.emplace_back("triangleCharts", deflate_raw(tb.data(), tb.size()));
     chunks.emplace_back("validity", deflate_raw(bake.validity.data(), bake.validity.size()));
     float scale = 1.0f;
-    if (bake.volume) {
+    if (bake.volume && enc) {
+        scale = enc->volume_scale;
+        chunks.emplace_back("volume", deflate_raw(enc->volume.data(), enc->volume.size()));
+    } else if (bake.volume) {
         scale = 1e-6f;
         for (auto &p : bake.volume->probes)
             for (int c = 0; c < 3; c++) scale = std::fmax(scale, p[c]);

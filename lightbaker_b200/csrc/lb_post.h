@@ -69,6 +69,14 @@ cudaError_t lb_composite(const CompositeArgs &c, float4 *scratch, uint8_t *has_b
 // the composite's block averages alone, before its dilations
 cudaError_t lb_composite_blocks(const CompositeArgs &c, cudaStream_t st);
 
+// The output encodings (encode.cu; encode.rs:7-70, output.rs:162-181): the direct atlas as BC5 blocks (w, h
+// multiples of 4; 16 bytes a 4 x 4 block), the indirect atlas as RGB9E5 words (float4 a texel in), the
+// probes as 16 bytes each (4 float4 a probe in) with their scale (the largest L0 colour, >= 1e-6) as bits.
+cudaError_t lb_encode_bc5(const float2 *direct, uint32_t w, uint32_t h, uint8_t *out, cudaStream_t st);
+cudaError_t lb_encode_rgb9e5(const float4 *v, uint32_t n, uint32_t *out, cudaStream_t st);
+cudaError_t lb_encode_volume(const float4 *probes, uint32_t n, unsigned int *scale_bits, uint8_t *out,
+                             cudaStream_t st);
+
 // The device rasteriser (raster.cu; raster.rs:39-114): the dirty tiles' texels (n_texels, the tiles in
 // `tiles`, concatenated) from their triangles (RasterTri, in the host rasteriser's order), written into
 // `tex` (64 bytes a texel, zero where uncovered); `scratch` holds n_texels claims; *pairs gets the number

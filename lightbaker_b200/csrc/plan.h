@@ -85,6 +85,7 @@ struct lb_plan {
     lbplan::DBuf s_ka, s_kb, s_f1, s_f2, s_v4, s_e0, s_e1;
     lbplan::DBuf probes, probes_init, probes_b, probe_items, probe_slot, pk_a, pk_b;
     lbplan::DBuf owner, direct_atlas, validity, indirect, indirect_b, has, has_b, counters;
+    lbplan::DBuf enc_bc5, enc_rgb, enc_vol, enc_scale;  // the output encodings (encode.cu)
     size_t select_bytes = 0;
     uint32_t aw = 0, ah = 0, iw = 0, ih = 0, ds = 1;
     int blocks_direct = 0, blocks_gather = 0, blocks_volume = 0;

@@ -1129,6 +1129,16 @@ size_t lb_transport_export(lb_transport *t, const char *name, void *out, size_t 
     else if (n == "direct_light") dev(t->dl0, size_t(t->n_tex) * 16);
     else if (n == "fixed_indirect") dev(t->fixed_ind, size_t(t->n_tex) * 16);
     else if (n == "owner") dev(p.owner, size_t(t->n_light) * 4);
+    // the bake's own arrays as it left them (the stages a test checks one by one)
+    else if (n == "direct_records") dev(p.direct_out, size_t(p.n_cov) * 16);
+    else if (n == "valid") dev(p.valid, t->n_tex);
+    else if (n == "field") dev(p.field, size_t(t->n_tex) * 4);
+    else if (n == "ao") dev(p.ao, size_t(t->n_tex) * 4);
+    else if (n == "direct") dev(p.dl, size_t(t->n_tex) * 16);
+    else if (n == "indirect_light") dev(p.ind, size_t(t->n_tex) * 16);
+    else if (n == "gather_out") dev(p.gather_out, size_t(t->n_gath) * 16);
+    else if (n == "light") dev(p.light, size_t(t->n_light) * 16);
+    else if (n == "probes") dev(p.probes, p.has_volume ? size_t(p.n_probes) * 64 : 0);
     else if (n == "light_flags") {
         // the atlas's known flags (w of the light atlas)
         std::vector<float> l(size_t(t->n_light) * 4);

@@ -24,6 +24,9 @@ _EXPORT_DTYPES = {
     "gathered": (np.uint8, 1), "known": (np.uint8, 1), "known_bounce": (np.uint8, 1), "state": (np.uint8, 1),
     "direct_light": (np.float32, 4), "fixed_indirect": (np.float32, 4), "owner": (np.uint32, 1),
     "light_flags": (np.uint8, 1), "tiles": (np.uint32, 5), "smooth_weights": (np.float32, 1), "shape": (np.uint32, 1),
+    "direct_records": (np.float32, 4), "valid": (np.uint8, 1), "field": (np.float32, 1), "ao": (np.float32, 1),
+    "direct": (np.float32, 4), "indirect_light": (np.float32, 4), "gather_out": (np.float32, 4),
+    "light": (np.float32, 4), "probes": (np.float32, 16),
 }
 
 
