@@ -125,9 +125,29 @@ def reduce_max(x: float, dist, device) -> float:
     return t.item()
 
 
-def job_value(rays_per_rank: int, world: int, ms_max: float) -> float:
-    """Whole-job Grays/s: every rank's rays over the slowest rank's time."""
-    return rays_per_rank * world / (ms_max / 1e3) / 1e9
+def sum_over_ranks(x: int, dist, device) -> int:
+    """x summed over the ranks (every rank gets it); x itself with one process."""
+    import torch
+    t = torch.tensor([int(x)], dtype=torch.int64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return int(t.item())
+
+
+def job_value(rays_all_ranks: int, ms_max: float) -> float:
+    """Whole-job Grays/s: the rays every rank traced (summed: each rank bakes its own map) over the slowest
+    rank's time."""
+    return rays_all_ranks / (ms_max / 1e3) / 1e9
+
+
+def algorithmic_bytes(workload: str, kernel: str):
+    """The reference walk's bytes per item for a pass (tests/golden/algobytes.json, counted by the oracle on a
+    1 % sample of the workload's items), or None."""
+    try:
+        d = json.loads((ROOT / "tests" / "golden" / "algobytes.json").read_text())
+        return float(d[workload][kernel]["bytes_per_item"])
+    except Exception:
+        return None
 
 
 def parse_tuning(tuning: str) -> dict:
@@ -383,7 +403,8 @@ def main():
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     ms_per_step = max_over_ranks(sum(ms) / len(ms))
-    value = job_value(rays_step, world, ms_per_step)
+    rays_job = sum_over_ranks(rays_step, dist, dev)
+    value = job_value(rays_job, ms_per_step)
     baked = plan.result()
     plan.close()
     if args.device_only:
@@ -436,9 +457,11 @@ def main():
             if i > 0:
                 times.append(e0.elapsed_time(e1))
         kms = statistics.median(times)
-        per_item = 80 if pass_ == lb.Pass.DIRECT else 80
-        alg = walk["nodes"] * 32 + walk["tris"] * 48 + walk["mats"] * 16 + len(items) * per_item
-        kernel_stats[name] = {"ms": kms, "rays": walk["rays"], "alg_bytes": alg, "nodes": walk["nodes"],
+        # the kernel's own fetches (its leaf lists and walks), counted on the device
+        fetched = walk["nodes"] * 32 + walk["tris"] * 48 + walk["mats"] * 16 + len(items) * 80
+        per_item = algorithmic_bytes(args.workload, name)
+        kernel_stats[name] = {"ms": kms, "rays": walk["rays"], "kernel_fetch_bytes": fetched,
+                              "alg_bytes": per_item * len(items) if per_item else None, "nodes": walk["nodes"],
                               "tris": walk["tris"], "mats": walk["mats"], "items": int(len(items))}
     gpu.set_pass_kernel(0)
     gpu.set_register_cap(0)
@@ -472,7 +495,7 @@ def main():
         b.close()
     h2d, d2h = gpu.transfer()
     e2e_t = max_over_ranks(sum(e2e_ms) / len(e2e_ms))
-    e2e_value = e2e_stats.rays * world / (e2e_t / 1e3) / 1e9
+    e2e_value = job_value(sum_over_ranks(e2e_stats.rays, dist, dev), e2e_t)
 
     # ---- the plain drop-in bake (the reference's structure), once ----
     plain = None
@@ -481,7 +504,7 @@ def main():
         pb = lb.bake(scene, gpu)
         pw = max_over_ranks(time.perf_counter() - t0)
         st = pb.stats
-        plain = {"bake_seconds": pw, "grays_e2e": st.rays * world / pw / 1e9,
+        plain = {"bake_seconds": pw, "grays_e2e": sum_over_ranks(st.rays, dist, dev) / pw / 1e9,
                  "grays_passes": st.rays / (st.t_direct + st.t_bounces + st.t_volume) / 1e9,
                  "pass_seconds": st.t_direct + st.t_bounces + st.t_volume, "rays": int(st.rays),
                  "stages_s": {"layout_bvh": st.t_layout, "direct": st.t_direct, "bounces": st.t_bounces,
@@ -569,6 +592,9 @@ def main():
         # each pass runs once a step (the gathers of later bounces are evaluated from records)
         dom = max(kernel_stats, key=lambda k: kernel_stats[k]["ms"])
         ks = kernel_stats[dom]
+        alg_src = "tests/golden/algobytes.json (the reference BVH2 walk's bytes per item, oracle, 1 % sample)"
+        if ks["alg_bytes"] is None:
+            ks["alg_bytes"], alg_src = ks["kernel_fetch_bytes"], "the kernel's own fetches (no frozen count)"
         achieved = ks["alg_bytes"] / (ks["ms"] / 1e3) / 1e9
         # DRAM bytes a launch from an ncu capture (profiles/traffic.txt: workload kernel bytes source)
         traffic, traffic_src = None, None
@@ -594,12 +620,19 @@ def main():
                        "autotune": tuning,
                        "parallelism": f"independent maps x{world}"},
             "bake_seconds": e2e_t / 1e3,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": traffic, "traffic_source": traffic_src and f"profiles/{traffic_src}, scaled by texels",
+            "roofline": {"bound": "issue", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic,
+                         "dram_frac": (traffic / (ks["ms"] / 1e3) / 1e9 / hbm) if traffic else None,
+                         "traffic_source": traffic_src and f"profiles/{traffic_src}, scaled by texels",
                          "kernel": dom, "peak_source": peak_src,
-                         "algorithmic_bytes_per_launch": ks["alg_bytes"], "kernel_ms": ks["ms"],
-                         "note": "algorithmic bytes = 32 B a node record fetched + 48 B a triangle tested + 16 B a "
-                                 "material read + 80 B an item, counted on the device; the BVH lives in L2"},
+                         "algorithmic_bytes_per_launch": ks["alg_bytes"], "algorithmic_bytes_source": alg_src,
+                         "kernel_fetch_bytes_per_launch": ks["kernel_fetch_bytes"], "kernel_ms": ks["ms"],
+                         "note": "achieved = the reference BVH2 walk's bytes (32 B a node record, 48 B a triangle "
+                                 "tested, 16 B a material, 80 B an item) for the launch's items over its time; "
+                                 "they come from L1/L2 (the BVH fits in L2), so frac compares work rates, not "
+                                 "HBM use: dram_frac is the DRAM bytes ncu measured over the same time. The "
+                                 "kernel is bound by instruction issue and dependent-arithmetic latency "
+                                 "(profiles/direct_warp_*.md)"},
             "kernels": kernel_stats,
             "cpu_baseline": {"value": cpu_g, "unit": "Grays/s", "cores": os.cpu_count(), "kind": "port",
                              "sample": f"oracle on {cpu_items['direct']} direct, {cpu_items['gather']} gather texels "
@@ -614,6 +647,9 @@ def main():
             "adjoint": adjoint,
             # the same bake (same outputs): the drop-in's pass seconds over the device step's seconds
             "batched_vs_plain": (plain["pass_seconds"] / (ms_per_step / 1e3)) if plain else None,
+            # the same comparison in the metric's unit: each path's traced rays over its own seconds (the device
+            # traces the first bounce's gather rays only; the drop-in traces every bounce's)
+            "batched_vs_plain_grays": (value / world / plain["grays_passes"]) if plain else None,
             "gpu_launches": kernels * args.steps,
             "clocks": clock_info,
         }

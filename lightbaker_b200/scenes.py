@@ -227,47 +227,56 @@ def reference_test(box_x: float = 8.0) -> bytes:
     return _assemble(groups, materials, sun, sky, lightmap, bake, volume, {"test": True})
 
 
-def uneven_tiles(seed: int = 0, tiles: int = 8, tri_range=(5_000, 500_000), grid: float = 0.25,
-                 bounces: int = 3) -> bytes:
-    """Tiles of uneven weight for the batched bake: a tiles x tiles grid of 16 m tiles (the layout's tile
-    size) on a flat-ish heightfield, each tile's triangle count drawn lognormal over tri_range and made up
-    with small open cylinders (64 triangles each) crowded into the tile, so that both the triangles a ray
-    meets and the texels a tile holds (its atlas region) vary by orders of magnitude. Materials, ray counts
-    and bounces as map_100m; the volume is left out."""
+def uneven_tiles(seed: int = 0, tiles: int = 8, tri_range=(5_000, 500_000), region_range=(64, 512),
+                 bounces: int = 1) -> bytes:
+    """Tiles of uneven weight for the batched bake, with the small plain bake's generators (a heightfield and
+    boxes): a tiles x tiles grid of 16 m tiles (the layout's tile size). Each tile draws two things of its
+    own: a triangle count, lognormal clipped to tri_range, made up by its own patch of heightfield
+    tessellated that finely (one chart: the patch is gently rolling); and an atlas region, log-uniform
+    between region_range[0]^2 and region_range[1]^2 texels at 4 texels/m, made up by boxes (sides U[1, 4]
+    m, six charts each) standing on the patch. So the texels a tile holds and the triangles its rays meet
+    both vary by orders of magnitude, independently. The small plain bake's ray counts and bounce: 64
+    occlusion rays reaching 2 m, one bounce of 64 gather rays; 16 materials; no volume."""
     rng = np.random.default_rng(seed)
     extent = 16.0 * tiles
     noise = _value_noise(rng, 3, 0.5, extent)
-    ground = heightfield(0.0, 0.0, extent, extent, grid, noise)
-    per_tile_ground = len(ground) // 3 // (tiles * tiles)
     lo, hi = np.log(tri_range[0]), np.log(tri_range[1])
     counts = np.exp(np.clip(rng.normal((lo + hi) / 2, (hi - lo) / 4, size=tiles * tiles), lo, hi)).astype(int)
+    side = np.exp(rng.uniform(np.log(region_range[0]), np.log(region_range[1]), size=tiles * tiles))
     materials = [_material(f"m{k}", rng.uniform(0.15, 0.85, size=3)) for k in range(16)]
     per_mat = [[] for _ in range(16)]
-    for t, want in enumerate(counts):
+    ground = []
+    density, pad = 4.0, 2
+    for t in range(tiles * tiles):
         tx, tz = (t % tiles) * 16.0, (t // tiles) * 16.0
-        n_cyl = max(0, (int(want) - per_tile_ground) // 64)
-        if n_cyl == 0:
-            continue
-        x = tx + rng.uniform(0.5, 15.5, n_cyl)
-        z = tz + rng.uniform(0.5, 15.5, n_cyl)
-        r = rng.uniform(0.03, 0.25, n_cyl)
-        h = rng.uniform(0.3, 4.0, n_cyl)
-        yaw = rng.uniform(0.0, 2 * math.pi, n_cyl)
-        m = rng.integers(0, 16, n_cyl)
-        base = noise(x, z) - 0.1
-        for k in range(n_cyl):
-            per_mat[int(m[k])].append(cylinder(x[k], base[k], z[k], r[k], h[k], yaw[k]))
-    groups = [("ground", 0, ground)]
+        # boxes until the tile's charts fill about side^2 texels (its ground chart takes 68^2)
+        budget = side[t] ** 2 - (16 * density + 2 * pad) ** 2
+        boxes = []
+        while budget > 0 and len(boxes) < 2000:
+            sx, sy, sz = rng.uniform(1.0, 4.0, size=3)
+            faces = [(sx, sy), (sx, sy), (sz, sy), (sz, sy), (sx, sz), (sx, sz)]
+            budget -= sum((a * density + 2 * pad + 1) * (b * density + 2 * pad + 1) for a, b in faces) * 1.15
+            x, z = tx + rng.uniform(0.2, 15.8 - sx), tz + rng.uniform(0.2, 15.8 - sz)
+            base = float(noise(np.array(x + sx / 2), np.array(z + sz / 2))) - 0.3
+            boxes.append((x, base, z, sx, sy, sz))
+        for (x, base, z, sx, sy, sz) in boxes:
+            per_mat[int(rng.integers(0, 16))].append(np.asarray(cube((x, base, z), (x + sx, base + sy, z + sz)),
+                                                                np.float32))
+        # the rest of the triangles in the tile's own ground patch, 2 a cell
+        cells = max(1, int(round(math.sqrt(max(2, counts[t] - 12 * len(boxes)) / 2))))
+        ground.append(heightfield(tx, tz, 16.0, 16.0, 16.0 / cells, noise))
+    groups = [("ground", 0, np.concatenate(ground))]
     for k in range(16):
         if per_mat[k]:
-            groups.append((f"props{k}", k, np.concatenate(per_mat[k])))
+            groups.append((f"boxes{k}", k, np.concatenate(per_mat[k])))
     sky = {"zenith": [0.5, 0.6, 0.8], "horizon": [0.5, 0.6, 0.8], "ground": [0.5, 0.6, 0.8]}
     sun = {"direction": sun_direction(40.0, 130.0), "radiusDeg": 0.5, "irradiance": [3.0, 3.0, 3.0]}
-    lightmap = {"texelsPerMeter": 4.0, "tileSize": 16.0, "chartAngleDeg": 40.0, "padding": 2, "atlasWidth": 4096,
-                "indirectDownscale": 2}
-    bake = _defaults_bake(aoRays=256, aoReach=2.0, giRays=128, giBounces=bounces)
+    lightmap = {"texelsPerMeter": density, "tileSize": 16.0, "chartAngleDeg": 40.0, "padding": pad,
+                "atlasWidth": 4096, "indirectDownscale": 2}
+    bake = _defaults_bake(aoRays=64, aoReach=2.0, giRays=64, giBounces=bounces)
     return _assemble(groups, materials, sun, sky, lightmap, bake, None,
-                     {"workload": "uneven_tiles", "seed": seed, "tile_triangles": [int(c) for c in counts]})
+                     {"workload": "uneven_tiles", "seed": seed, "tile_triangles": [int(c) for c in counts],
+                      "tile_region_side": [float(v) for v in side]})
 
 
 def stress_map(seed: int = 0, size: float = 400.0, boxes: int = 6000, cylinders: int = 30000, bounces: int = 4,

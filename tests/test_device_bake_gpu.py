@@ -45,7 +45,7 @@ def test_device_bake_equals_drop_in(gpu, name):
 def test_uneven_tiles_in_one_graph(gpu):
     """Tiles whose triangle counts (lognormal, 2k to 40k) and atlas regions differ by an order of magnitude,
     all rebaked in one graph with the autotuner on: the same bits as the drop-in bake."""
-    s = scenes.uneven_tiles(seed=1, tiles=4, tri_range=(2_000, 40_000), grid=0.5, bounces=2)
+    s = scenes.uneven_tiles(seed=1, tiles=4, tri_range=(2_000, 40_000), bounces=2)
     P = lb.prepare(s)
     areas = [int(t["w"]) * int(t["h"]) for t in P.tiles]
     assert max(areas) >= 8 * min(areas)

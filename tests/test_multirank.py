@@ -1,6 +1,6 @@
 """The bench's multi-GPU path on the CPU: two gloo ranks, each baking its own map (seed = rank, no
-collective on the data path), the step time taken as the maximum over ranks and the job's value as every
-rank's rays over it. The bake itself runs on the oracle's tracer here (no GPU)."""
+collective on the data path), the step time taken as the maximum over ranks and the job's value as the
+sum of every rank's rays over it. The bake itself runs on the oracle's tracer here (no GPU)."""
 import os
 import socket
 
@@ -37,7 +37,7 @@ def _rank(rank, world, port, out):
         ms = (time.perf_counter() - t0) * 1e3
         ms_max = bench.reduce_max(ms, dist, "cpu")
         rays = baked.stats.rays
-        out.put((rank, ms, ms_max, rays, bench.job_value(rays, world, ms_max),
+        out.put((rank, ms, ms_max, rays, bench.job_value(bench.sum_over_ranks(rays, dist, "cpu"), ms_max),
                  float(np.asarray(baked.indirect, np.float64).sum())))
         dist.barrier()
         del keep
@@ -65,4 +65,6 @@ def test_two_ranks_bake_their_own_maps_and_time_as_the_slowest():
     assert max0 == max1 == pytest.approx(max(ms0, ms1))
     # weak scaling: each rank its own map
     assert ind0 != ind1
-    assert v0 == pytest.approx(rays0 * 2 / (max0 / 1e3) / 1e9)
+    # the job's rays are both ranks' own counts summed (the maps differ, so do their ray counts)
+    assert rays0 != rays1
+    assert v0 == v1 == pytest.approx((rays0 + rays1) / (max0 / 1e3) / 1e9)
