@@ -143,7 +143,10 @@ int lb_trace(lb_gpu *gpu, lb_scene *scene, const lb_ray *rays, size_t n, int any
 
 /* Gpu::run (gpu/mod.rs:140-196): runs `pass` over `n` items, reading `light` (4 floats an atlas
  * texel; may be empty), writing n * width float4 records into the caller's `out` (width 4 for
- * LB_PASS_VOLUME, else 1). params->counts[3] and atlas[2] are set per batch as the reference does. */
+ * LB_PASS_VOLUME, else 1). One launch over the list: item i is keyed as the shader keys it, by
+ * params->atlas[2] + i (trace.wgsl:172-173). The bake's Params hold 0 there, as the reference's
+ * Gpu::run gives its first batch; a caller running part of a longer list (one rank's shard of the
+ * tiles) passes the index of its first item in the whole list, so every item keeps its key. */
 int lb_run(lb_gpu *gpu, lb_scene *scene, int pass, const lb_params *params, const lb_texel *items,
            size_t n, const float *light, size_t n_light, float *out);
 
@@ -275,6 +278,19 @@ typedef struct lb_tracer {
                const float *light, size_t n_light, float *out, uint64_t *rays);
 } lb_tracer;
 
+/* How the ranks of a bake split over several processes (one a GPU) exchange what the others need: the
+ * light atlas after each bounce, the probes, the atlases' pieces and some counts. No counterpart in the
+ * reference (one process bakes everything). `sum` adds `count` 32-bit words at `data` element-wise over
+ * every rank, in place, as unsigned integers: every exchanged word is written by one rank and zero on
+ * the others, so the sum carries that rank's bits exactly (floats included). device: 0 host memory, 1
+ * device memory (the library's stream is synchronised before the call). 0 on success. Every rank makes
+ * the same calls in the same order. */
+typedef struct lb_exchange {
+    void *ctx;
+    int rank, world;
+    int (*sum)(void *ctx, void *data, size_t count, int device);
+} lb_exchange;
+
 typedef struct lb_bake_options {
     const char *cache_dir;                      /* NULL: no cache (bake.rs:30-34) */
     void (*log)(void *ctx, const char *line);   /* NULL: quiet */
@@ -286,6 +302,10 @@ typedef struct lb_bake_options {
     int watertight;                             /* the watertight triangle test (lb_scene_set_vertices) in
                                                  * every pass; such tiles are cached apart (default 0: the
                                                  * shader's test) */
+    const lb_exchange *exchange;                /* NULL: one process bakes every tile. Else this rank bakes its
+                                                 * share of the dirty tiles (contiguous in tile order, balanced
+                                                 * by their texels) and probe chunks, and every rank returns
+                                                 * the whole bake, equal to one process's bit for bit */
 } lb_bake_options;
 
 typedef struct lb_bake lb_bake;

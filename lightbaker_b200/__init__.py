@@ -370,12 +370,56 @@ class Bake:
             pass
 
 
-def _options(cache, log, autotune=False, trace_every_bounce=False, watertight=False):
+class Exchange:
+    """How the ranks of a bake split over processes add up what each baked (lb_exchange): element-wise sums of
+    32-bit words over a torch.distributed process group (gloo for host memory; NCCL: host memory is staged
+    through the device). Every rank bakes its share of the tiles and gets the whole bake."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+        self._dist, self._group = dist, group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        self._cb = N.SUM_CB(self._sum)
+        self.struct = N.Exchange(None, self.rank, self.world, self._cb)
+
+    def _sum(self, ctx, data, count, device):
+        import torch
+        try:
+            if device:
+                t = torch.as_tensor(_DeviceWords(data, count), device="cuda")
+                torch.cuda.synchronize()
+                self._dist.all_reduce(t, group=self._group)
+                torch.cuda.synchronize()
+                return 0
+            a = np.ctypeslib.as_array(C.cast(data, C.POINTER(C.c_int32)), shape=(count,))
+            t = torch.from_numpy(a)
+            if self._dist.get_backend(self._group) == "nccl":
+                g = t.cuda()
+                self._dist.all_reduce(g, group=self._group)
+                t.copy_(g.cpu())
+            else:
+                self._dist.all_reduce(t, group=self._group)
+            return 0
+        except Exception:
+            return 1
+
+
+class _DeviceWords:
+    """A device buffer of 32-bit words as __cuda_array_interface__ (for torch.as_tensor)."""
+
+    def __init__(self, ptr, count):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<i4", "data": (ptr, False), "version": 3}
+
+
+def _options(cache, log, autotune=False, trace_every_bounce=False, watertight=False, exchange=None):
     opts = N.BakeOptions()
     opts.cache_dir = str(cache).encode() if cache else None
     opts.autotune = int(bool(autotune))
     opts.trace_every_bounce = int(bool(trace_every_bounce))
     opts.watertight = int(bool(watertight))
+    if exchange is not None:
+        opts.exchange = C.pointer(exchange.struct)
     keep = None
     if log is not None:
         keep = N.LOG_CB(lambda ctx, line: log(line.decode("utf-8", "replace")))
@@ -383,10 +427,11 @@ def _options(cache, log, autotune=False, trace_every_bounce=False, watertight=Fa
     return opts, keep
 
 
-def bake(scene: bytes, gpu: Gpu, cache=None, log=None, watertight: bool = False) -> Bake:
+def bake(scene: bytes, gpu: Gpu, cache=None, log=None, watertight: bool = False, exchange: Exchange = None) -> Bake:
     """bake() (bake.rs:94-432): the whole bake with the passes on `gpu`; `watertight`: the watertight
-    triangle test instead of the shader's (lb_bake_options)."""
-    opts, keep = _options(cache, log, watertight=watertight)
+    triangle test instead of the shader's; `exchange`: this process is one rank of a bake split over
+    several (lb_bake_options)."""
+    opts, keep = _options(cache, log, watertight=watertight, exchange=exchange)
     h = N.lib().lb_bake_run(gpu.handle, scene, len(scene), C.byref(opts))
     del keep
     if not h:
@@ -444,9 +489,9 @@ class Plan:
             pass
 
 
-def bake_with(scene: bytes, tracer: "N.Tracer", cache=None, log=None) -> Bake:
+def bake_with(scene: bytes, tracer: "N.Tracer", cache=None, log=None, exchange: Exchange = None) -> Bake:
     """The same bake with the passes on a caller's runner (an lb_tracer)."""
-    opts, keep = _options(cache, log)
+    opts, keep = _options(cache, log, exchange=exchange)
     h = N.lib().lb_bake_run_with(C.byref(tracer), scene, len(scene), C.byref(opts))
     del keep
     if not h:

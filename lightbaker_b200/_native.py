@@ -85,9 +85,18 @@ class Tracer(C.Structure):
     _fields_ = [("ctx", C.c_void_p), ("scene", SCENE_CB), ("run", RUN_CB)]
 
 
+SUM_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int)
+
+
+class Exchange(C.Structure):
+    """lb_exchange: the ranks' element-wise sum of 32-bit words."""
+
+    _fields_ = [("ctx", C.c_void_p), ("rank", C.c_int), ("world", C.c_int), ("sum", SUM_CB)]
+
+
 class BakeOptions(C.Structure):
     _fields_ = [("cache_dir", C.c_char_p), ("log", LOG_CB), ("log_ctx", C.c_void_p), ("autotune", C.c_int),
-                ("trace_every_bounce", C.c_int), ("watertight", C.c_int)]
+                ("trace_every_bounce", C.c_int), ("watertight", C.c_int), ("exchange", C.POINTER(Exchange))]
 
 
 # every exported entry point: name -> (restype, argtypes)

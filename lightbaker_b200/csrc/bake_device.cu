@@ -757,6 +757,9 @@ lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_
         }
         p->opt.watertight = opts && opts->watertight;
         p->autotune = opts && opts->autotune;
+        if (opts && opts->exchange && opts->exchange->world > 1)
+            throw std::runtime_error("lb_plan_create: a bake split over ranks runs through lb_bake_run or "
+                                     "lb_bake_run_with (exchange set)");
         p->reuse = !(opts && opts->trace_every_bounce);
         p->keep_records = keep_records;
         p->group_direct = g->group_direct;

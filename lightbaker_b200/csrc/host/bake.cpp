@@ -196,7 +196,8 @@ namespace {
 // volume.rs:34-120
 Volume bake_volume(const Scene &scene, Tracer &gpu, lb_params params, const std::vector<float> &light,
                    const VolumeSettings &v, const Boxes &boxes, const Hash &global, const Cache &cache, Stats &stats,
-                   const std::function<void(const std::string &)> &log) {
+                   const std::function<void(const std::string &)> &log, int rank, int world,
+                   const std::function<void(void *, size_t)> &sum_words) {
     auto started = std::chrono::steady_clock::now();
     auto n = [&](int a) { return uint32_t(std::round((v.max[a] - v.min[a]) / v.step)) + 1; };
     std::array<uint32_t, 3> size = {std::max(n(0), 2u), std::max(n(1), 2u), std::max(n(2), 2u)};
@@ -232,16 +233,33 @@ Volume bake_volume(const Scene &scene, Tracer &gpu, lb_params params, const std:
             keys.emplace_back(hash, kv.second);
         }
     }
-    std::vector<lb_texel> items(todo.size());
-    for (size_t i = 0; i < todo.size(); i++) {
+    // a bake split over ranks: this rank's contiguous run of the chunks to bake, balanced by probes (a probe's
+    // keys are its own index, so any split keeps them); the others' probes arrive through the sum
+    std::vector<uint64_t> chunk_cost;
+    for (auto &kv : keys) chunk_cost.push_back(kv.second.size());
+    const auto share = shard_range(chunk_cost, rank, world);
+    size_t p0 = 0, p1 = 0;
+    for (size_t c = 0; c < keys.size(); c++) {
+        if (c < share.first) p0 += keys[c].second.size();
+        if (c < share.second) p1 += keys[c].second.size();
+    }
+    std::vector<lb_texel> items(p1 - p0);
+    for (size_t i = p0; i < p1; i++) {
         Vec3 p = at(todo[i]);
-        items[i] = lb_texel{{p.x, p.y, p.z, 1.0f}, {0.0f, 1.0f, 0.0f, u2f(todo[i])}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+        items[i - p0] = lb_texel{{p.x, p.y, p.z, 1.0f}, {0.0f, 1.0f, 0.0f, u2f(todo[i])}, {0, 0, 0, 0}, {0, 0, 0, 0}};
     }
     params.counts[2] = v.rays;
     std::vector<float> res;
     stats.rays_volume += gpu.run(LB_PASS_VOLUME, params, items, light, res);
+    if (world > 1) {
+        std::vector<float> all(todo.size() * 16, 0.0f);
+        std::memcpy(all.data() + p0 * 16, res.data(), (p1 - p0) * 64);
+        sum_words(all.data(), all.size());
+        res = std::move(all);
+    }
     for (size_t i = 0; i < todo.size(); i++) std::memcpy(vol.probes[todo[i]].data(), &res[i * 16], 64);
-    for (auto &kv : keys) {
+    for (size_t c = share.first; c < share.second; c++) {
+        auto &kv = keys[c];
         std::vector<uint8_t> bytes(kv.second.size() * 64);
         for (size_t i = 0; i < kv.second.size(); i++) std::memcpy(bytes.data() + i * 64, vol.probes[kv.second[i]].data(), 64);
         cache.put("probes", kv.first, bytes);
@@ -282,6 +300,29 @@ Volume bake_volume(const Scene &scene, Tracer &gpu, lb_params params, const std:
 
 }  // namespace
 
+std::pair<size_t, size_t> shard_range(const std::vector<uint64_t> &cost, int rank, int world) {
+    if (world <= 1) return {0, cost.size()};
+    std::vector<uint64_t> prefix(cost.size() + 1, 0);
+    for (size_t i = 0; i < cost.size(); i++) prefix[i + 1] = prefix[i] + cost[i];
+    const uint64_t total = prefix.back();
+    // boundary r: the item index whose prefix cost is nearest total * r / world (ties to the lower), never
+    // before boundary r - 1
+    auto boundary = [&](int r) {
+        if (r <= 0) return size_t(0);
+        if (r >= world) return cost.size();
+        size_t k = 0;
+        while (k < cost.size() && prefix[k] * uint64_t(world) < total * uint64_t(r)) k++;
+        if (k > 0 && (prefix[k] * uint64_t(world) - total * uint64_t(r)) >
+                         (total * uint64_t(r) - prefix[k - 1] * uint64_t(world)))
+            k--;
+        return k;
+    };
+    size_t a = 0;
+    for (int r = 1; r <= rank; r++) a = std::max(a, boundary(r));
+    size_t b = std::max(a, boundary(rank + 1));
+    return {a, b};
+}
+
 Bake bake(const Scene &scene, Tracer &gpu, const Options &o) {
     auto started = std::chrono::steady_clock::now();
     auto log = [&](const std::string &s) {
@@ -320,17 +361,43 @@ Bake bake(const Scene &scene, Tracer &gpu, const Options &o) {
                                 tile_seed(scene, layout, t.key, t.charts));
         if (auto bytes = cache.get("tile", hashes[ti])) lights[ti] = TileLight::unpack(*bytes, size_t(t.w) * t.h);
     }
-    std::vector<size_t> dirty;
-    for (size_t i = 0; i < nt; i++)
-        if (!lights[i]) dirty.push_back(i);
+    std::vector<size_t> dirty, cached;
+    for (size_t i = 0; i < nt; i++) (lights[i] ? cached : dirty).push_back(i);
     log(std::to_string(dirty.size()) + " of " + std::to_string(nt) + " tiles to bake");
 
+    // A bake split over ranks (beyond the reference): this rank bakes a contiguous run of the dirty tiles,
+    // balanced by their texels, so its items are a contiguous run of each pass's whole list and keep their
+    // keys (the index in that list) from one base; what the others bake arrives through sums of 32-bit words
+    // in which every word has one writer. One rank: everything, and the sums are no-ops.
+    const int world = (o.world > 1 && o.sum) ? o.world : 1, rank = world > 1 ? o.rank : 0;
+    auto sum_words = [&](void *data, size_t words) {
+        if (world > 1 && words) o.sum(data, words, false);
+    };
+    std::vector<uint64_t> tile_cost;
+    for (size_t ti : dirty) tile_cost.push_back(uint64_t(layout.tiles[ti].w) * layout.tiles[ti].h);
+    const auto shard = shard_range(tile_cost, rank, world);
+    std::vector<size_t> mine(dirty.begin() + shard.first, dirty.begin() + shard.second);
+    if (world > 1)
+        log("rank " + std::to_string(rank) + " of " + std::to_string(world) + ": dirty tiles " +
+            std::to_string(shard.first) + " to " + std::to_string(shard.second));
+    // counts of every dirty tile from every rank: the bases of this rank's keys
+    auto shared_counts = [&](const std::vector<size_t> &own, uint64_t &before, uint64_t &all) {
+        std::vector<uint32_t> c(dirty.size(), 0);
+        for (size_t k = 0; k < own.size(); k++) c[shard.first + k] = uint32_t(own[k]);
+        sum_words(c.data(), c.size());
+        before = all = 0;
+        for (size_t k = 0; k < c.size(); k++) {
+            if (k < shard.first) before += c[k];
+            all += c[k];
+        }
+    };
+
     // the dirty tiles' texels (bake.rs:138-149)
-    std::vector<Work> work(dirty.size());
+    std::vector<Work> work(mine.size());
 #pragma omp parallel for schedule(dynamic, 1)
-    for (long long wi = 0; wi < (long long)dirty.size(); wi++) {
+    for (long long wi = 0; wi < (long long)mine.size(); wi++) {
         Work &w = work[wi];
-        w.tile = dirty[wi];
+        w.tile = mine[wi];
         w.texels = rasterize(scene, layout, layout.tiles[w.tile]);
         size_t n = w.texels.size();
         w.chart.resize(n);
@@ -344,12 +411,23 @@ Bake bake(const Scene &scene, Tracer &gpu, const Options &o) {
         }
     }
     std::vector<lb_texel> covered_list;
-    for (auto &w : work)
+    std::vector<size_t> cov_counts;
+    for (auto &w : work) {
+        size_t c = 0;
         for (auto &t : w.texels)
-            if (covered(t)) covered_list.push_back(t);
+            if (covered(t)) {
+                covered_list.push_back(t);
+                c++;
+            }
+        cov_counts.push_back(c);
+    }
+    uint64_t direct_base = 0, covered_all = 0;
+    shared_counts(cov_counts, direct_base, covered_all);
     auto t0 = std::chrono::steady_clock::now();
     std::vector<float> direct;
-    stats.rays_direct = gpu.run(LB_PASS_DIRECT, params, covered_list, {}, direct);
+    lb_params p_direct = params;
+    p_direct.atlas[2] = uint32_t(direct_base);
+    stats.rays_direct = gpu.run(LB_PASS_DIRECT, p_direct, covered_list, {}, direct);
     stats.t_direct = since(t0);
     log("sun and occlusion: " + std::to_string(covered_list.size()) + " texels, " + fmt("%.1f s", stats.t_direct));
 
@@ -460,9 +538,16 @@ Bake bake(const Scene &scene, Tracer &gpu, const Options &o) {
     }
     for (size_t wi = 0; wi < work.size(); wi++) lights[work[wi].tile] = std::move(made[wi]);
 
-    // the bounces, each gathering what the last left in the atlas (bake.rs:277-330)
+    // the bounces, each gathering what the last left in the atlas (bake.rs:277-330): this rank's tiles'
+    // light, the other ranks' through the sum, the cached tiles' (the same on every rank) after it
     std::vector<float> light(aw * ah * 4, 0.0f);
-    for (size_t ti = 0; ti < nt; ti++) write_light(layout, ti, *lights[ti], light);
+    auto share_light = [&]() {
+        std::fill(light.begin(), light.end(), 0.0f);
+        for (auto &w : work) write_light(layout, w.tile, *lights[w.tile], light);
+        sum_words(light.data(), light.size());
+        for (size_t ti : cached) write_light(layout, ti, *lights[ti], light);
+    };
+    share_light();
     size_t ds = lm.indirect_downscale;
     for (auto &w : work) {
         size_t tw = layout.tiles[w.tile].w;
@@ -491,11 +576,15 @@ Bake bake(const Scene &scene, Tracer &gpu, const Options &o) {
         gcounts.push_back(c);
     }
     std::vector<size_t> gstarts = offsets(gcounts);
+    uint64_t gather_base = 0, gathered_all = 0;
+    shared_counts(gcounts, gather_base, gathered_all);
+    lb_params p_gather = params;
+    p_gather.atlas[2] = uint32_t(gather_base);
     auto tb = std::chrono::steady_clock::now();
     for (uint32_t bounce = 0; bounce < b.gi_bounces; bounce++) {
         auto t1 = std::chrono::steady_clock::now();
         std::vector<float> res;
-        stats.rays_gather += gpu.run(LB_PASS_GATHER, params, gather, light, res);
+        stats.rays_gather += gpu.run(LB_PASS_GATHER, p_gather, gather, light, res);
         std::vector<std::vector<float>> updated(work.size());
 #pragma omp parallel for schedule(dynamic, 1)
         for (long long wi = 0; wi < (long long)work.size(); wi++) {
@@ -521,15 +610,17 @@ Bake bake(const Scene &scene, Tracer &gpu, const Options &o) {
             TileLight &l = *lights[work[wi].tile];
             for (size_t i = 0; i < l.indirect.size(); i++)
                 l.indirect[i] = {updated[wi][i * 3], updated[wi][i * 3 + 1], updated[wi][i * 3 + 2]};
-            write_light(layout, work[wi].tile, l, light);
         }
+        share_light();
         log("bounce " + std::to_string(bounce + 1) + ": " + std::to_string(gather.size()) + " texels x " +
             std::to_string(b.gi_rays) + " rays, " + fmt("%.1f s", since(t1)));
     }
     stats.t_bounces = since(tb);
     std::optional<Volume> volume;
     auto tv = std::chrono::steady_clock::now();
-    if (h.volume) volume = bake_volume(scene, gpu, params, light, *h.volume, boxes, global, cache, stats, o.log);
+    if (h.volume)
+        volume = bake_volume(scene, gpu, params, light, *h.volume, boxes, global, cache, stats, o.log, rank, world,
+                             sum_words);
     stats.t_volume = since(tv);
     // texels left without light of their own take the volume's (bake.rs:335-359)
     auto tc = std::chrono::steady_clock::now();
@@ -557,13 +648,14 @@ Bake bake(const Scene &scene, Tracer &gpu, const Options &o) {
     }
     for (auto &w : work) cache.put("tile", hashes[w.tile], lights[w.tile]->pack());
 
-    // the atlas from every tile (bake.rs:364-421)
+    // the atlas from every tile (bake.rs:364-421): this rank's tiles, the others' through the sums (each
+    // ds x ds block lies in one tile: tiles start on a 4-texel grid and ds divides 4), then the cached tiles'
     Bake out;
     size_t iw = (aw + ds - 1) / ds, ih = (ah + ds - 1) / ds;
-    out.direct.assign(aw * ah, {1.0f, 1.0f});
-    out.validity.assign(aw * ah, V_NONE);
+    std::vector<std::array<float, 2>> dpart(aw * ah, {0.0f, 0.0f});
+    std::vector<uint8_t> vpart((aw * ah + 3) & ~size_t(3), 0), kpart((aw * ah + 3) & ~size_t(3), 0);
     std::vector<std::array<float, 4>> sum(iw * ih, {0, 0, 0, 0});
-    for (size_t ti = 0; ti < nt; ti++) {
+    auto put = [&](size_t ti) {
         const Tile &t = layout.tiles[ti];
         const TileLight &l = *lights[ti];
         for (size_t y = 0; y < t.h; y++)
@@ -571,13 +663,26 @@ Bake bake(const Scene &scene, Tracer &gpu, const Options &o) {
                 size_t i = y * t.w + x;
                 if (l.known[i] == 0) continue;
                 size_t ax = t.x + x, ay = t.y + y;
-                out.direct[ay * aw + ax] = {l.field[i], l.ao[i]};
-                out.validity[ay * aw + ax] = l.state[i];
+                dpart[ay * aw + ax] = {l.field[i], l.ao[i]};
+                vpart[ay * aw + ax] = l.state[i];
+                kpart[ay * aw + ax] = 1;
                 float k = l.known[i] == 2 ? 1.0f : 1e-3f;
                 auto &s = sum[(ay / ds) * iw + ax / ds];
                 for (int c = 0; c < 3; c++) s[c] += l.indirect[i][c] * k;
                 s[3] += k;
             }
+    };
+    for (auto &w : work) put(w.tile);
+    sum_words(dpart.data(), dpart.size() * 2);
+    sum_words(vpart.data(), vpart.size() / 4);
+    sum_words(kpart.data(), kpart.size() / 4);
+    sum_words(sum.data(), sum.size() * 4);
+    for (size_t ti : cached) put(ti);
+    out.direct.resize(aw * ah);
+    out.validity.resize(aw * ah);
+    for (size_t a = 0; a < aw * ah; a++) {
+        out.direct[a] = kpart[a] ? dpart[a] : std::array<float, 2>{1.0f, 1.0f};
+        out.validity[a] = vpart[a];
     }
     out.indirect.resize(iw * ih);
     std::vector<uint8_t> has(iw * ih);
@@ -612,8 +717,8 @@ Bake bake(const Scene &scene, Tracer &gpu, const Options &o) {
     }
     stats.t_composite = since(tc);
     stats.tiles = nt;
-    stats.tiles_baked = work.size();
-    stats.texels_baked = covered_list.size();
+    stats.tiles_baked = dirty.size();
+    stats.texels_baked = covered_all;
     stats.chunks = volume ? volume->chunks : 0;
     stats.chunks_baked = volume ? volume->chunks_baked : 0;
     stats.seconds = since(started);

@@ -88,7 +88,15 @@ struct Options {  // bake.rs:30-34
     std::string cache;  // empty: none
     std::function<void(const std::string &)> log;
     bool watertight = false;  // beyond the reference: the watertight triangle test (Tracer::watertight)
+    // beyond the reference: a bake split over `world` processes, this one rank `rank`. sum: the ranks'
+    // element-wise sum of 32-bit words in place (data in host memory, or in device memory when `device`)
+    int rank = 0, world = 1;
+    std::function<void(void *data, size_t words, bool device)> sum;
 };
+
+// One rank's share of items with these costs: a contiguous range [first, last) of them, the ranges of
+// ranks 0 .. world-1 following one another and splitting the total cost as evenly as whole items allow.
+std::pair<size_t, size_t> shard_range(const std::vector<uint64_t> &cost, int rank, int world);
 
 // The inputs every pass needs, built once per bake.
 struct Prepared {

@@ -88,6 +88,15 @@ lb::Options options(const lb_bake_options *o) {
         opt.log = [fn, ctx](const std::string &s) { fn(ctx, s.c_str()); };
     }
     if (o) opt.watertight = o->watertight != 0;
+    if (o && o->exchange && o->exchange->world > 1) {
+        const lb_exchange *ex = o->exchange;
+        if (!ex->sum || ex->rank < 0 || ex->rank >= ex->world) throw std::runtime_error("lb_exchange: bad rank or no sum");
+        opt.rank = ex->rank;
+        opt.world = ex->world;
+        opt.sum = [ex](void *data, size_t words, bool device) {
+            if (ex->sum(ex->ctx, data, words, device ? 1 : 0) != 0) throw std::runtime_error("lb_exchange: sum failed");
+        };
+    }
     return opt;
 }
 

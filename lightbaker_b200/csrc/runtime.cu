@@ -309,8 +309,10 @@ int lb_run(lb_gpu *g, lb_scene *s, int pass, const lb_params *params, const lb_t
     }
     lb_params P = *params;
     P.counts[3] = uint32_t(n);
-    P.atlas[2] = 0;
-    rc = lb_run_device(g, s, pass, P, (const float4 *)g->items.ptr, uint32_t(n), 0, (const float4 *)g->light.ptr,
+    // one launch over the whole list: item i keyed by atlas.z + i (0 in the bake's Params; a shard passes its
+    // first item's index in the whole list)
+    const uint32_t base = params->atlas[2];
+    rc = lb_run_device(g, s, pass, P, (const float4 *)g->items.ptr, uint32_t(n), base, (const float4 *)g->light.ptr,
                        uint32_t(nl), (float4 *)g->out.ptr);
     if (rc != LB_OK) return rc;
     LB_CUDA(cudaMemcpyAsync(out, g->out.ptr, n * width * 16, cudaMemcpyDeviceToHost, g->stream), "copy results");

@@ -511,8 +511,11 @@ int or_run_ex(int pass, const lb_node *nodes, size_t n_nodes, const lb_tri *tris
 #pragma omp for schedule(dynamic, 16)
         for (long long i = 0; i < (long long)n; i++) {
             float *o = out + size_t(i) * width * 4;
-            if (pass == LB_PASS_DIRECT) direct_item(C, items[i], uint32_t(i), o);
-            else if (pass == LB_PASS_GATHER) gather_item(C, items[i], uint32_t(i), o);
+            // the shader keys item i of a dispatch by P.atlas.z + i (trace.wgsl:172-173): the item's index in the
+            // whole list (Gpu::run sets atlas.z to each batch's first, gpu/mod.rs:160-166)
+            uint32_t index = params->atlas[2] + uint32_t(i);
+            if (pass == LB_PASS_DIRECT) direct_item(C, items[i], index, o);
+            else if (pass == LB_PASS_GATHER) gather_item(C, items[i], index, o);
             else volume_item(C, items[i], o);
         }
         if (counters) {
@@ -742,7 +745,7 @@ int or_gather_records(const lb_node *nodes, size_t n_nodes, const lb_tri *tris, 
         const lb_texel &tx = items[k];
         V3<float> nrm = f3(tx.normal), pos = f3(tx.pos), dx = f3(tx.dx), dy = f3(tx.dy);
         Frame f = frame(nrm);
-        uint32_t key = uint32_t(k) * 7919u;
+        uint32_t key = (P->atlas[2] + uint32_t(k)) * 7919u;
         float s1 = rnd(key, 11u, C.seed), s2 = rnd(key, 13u, C.seed);
         for (uint32_t r = 0; r < rays; r++) {
             float jx = rnd(key + r, 19u, C.seed) - 0.5f, jy = rnd(key + r, 23u, C.seed) - 0.5f;
