@@ -4,9 +4,11 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <set>
 #include <stdexcept>
+#include <thread>
 
 #include "cache.h"
 #include "deps.h"
@@ -150,13 +152,31 @@ void Volume::irradiance(Vec3 p, Vec3 n, float e[3], float &sun) const {
 Prepared prepare(const Scene &scene) {
     const SceneHeader &h = scene.header;
     const BakeSettings &b = h.bake;
-    Prepared P{Layout::build(scene), {}, {}, {}, {}, {}, {}, 0};
+    // The layout and the BVH at once: the tree's splits do not depend on the charts, so the BVH is built
+    // beside the layout and the triangles' chart bits written in afterwards (the same bytes).
+    Prepared P{Layout(), {}, {}, {}, {}, {}, {}, 0};
+    std::exception_ptr layout_error;
+    std::thread layout_thread([&]() {
+        try {
+            P.layout = Layout::build(scene);
+        } catch (...) {
+            layout_error = std::current_exception();
+        }
+    });
+    try {
+        P.bvh = Bvh::build(scene, [](size_t, size_t) { return 0xffffffffu; });
+    } catch (...) {
+        layout_thread.join();
+        throw;
+    }
+    layout_thread.join();
+    if (layout_error) std::rethrow_exception(layout_error);
+    P.bvh.set_charts([&](size_t m, size_t t) { return P.layout.tri_chart[m][t]; });
     P.chart_tile = P.layout.chart_tile();
     for (size_t i = 0; i < P.layout.charts.size(); i++) {
         auto a = P.layout.charts[i].affine(P.layout.tiles[P.chart_tile[i]], P.layout.density, P.layout.padding);
         for (auto &r : a) P.affines.insert(P.affines.end(), r.begin(), r.end());
     }
-    P.bvh = Bvh::build(scene, [&](size_t m, size_t t) { return P.layout.tri_chart[m][t]; });
     for (auto &m : h.materials) P.materials.insert(P.materials.end(), {m.albedo[0], m.albedo[1], m.albedo[2], m.opacity});
     P.sun = v3(h.sun.direction).normalize();
     P.g = uint32_t(std::sqrt(float(b.sun_samples)));

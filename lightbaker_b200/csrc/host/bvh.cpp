@@ -115,17 +115,29 @@ bool best_split(const Prim *p, size_t n, int &axis_out, float &at_out) {
                 bmax[b] = bmax[b].max(tmax[size_t(k) * BINS + b]);
                 bn[b] += tn[size_t(k) * BINS + b];
             }
+        // the bins' bounds and counts below and from each plane, swept once each way: min and max give the
+        // reference's per-plane folds (bvh.rs:135-137) up to the sign of a zero, which no area changes
+        // (max - min and its clamp at 0 are the same for either zero), so every cost compares the same
+        Vec3 lo_min[BINS], lo_max[BINS], hi_min[BINS], hi_max[BINS];
+        uint32_t lo_n[BINS], hi_n[BINS];
+        {
+            Vec3 mn = Vec3::splat(INFINITY), mx = Vec3::splat(-INFINITY);
+            uint32_t c = 0;
+            for (size_t b = 0; b < BINS; b++) {
+                lo_min[b] = mn, lo_max[b] = mx, lo_n[b] = c;  // bins [0, b)
+                bounds_add(mn, mx, bmin[b], bmax[b]);
+                c += bn[b];
+            }
+            mn = Vec3::splat(INFINITY), mx = Vec3::splat(-INFINITY), c = 0;
+            for (size_t b = BINS; b-- > 0;) {
+                bounds_add(mn, mx, bmin[b], bmax[b]);
+                c += bn[b];
+                hi_min[b] = mn, hi_max[b] = mx, hi_n[b] = c;  // bins [b, BINS)
+            }
+        }
         for (size_t s = 1; s < BINS; s++) {
-            uint32_t ln = 0, rn = 0;
-            Vec3 lmin = Vec3::splat(INFINITY), lmax = Vec3::splat(-INFINITY), rmin = lmin, rmax = lmax;
-            for (size_t b = 0; b < s; b++) {
-                ln += bn[b];
-                bounds_add(lmin, lmax, bmin[b], bmax[b]);
-            }
-            for (size_t b = s; b < BINS; b++) {
-                rn += bn[b];
-                bounds_add(rmin, rmax, bmin[b], bmax[b]);
-            }
+            uint32_t ln = lo_n[s], rn = hi_n[s];
+            Vec3 lmin = lo_min[s], lmax = lo_max[s], rmin = hi_min[s], rmax = hi_max[s];
             if (ln == 0 || rn == 0) continue;
             float cost = float(ln) * area(lmin, lmax) + float(rn) * area(rmin, rmax);
             if (!have || cost < best_cost) {
@@ -221,6 +233,7 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
         out.nodes[0] = lb_node{{FLT_MAX, FLT_MAX, FLT_MAX}, 0, {-FLT_MAX, -FLT_MAX, -FLT_MAX}, 0};
         out.tris.push_back(lb_tri{});
         out.verts.assign(9, 0.0f);
+        out.source.assign(1, {0xffffffffu, 0xffffffffu});
         return out;
     }
     // The serial walk below (bvh.rs:62-104) pops a node, decides it a leaf or splits its primitives in
@@ -312,9 +325,11 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
     }
     out.tris.reserve(prims.size());
     for (auto &p : prims) out.tris.push_back(sources[p.id].tri);
+    out.source.resize(prims.size());
     out.verts.resize(prims.size() * 9);
     for (size_t i = 0; i < prims.size(); i++) {
         const Source &src = sources[prims[i].id];
+        out.source[i] = {src.mesh, src.index};
         const std::vector<Vec3> &p = scene.positions[src.mesh];
         for (int k = 0; k < 3; k++) {
             Vec3 v = p[size_t(src.index) * 3 + k];
@@ -324,6 +339,11 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
         }
     }
     return out;
+}
+
+void Bvh::set_charts(const std::function<uint32_t(size_t, size_t)> &chart) {
+    for (size_t i = 0; i < tris.size(); i++)
+        if (source[i][0] != 0xffffffffu) tris[i].e1[3] = u2f(chart(source[i][0], source[i][1]));
 }
 
 }  // namespace lb
