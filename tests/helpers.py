@@ -4,10 +4,6 @@ import math
 import numpy as np
 
 
-def ground_texel(scene_positions_ground, prepared_charts, tri_chart_ground, tiles_of_chart, width, x, z):
-    raise NotImplementedError
-
-
 def affine_texel(chart_rows, p):
     """floor of a chart's affine rows applied to a world point: (atlas x, atlas y)."""
     r0, r1 = chart_rows[:4], chart_rows[4:]
