@@ -175,6 +175,9 @@ class Gpu:
         """The warp kernels' ray order (see include/lightbaker.h lb_set_ray_order). Same results."""
         N.check(N.lib().lb_set_ray_order(self._h, int(direct), int(gather)), "lb_set_ray_order")
 
+    def set_fetch(self, on: bool) -> None:
+        N.check(N.lib().lb_set_fetch(self._h, int(bool(on))), "lb_set_fetch")
+
     def set_refill(self, on: bool) -> None:
         """Lane refill in the warp kernels (occlusion and gather rays over the BVH2). Same results."""
         N.check(N.lib().lb_set_refill(self._h, int(on)), "lb_set_refill")

@@ -415,7 +415,7 @@ void build(lb_plan &p) {
     p.enc_rgb.alloc(size_t(p.iw) * p.ih * 4);
     p.enc_vol.alloc(NP * 16);
     p.enc_scale.alloc(4);
-    p.counters.alloc(12 * 8);
+    p.counters.alloc(16 * 8);  // rays, nodes, tris, mats of each pass; then the passes' work counters
     // the first bounce's gather records, which the later bounces evaluate instead of tracing again (their
     // rays are the first bounce's: the keys depend on the gathered texel, not the bounce), and theta at the
     // scene's own values for that evaluation
@@ -498,9 +498,10 @@ void autotune(lb_plan &p) {
     std::string report;
     for (int pass : {LB_PASS_DIRECT, LB_PASS_GATHER}) {
         float best = 1e30f;
-        int best_order = 8, best_blocks = 0, best_bvh = 2, best_refill = 0, best_near = 0, best_occ = 0;
+        int best_order = 8, best_blocks = 0, best_bvh = 2, best_refill = 0, best_near = 0, best_occ = 0, best_fetch = 0;
         for (const Shape &sh : shapes)
-        for (int order : orders) {
+        for (int order : orders)
+        for (int fetch : {0, 1}) {
             WarpPass probe{};
             probe.S = &S;
             probe.pass = pass;
@@ -530,6 +531,7 @@ void autotune(lb_plan &p) {
                 w.refill = sh.refill;
                 w.near = sh.near;
                 w.occ = sh.occ;
+                w.work = fetch ? reinterpret_cast<unsigned int *>(p.counters.as<unsigned long long>() + 12) : nullptr;
                 float t = 0;
                 for (int rep = 0; rep < 2; rep++) {
                     ck(cudaEventRecord(e0, st), "autotune");
@@ -546,6 +548,7 @@ void autotune(lb_plan &p) {
                     best_refill = sh.refill;
                     best_near = sh.near;
                     best_occ = sh.occ;
+                    best_fetch = fetch;
                 }
             }
         }
@@ -556,6 +559,7 @@ void autotune(lb_plan &p) {
             p.refill_direct = best_refill;
             p.near_direct = best_near;
             p.occ_direct = best_occ;
+            p.fetch_direct = best_fetch;
         } else {
             p.group_gather = best_order;
             p.blocks_gather = best_blocks;
@@ -563,10 +567,12 @@ void autotune(lb_plan &p) {
             p.refill_gather = best_refill;
             p.near_gather = best_near;
             p.occ_gather = best_occ;
+            p.fetch_gather = best_fetch;
         }
         report += std::string(pass == LB_PASS_DIRECT ? "direct" : "gather") + ": bvh " + std::to_string(best_bvh) +
                   ", refill " + std::to_string(best_refill) + ", near " + std::to_string(best_near) + ", order " +
-                  std::to_string(best_order) + ", register cap " + std::to_string(best_occ) + ", " +
+                  std::to_string(best_order) + ", register cap " + std::to_string(best_occ) + ", fetch " +
+                  std::to_string(best_fetch) + ", " +
                   std::to_string(best_blocks / std::max(1, p.g->sms)) + " blocks/SM (" + std::to_string(best) +
                   " ms on " + std::to_string(sample.size()) + " texels); ";
     }
@@ -611,6 +617,7 @@ void capture(lb_plan &p) {
             w.refill = p.refill_direct;
             w.near = p.near_direct;
             w.occ = p.occ_direct;
+            w.work = p.fetch_direct ? reinterpret_cast<unsigned int *>(cnt + 12) : nullptr;
             ck(lb_launch_pass_warp(w, st), "direct pass");
         }
         ck(lb_post_direct(a, int(h.lightmap.padding) + 4, s, st), "direct texel passes");
@@ -637,6 +644,7 @@ void capture(lb_plan &p) {
             gw.refill = p.refill_gather;
             gw.near = p.near_gather;
             gw.occ = p.occ_gather;
+            gw.work = p.fetch_gather ? reinterpret_cast<unsigned int *>(cnt + 13) : nullptr;
             bool replay = p.reuse && b.gi_bounces > 1, record = replay || p.keep_records;
             if (replay && bounce > 0) {
                 // the same rays met the same surfaces: evaluate the first bounce's records against this

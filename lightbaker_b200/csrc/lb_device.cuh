@@ -218,13 +218,27 @@ __device__ __forceinline__ bool tri_hit(const Scene &S, uint32_t ref, float4 v0,
     return true;
 }
 
+// Three-way max and min in one instruction each (sm_100's three-source max.f32 / min.f32): the values
+// of max(max(a, b), c) and min(min(a, b), c); only the sign of a zero result can differ, and the walk
+// only compares these distances.
+__device__ __forceinline__ float max3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // trace.wgsl:74-80; the watertight walks (WT) scale the exit distance by `grow`
 template <bool WT = false>
 __device__ __forceinline__ float box(float3 o, float3 inv, float4 mn, float4 mx, float tmax, float grow = 1.0f) {
     float ax = (mn.x - o.x) * inv.x, ay = (mn.y - o.y) * inv.y, az = (mn.z - o.z) * inv.z;
     float bx = (mx.x - o.x) * inv.x, by = (mx.y - o.y) * inv.y, bz = (mx.z - o.z) * inv.z;
-    float lo = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
-    float hi = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+    float lo = max3(fminf(ax, bx), fminf(ay, by), fminf(az, bz));
+    float hi = min3(fmaxf(ax, bx), fmaxf(ay, by), fmaxf(az, bz));
     if (WT) hi = hi * grow;
     float l0 = fmaxf(lo, 0.0f);
     return (hi >= l0 && lo < tmax) ? l0 : FAR;

@@ -43,6 +43,8 @@ struct WarpPass {
     int occ;                  // BVH2 direct and gather passes without counting: 3 or 4 caps registers so that
                               // this many 256-thread blocks fit an SM; else the compiler's own budget
     uint2 *rec;               // optional (gather): every ray's outcome, [item][ray] (lb_device.cuh gather_record)
+    unsigned int *work;       // optional (direct, gather): a counter the launch zeroes, from which warps take
+                              // their next item as they free up; null: a static stride over the items
 };
 // The gather records evaluated against a light atlas and theta (albedo 3 a material, zenith, horizon,
 // ground, sun scale; transport.cu): each item's gather result, its terms summed in ray order, equal to

@@ -128,6 +128,16 @@ __device__ __forceinline__ bool inside_list(const Scene &S, const lb_params &P, 
     return nb / 16.0f > __uint_as_float(P.atlas[3]);
 }
 
+// The item a warp takes next. With a work counter (zeroed before the launch) every warp takes the next item
+// not yet taken as soon as it is free, so warps behind heavy items (texels whose inside tests retry, long
+// escaping rays) no longer hold up the pass's end; without one, a static stride. Called by the whole warp.
+__device__ __forceinline__ uint32_t take_item(unsigned int *work, uint32_t k, uint32_t step, int lane) {
+    if (!work) return k + step;
+    uint32_t v = 0;
+    if (lane == 0) v = atomicAdd(work, 1u);
+    return __shfl_sync(FULL, v, 0);
+}
+
 template <bool COUNT>
 __device__ __forceinline__ void flush_counts(Count &c, unsigned long long *counters) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -153,7 +163,8 @@ __device__ __forceinline__ void flush_counts(Count &c, unsigned long long *count
 template <int BVH, bool COUNT, int OCC = 1, int WALK = 0, bool WT = false>
 __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
-                                                   unsigned long long *counters, int group, int refill, int near) {
+                                                   unsigned long long *counters, int group, int refill, int near,
+                                                   unsigned int *work) {
     // each occlusion ray's term by ray index (0 for a miss: adding it to the sum changes no bit, as the sum
     // starts at +0 and every term is >= 0); before the rays, the ball query's scratch
     __shared__ float s_term[WARPS][AO_CAP];
@@ -167,7 +178,8 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
     const uint32_t seed = __float_as_uint(P.reach[3]);
     Count c;
     c.zero();
-    for (uint32_t k = warp; k < n; k += warps) {
+    const uint32_t first = work ? take_item(work, 0, 0, lane) : warp;
+    for (uint32_t k = first; k < n; k = take_item(work, k, warps, lane)) {
         Item it = load_item(tex, idx, nullptr, k);
         float3 nrm = xyz(it.nrm), pos = xyz(it.pos), dx = xyz(it.dx), dy = xyz(it.dy);
         uint32_t key = (base + k) * 7919u;
@@ -399,7 +411,7 @@ template <int BVH, bool COUNT, int OCC = 1, int WALK = 0, bool WT = false>
 __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) gather_warp(
     Scene S, lb_params P, const float4 *tex, const uint32_t *idx, const float4 *pos_override, const uint32_t *n_dev,
     uint32_t n_host, uint32_t base, const float4 *light, uint32_t n_light, float4 *out, unsigned long long *counters,
-    int group, int refill, uint2 *rec) {
+    int group, int refill, uint2 *rec, unsigned int *work) {
     constexpr int LW = (BVH == 2 && WALK == 1) ? WARPS : 1;  // the leaf lists' shared memory, when used
     __shared__ float3 s_term[WARPS][GI_CAP];
     __shared__ uint8_t s_on[WARPS][GI_CAP];
@@ -413,7 +425,8 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) gather_warp(
     const uint32_t seed = __float_as_uint(P.reach[3]);
     Count c;
     c.zero();
-    for (uint32_t k = warp; k < n; k += warps) {
+    const uint32_t first = work ? take_item(work, 0, 0, lane) : warp;
+    for (uint32_t k = first; k < n; k = take_item(work, k, warps, lane)) {
         Item it = load_item(tex, idx, pos_override, k);
         float3 nrm = xyz(it.nrm), pos = xyz(it.pos), dx = xyz(it.dx), dy = xyz(it.dy);
         Frame f = frame(nrm);
@@ -697,12 +710,12 @@ void launch_walk(const WarpPass &w, int blocks, cudaStream_t stream) {
     switch (w.pass) {
     case LB_PASS_DIRECT:
         lbd::direct_warp<BVH, COUNT, OCC, WALK, WT><<<blocks, T, 0, stream>>>(
-            *w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base, w.out, w.counters, w.group, w.refill, w.near);
+            *w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base, w.out, w.counters, w.group, w.refill, w.near, w.work);
         break;
     case LB_PASS_GATHER:
         lbd::gather_warp<BVH, COUNT, OCC, WALK, WT><<<blocks, T, 0, stream>>>(
             *w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host, w.base, w.light, w.n_light, w.out, w.counters, w.group,
-            w.refill, w.rec);
+            w.refill, w.rec, w.work);
         break;
     default:
         lbd::volume_warp<BVH, COUNT, WT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light,
@@ -770,6 +783,10 @@ cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream) {
         uint32_t need = (w.n_host + (T / 32) - 1) / (T / 32);
         if (need == 0) return cudaSuccess;
         if ((uint32_t)blocks > need) blocks = (int)need;
+    }
+    if (w.work && w.pass != LB_PASS_VOLUME) {
+        cudaError_t e = cudaMemsetAsync(w.work, 0, sizeof(unsigned int), stream);
+        if (e != cudaSuccess) return e;
     }
     if (capped(w)) {
         if (w.occ == 3) launch<2, false, 3>(w, blocks, stream);

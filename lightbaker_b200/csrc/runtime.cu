@@ -376,6 +376,12 @@ int lb_set_register_cap(lb_gpu *g, int blocks) {
     return LB_OK;
 }
 
+int lb_set_fetch(lb_gpu *g, int on) {
+    if (!g) return LB_EINVAL;
+    g->fetch = on != 0;
+    return LB_OK;
+}
+
 int lb_set_refill(lb_gpu *g, int on) {
     if (!g) return LB_EINVAL;
     g->refill = on != 0;
@@ -435,6 +441,8 @@ int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const fl
         w.refill = g->refill;
         w.near = g->near;
         w.occ = g->occ;
+        // the work counter: the handle's counter slot 4 (slots 4..7 of its 8 are otherwise unused)
+        w.work = g->fetch ? reinterpret_cast<unsigned int *>(g->counters + 4) : nullptr;
         LB_CUDA(lb_launch_pass_warp(w, g->stream), "pass launch");
     } else {
         LB_CUDA(lb_launch_pass_bvh2(pass, S, P, items, n, base, light, n_light, out, g->counters, g->counting,

@@ -168,3 +168,35 @@ def test_bake_matches_oracle_bake(gpu, oracle_mod):
     assert np.array_equal(a.volume.view(np.uint32), b.volume.view(np.uint32))
     assert a.stats.rays == b.stats.rays
     assert a.write()[64:] != b""
+
+
+@pytest.mark.parametrize("near", [0, 1])
+@pytest.mark.parametrize("name,limit", [("small_map", 12000), ("map_100m", 3000)])
+def test_dynamic_fetch_bit_exact(gpu, oracle_mod, name, limit, near):
+    """Warps taking their next item from a work counter (lb_set_fetch) give the same records: an item's
+    keys are its index in the list, whichever warp takes it."""
+    scene = scenes.WORKLOADS[name]()
+    P = lb.prepare(scene)
+    buffers = gpu.scene(P.nodes, P.tris, P.materials, P.charts)
+    sc = oracle_mod.Scene.of(P)
+    rng = np.random.default_rng(5)
+    items = P.covered_texels()
+    items = items[np.sort(rng.choice(len(items), size=min(limit, len(items)), replace=False))]
+    gpu.set_pass_kernel(1)
+    gpu.set_near(near)
+    gpu.set_fetch(True)
+    try:
+        for rep in range(2):  # the counter starts again from zero at every launch
+            g = gpu.run(lb.Pass.DIRECT, buffers, P.params, items)
+            c, _ = oracle_mod.run(0, sc, P.params, items)
+            _compare(g, c, f"{name} direct, fetch")
+            light = _light_for(P, rng)
+            gi = items[: limit // 4]
+            g = gpu.run(lb.Pass.GATHER, buffers, P.params, gi, light)
+            c, _ = oracle_mod.run(1, sc, P.params, gi, light)
+            _compare(g, c, f"{name} gather, fetch")
+    finally:
+        gpu.set_fetch(False)
+        gpu.set_pass_kernel(0)
+        gpu.set_near(1)
+        buffers.close()
