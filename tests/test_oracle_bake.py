@@ -70,3 +70,26 @@ def test_bvh_equals_oracle_build(name):
     nodes, tris = build_bvh(s, P.layout())
     assert_same("nodes", nodes.reshape(-1), P.nodes.view(np.uint32).reshape(-1))
     assert_same("triangles", tris.reshape(-1), P.tris.view(np.uint32).reshape(-1))
+
+
+@pytest.mark.parametrize("name", ["opacity", "casts_only", "degenerate", "no_bounce", "night", "inside"])
+def test_edge_scenes_equal_oracle_bake(name):
+    """The edge scenes (tests/edge_scenes.py): the opacity coin, casters that are not laid out and receivers
+    that cast nothing, degenerate and sub-texel triangles, no bounce, no sun, texels inside solids. The host
+    pipeline on the oracle's tracer equals the oracle's whole bake, BVH included."""
+    from edge_scenes import EDGE_SCENES
+    from oracle.bake_ref import build_bvh
+    s = EDGE_SCENES[name]()
+    P = lb.prepare(s)
+    nodes, tris = build_bvh(s, P.layout())
+    assert_same("nodes", nodes.reshape(-1), P.nodes.view(np.uint32).reshape(-1))
+    assert_same("triangles", tris.reshape(-1), P.tris.view(np.uint32).reshape(-1))
+    ob = OracleBake(s, P)
+    t, keep = oracle.tracer()
+    hb = lb.bake_with(s, t)
+    assert_same("direct atlas", ob.direct, hb.direct)
+    assert_same("validity", ob.validity, hb.validity)
+    assert_same("indirect atlas", ob.indirect, hb.indirect)
+    if ob.volume is not None or hb.volume is not None:
+        assert_same("volume", ob.volume, hb.volume)
+    assert ob.rays["direct"] == hb.stats.rays_direct and ob.rays["gather"] == hb.stats.rays_gather

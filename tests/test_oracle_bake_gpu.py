@@ -226,3 +226,18 @@ def test_map_100m_last_bounce_filters_per_tile(map100):
 
 def test_map_100m_light_fallback_and_composite(map100):
     assert check_light_fallback_composite(map100) > 0
+
+
+@pytest.mark.parametrize("name", ["opacity", "casts_only", "degenerate", "no_bounce", "night", "inside"])
+def test_device_bake_edge_scenes_equal_oracle_bake(gpu, name):
+    """The edge scenes (tests/edge_scenes.py) through the device-resident bake and through the drop-in bake on
+    the GPU: both equal the oracle's whole bake bit for bit."""
+    from edge_scenes import EDGE_SCENES
+    s = EDGE_SCENES[name]()
+    ob = OracleBake(s, lb.prepare(s))
+    for b in (lb.bake_device(s, gpu), lb.bake(s, gpu)):
+        assert_same("direct atlas", b.direct, ob.direct)
+        assert_same("validity", b.validity, ob.validity)
+        assert_same("indirect atlas", b.indirect, ob.indirect)
+        if ob.volume is not None:
+            assert_same("volume", b.volume, ob.volume)
