@@ -7,6 +7,7 @@
                  conservative pass, raster.rs:49-51)
   no_bounce      giBounces 0 (no gather pass), no volume
   night          the sun below the horizon (no sun ray is cast), one bounce from the sky alone
+  nothing_received / nothing_casts   no chart at all; the empty BVH
   inside         boxes sunk into each other and into the ground, and a plate just under a box's top: texels
                  inside solids, sample points moved and pushed, the volume's fallback
 """
@@ -90,5 +91,19 @@ def inside():
     return S._assemble(groups, mats, SUN, SKY, _lightmap(), bake, vol)
 
 
+def nothing_received():
+    """No material receives: no chart, no tile, an atlas of padding only (every texel its default)."""
+    mats = [S._material("ground", [0.5, 0.5, 0.5], receives=False)]
+    return S._assemble([("ground", 0, ground())], mats, SUN, SKY, _lightmap(), S._defaults_bake(), None)
+
+
+def nothing_casts():
+    """No material casts: the reference's empty BVH (one leaf nothing reaches); every ray escapes."""
+    mats = [S._material("ground", [0.5, 0.5, 0.5], casts=False)]
+    vol = {"min": [0.5, 0.5, 0.5], "max": [11.5, 2.5, 11.5], "step": 2.0, "rays": 16}
+    return S._assemble([("ground", 0, ground())], mats, SUN, SKY, _lightmap(), S._defaults_bake(aoRays=16, giRays=16),
+                       vol)
+
+
 EDGE_SCENES = {"opacity": opacity, "casts_only": casts_only, "degenerate": degenerate, "no_bounce": no_bounce,
-               "night": night, "inside": inside}
+               "night": night, "inside": inside, "nothing_received": nothing_received, "nothing_casts": nothing_casts}

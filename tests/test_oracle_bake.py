@@ -72,7 +72,8 @@ def test_bvh_equals_oracle_build(name):
     assert_same("triangles", tris.reshape(-1), P.tris.view(np.uint32).reshape(-1))
 
 
-@pytest.mark.parametrize("name", ["opacity", "casts_only", "degenerate", "no_bounce", "night", "inside"])
+@pytest.mark.parametrize("name", ["opacity", "casts_only", "degenerate", "no_bounce", "night", "inside",
+                                  "nothing_received", "nothing_casts"])
 def test_edge_scenes_equal_oracle_bake(name):
     """The edge scenes (tests/edge_scenes.py): the opacity coin, casters that are not laid out and receivers
     that cast nothing, degenerate and sub-texel triangles, no bounce, no sun, texels inside solids. The host

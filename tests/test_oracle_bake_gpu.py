@@ -228,7 +228,8 @@ def test_map_100m_light_fallback_and_composite(map100):
     assert check_light_fallback_composite(map100) > 0
 
 
-@pytest.mark.parametrize("name", ["opacity", "casts_only", "degenerate", "no_bounce", "night", "inside"])
+@pytest.mark.parametrize("name", ["opacity", "casts_only", "degenerate", "no_bounce", "night", "inside",
+                                  "nothing_received", "nothing_casts"])
 def test_device_bake_edge_scenes_equal_oracle_bake(gpu, name):
     """The edge scenes (tests/edge_scenes.py) through the device-resident bake and through the drop-in bake on
     the GPU: both equal the oracle's whole bake bit for bit."""
