@@ -754,6 +754,7 @@ lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_
     }
     try {
         ck(cudaSetDevice(g->device), "cudaSetDevice");
+        lbplan::DBufScope spares(g);  // the plan's device buffers from (and back to) the handle's spares
         auto p = std::make_unique<lb_plan>();
         p->g = g;
         p->scene = lb::Scene::read(scene, len);

@@ -3,7 +3,10 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "../../include/lightbaker.h"
 
@@ -33,6 +36,11 @@ struct lb_gpu {
     lb_buffer items, out, light, scratch;
     void *stage = nullptr;  // pinned host memory for downloads (lb_host_stage_reserve), kept between calls
     size_t stage_cap = 0;
+    // device buffers a freed plan or transport gave back (plan.h DBuf), kept for the next one: no cudaFree,
+    // which waits for the whole device, between bakes, and no cudaMalloc for a buffer a spare fits
+    std::mutex spare_mu;
+    std::vector<std::pair<void *, size_t>> spare;
+    size_t spare_bytes = 0;
 };
 
 // The scene's buffers (gpu/mod.rs:65-71).
@@ -60,3 +68,9 @@ void lb_buffer_free(lb_buffer &b);
 int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const float4 *items, uint32_t n, uint32_t base,
                   const float4 *light, uint32_t n_light, float4 *out);
 void lb_collect_counters(lb_gpu *g);
+// A spare buffer of at least `bytes` (and not more than twice that, plus 1 MiB) from the handle's spares,
+// its size in *cap, or nullptr.
+void *lb_spare_take(lb_gpu *g, size_t bytes, size_t *cap);
+// Gives a buffer back to the handle's spares once the handle's stream has finished with it (it is
+// synchronised here), or frees it when the spares already hold their limit.
+void lb_spare_give(lb_gpu *g, void *p, size_t cap);

@@ -22,21 +22,41 @@ inline void ck(cudaError_t e, const char *what) {
     if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-// A device allocation freed with its owner.
+// The handle whose spare buffers DBufs allocated on this thread draw on (set by a DBufScope; none: plain
+// cudaMalloc and cudaFree).
+inline thread_local lb_gpu *g_dbuf_gpu = nullptr;
+struct DBufScope {
+    lb_gpu *prev;
+    explicit DBufScope(lb_gpu *g) : prev(g_dbuf_gpu) { g_dbuf_gpu = g; }
+    ~DBufScope() { g_dbuf_gpu = prev; }
+    DBufScope(const DBufScope &) = delete;
+    DBufScope &operator=(const DBufScope &) = delete;
+};
+
+// A device allocation freed with its owner: taken from, and given back to, its handle's spares when it was
+// allocated inside a DBufScope (lb_spare_take / lb_spare_give), else cudaMalloc and cudaFree.
 struct DBuf {
     void *p = nullptr;
-    size_t bytes = 0;
+    size_t bytes = 0, cap = 0;
+    lb_gpu *owner = nullptr;
     DBuf() = default;
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
+    void release() {
+        if (!p) return;
+        if (owner) lb_spare_give(owner, p, cap);
+        else cudaFree(p);
+        p = nullptr;
+    }
     void alloc(size_t n) {
-        if (p) cudaFree(p);
+        release();
         bytes = n ? n : 16;
+        owner = g_dbuf_gpu;
+        if (owner && (p = lb_spare_take(owner, bytes, &cap)) != nullptr) return;
         ck(cudaMalloc(&p, bytes), "cudaMalloc");
+        cap = bytes;
     }
-    ~DBuf() {
-        if (p) cudaFree(p);
-    }
+    ~DBuf() { release(); }
     template <class T> T *as() const { return (T *)p; }
 };
 

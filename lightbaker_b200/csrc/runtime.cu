@@ -72,6 +72,41 @@ void lb_buffer_free(lb_buffer &b) {
     b.cap = 0;
 }
 
+namespace {
+constexpr size_t SPARE_LIMIT = size_t(24) << 30;  // device memory the spares may hold
+}  // namespace
+
+void *lb_spare_take(lb_gpu *g, size_t bytes, size_t *cap) {
+    std::lock_guard<std::mutex> lock(g->spare_mu);
+    size_t best = g->spare.size();
+    for (size_t i = 0; i < g->spare.size(); i++) {
+        size_t c = g->spare[i].second;
+        if (c >= bytes && c <= 2 * bytes + (size_t(1) << 20) && (best == g->spare.size() || c < g->spare[best].second))
+            best = i;
+    }
+    if (best == g->spare.size()) return nullptr;
+    void *p = g->spare[best].first;
+    *cap = g->spare[best].second;
+    g->spare_bytes -= *cap;
+    g->spare[best] = g->spare.back();
+    g->spare.pop_back();
+    return p;
+}
+
+void lb_spare_give(lb_gpu *g, void *p, size_t cap) {
+    if (!p) return;
+    cudaStreamSynchronize(g->stream);
+    {
+        std::lock_guard<std::mutex> lock(g->spare_mu);
+        if (g->spare_bytes + cap <= SPARE_LIMIT) {
+            g->spare.emplace_back(p, cap);
+            g->spare_bytes += cap;
+            return;
+        }
+    }
+    cudaFree(p);
+}
+
 extern "C" {
 
 const char *lb_last_error(void) { return g_error.c_str(); }
@@ -124,6 +159,8 @@ void lb_gpu_close(lb_gpu *g) {
     if (!g) return;
     cudaSetDevice(g->device);
     cudaStreamSynchronize(g->stream);
+    for (auto &s : g->spare) cudaFree(s.first);
+    g->spare.clear();
     lb_buffer_free(g->items);
     lb_buffer_free(g->out);
     lb_buffer_free(g->light);

@@ -1011,6 +1011,7 @@ lb_transport *lb_transport_create(lb_gpu *g, const uint8_t *scene, size_t len, u
     t->plan = p;
     t->g = g;
     try {
+        lbplan::DBufScope spares(g);  // the transport's device buffers from (and back to) the handle's spares
         build(*t, max_checkpoints);
         return t.release();
     } catch (const std::exception &e) {

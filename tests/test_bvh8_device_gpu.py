@@ -62,5 +62,15 @@ def test_device_bvh8_empty_and_big_leaf(gpu):
 def test_upload_rejects_leaf_past_triangles(gpu):
     nodes = np.zeros(1, lb.NODE)
     nodes[0]["first"], nodes[0]["count"] = 0, 5
-    with pytest.raises(lb.LightbakerError, match="leaf reaches past"):
+    with pytest.raises(lb.LightbakerError, match="leaf 0 reaches past the triangle array"):
+        _upload(gpu, nodes, np.zeros(4, lb.TRI))
+
+
+def test_upload_rejects_cyclic_bvh(gpu):
+    """An inner node whose child points back at it would make every walk loop: refused before the upload."""
+    nodes = np.zeros(3, lb.NODE)
+    nodes[0]["first"], nodes[0]["count"] = 1, 0
+    nodes[1]["first"], nodes[1]["count"] = 0, 0
+    nodes[2]["first"], nodes[2]["count"] = 0, 2
+    with pytest.raises(lb.LightbakerError, match="not a tree node"):
         _upload(gpu, nodes, np.zeros(4, lb.TRI))
