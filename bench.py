@@ -469,6 +469,7 @@ def main():
     gpu.set_register_cap(0)
     gpu.set_ray_order(8, 8)
     gpu.set_near(1)
+    gpu.set_fetch(True)
     buffers.close()
     del d_direct, d_gather, d_light, out
 
@@ -604,13 +605,14 @@ def main():
             ks["alg_bytes"], alg_src = ks["kernel_fetch_bytes"], "the kernel's own fetches (no frozen count)"
         achieved = ks["alg_bytes"] / (ks["ms"] / 1e3) / 1e9
         # DRAM bytes a launch from an ncu capture (profiles/traffic.txt: workload kernel bytes source)
-        traffic, traffic_src = None, None
+        # (profiles/traffic.txt: workload kernel dram_bytes l2_bytes simt_efficiency source, a full launch each)
+        traffic, traffic_src, l2_bytes, simt = None, None, None, None
         tfile = ROOT / "profiles" / "traffic.txt"
         if tfile.exists():
             for row in tfile.read_text().splitlines():
                 f = row.split()
-                if len(f) >= 3 and not row.startswith("#") and f[0] == args.workload and f[1] == dom:
-                    traffic, traffic_src = int(f[2]), (f[3] if len(f) > 3 else None)
+                if len(f) >= 6 and not row.startswith("#") and f[0] == args.workload and f[1] == dom:
+                    traffic, l2_bytes, simt, traffic_src = int(f[2]), int(f[3]), float(f[4]), f[5]
         cpu_g, cpu_rays, cpu_secs, cpu_items = cpu_baseline(P, direct, gather, probes, light, args.cpu_seconds)
         line = {
             "metric": "Grays/s", "value": value, "unit": "Grays/s", "n_gpus": world, "steps": args.steps,
@@ -630,6 +632,8 @@ def main():
             "roofline": {"bound": "issue", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic,
                          "dram_frac": (traffic / (ks["ms"] / 1e3) / 1e9 / hbm) if traffic else None,
+                         "l2_gbs": (l2_bytes / (ks["ms"] / 1e3) / 1e9) if l2_bytes else None,
+                         "simt_efficiency": simt,
                          "traffic_source": traffic_src and f"profiles/{traffic_src}, scaled by texels",
                          "kernel": dom, "peak_source": peak_src,
                          "algorithmic_bytes_per_launch": ks["alg_bytes"], "algorithmic_bytes_source": alg_src,

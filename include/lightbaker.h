@@ -190,8 +190,9 @@ int lb_set_register_cap(lb_gpu *gpu, int blocks);
 /* Lane refill in the warp kernels' occlusion and gather rays over the BVH2 (default off): a lane whose
  * ray has ended starts the item's next one instead of waiting for its round. Same results. */
 int lb_set_refill(lb_gpu *gpu, int on);
-/* Dynamic item fetch in the warp kernels' direct and gather passes (default off): each warp takes its next
- * item from a counter as soon as it is free, instead of a static stride over the items. Same results. */
+/* Dynamic item fetch in the warp kernels' direct and gather passes and in lb_bake_device's untuned shapes
+ * (default on): each warp takes its next item from a counter as soon as it is free, instead of a static
+ * stride over the items, so warps behind heavy items no longer hold up the pass's end. Same results. */
 int lb_set_fetch(lb_gpu *gpu, int on);
 /* The BVH the warp kernels walk: 2, the reference's (as uploaded); 8, the 8-wide BVH lb_scene_upload
  * collapses from it (80-byte nodes, 8-bit child boxes). Same hits, faces and records. */

@@ -776,6 +776,7 @@ lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_
         p->bvh_direct = p->bvh_gather = p->bvh_volume = g->bvh;
         p->refill_direct = p->refill_gather = g->refill;
         p->near_direct = p->near_gather = g->near;
+        p->fetch_direct = p->fetch_gather = g->fetch;
         // the gathers default to the 4-block register cap (fastest on B200 for the BVH2 gather walk)
         p->occ_direct = g->occ;
         p->occ_gather = g->occ ? g->occ : 4;

@@ -28,7 +28,7 @@ struct lb_gpu {
     int refill = 0;  // the warp kernels' lane refill (occlusion and gather rays over the BVH2)
     int near = 1;    // the warp kernels' leaf list for occlusion rays (BVH2)
     int occ = 0;     // the warp kernels' register cap (WarpPass::occ)
-    int fetch = 0;   // the warp kernels take items from a work counter (WarpPass::work)
+    int fetch = 1;   // the warp kernels take items from a work counter (WarpPass::work)
     unsigned long long *counters = nullptr;       // device: rays, nodes, tris, mats
     unsigned long long *host_counters = nullptr;  // pinned copy, written by the stream
     lb_counters last = {};
