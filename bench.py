@@ -301,6 +301,7 @@ def kernel_only(args):
     bvh, refill, near, order = walk[:4]
     gpu.set_register_cap(walk[4] if len(walk) > 4 else 0)
     gpu.set_fetch(walk[5] if len(walk) > 5 else 0)
+    gpu.set_warp_walk(walk[6] if len(walk) > 6 else 0)
     gpu.set_bvh(bvh)
     gpu.set_refill(refill)
     gpu.set_near(near)
@@ -348,7 +349,8 @@ def main():
                     help="run one warp-per-item pass over --items texels of the workload, warmup + steps times "
                          "(for profiler captures; prints its own line)")
     ap.add_argument("--items", type=int, default=262144)
-    ap.add_argument("--walk", default="2,0,1,8", help="kernel-only: bvh,refill,near,order[,register cap[,fetch]]")
+    ap.add_argument("--walk", default="2,0,1,8",
+                    help="kernel-only: bvh,refill,near,order[,register cap[,fetch[,warp walk]]]")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -439,6 +441,7 @@ def main():
         gpu.set_register_cap(sh.get("register cap", 0))
         gpu.set_ray_order(sh.get("order", 8), sh.get("order", 8))
         gpu.set_fetch(sh.get("fetch", 0))
+        gpu.set_warp_walk(sh.get("warp walk", 0))
         gpu.set_counting(True)
         gpu.run_async(pass_, buffers, P.params, d_items.data_ptr(), len(items), 0, d_light.data_ptr(), len(light),
                       out.data_ptr())
@@ -470,6 +473,7 @@ def main():
     gpu.set_ray_order(8, 8)
     gpu.set_near(1)
     gpu.set_fetch(True)
+    gpu.set_warp_walk(True)
     buffers.close()
     del d_direct, d_gather, d_light, out
 

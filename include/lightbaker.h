@@ -194,6 +194,13 @@ int lb_set_refill(lb_gpu *gpu, int on);
  * (default on): each warp takes its next item from a counter as soon as it is free, instead of a static
  * stride over the items, so warps behind heavy items no longer hold up the pass's end. Same results. */
 int lb_set_fetch(lb_gpu *gpu, int on);
+/* The warp kernels' direct pass over the BVH2 (default on): a texel's 32 sun rays (16 cells' hard and soft
+ * rays, near-parallel, from within the texel) walk the tree together, one node at a time for the warp, each
+ * lane testing its own ray; lanes leave subtrees their rays miss and the walk when their rays are stopped.
+ * Used when the BVH2 has at most 48 inner nodes on any path (then no per-ray walk drops a child); the
+ * same shadow bits, since whether a shadow ray is stopped does not depend on the order its triangles are
+ * tested in. No counterpart in the reference. */
+int lb_set_warp_walk(lb_gpu *gpu, int on);
 /* The BVH the warp kernels walk: 2, the reference's (as uploaded); 8, the 8-wide BVH lb_scene_upload
  * collapses from it (80-byte nodes, 8-bit child boxes). Same hits, faces and records. */
 int lb_set_bvh(lb_gpu *gpu, int width);

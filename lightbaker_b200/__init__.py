@@ -175,6 +175,9 @@ class Gpu:
         """The warp kernels' ray order (see include/lightbaker.h lb_set_ray_order). Same results."""
         N.check(N.lib().lb_set_ray_order(self._h, int(direct), int(gather)), "lb_set_ray_order")
 
+    def set_warp_walk(self, on: bool) -> None:
+        N.check(N.lib().lb_set_warp_walk(self._h, int(bool(on))), "lb_set_warp_walk")
+
     def set_fetch(self, on: bool) -> None:
         N.check(N.lib().lb_set_fetch(self._h, int(bool(on))), "lb_set_fetch")
 

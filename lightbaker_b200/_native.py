@@ -118,6 +118,7 @@ SIGNATURES = {
     "lb_set_pass_kernel": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_set_ray_order": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "lb_set_bvh": (C.c_int, [C.c_void_p, C.c_int]),
+    "lb_set_warp_walk": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_set_fetch": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_set_refill": (C.c_int, [C.c_void_p, C.c_int]),
     "lb_set_near": (C.c_int, [C.c_void_p, C.c_int]),

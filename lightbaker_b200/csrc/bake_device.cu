@@ -498,10 +498,13 @@ void autotune(lb_plan &p) {
     std::string report;
     for (int pass : {LB_PASS_DIRECT, LB_PASS_GATHER}) {
         float best = 1e30f;
-        int best_order = 8, best_blocks = 0, best_bvh = 2, best_refill = 0, best_near = 0, best_occ = 0, best_fetch = 0;
+        int best_order = 8, best_blocks = 0, best_bvh = 2, best_refill = 0, best_near = 0, best_occ = 0, best_fetch = 0,
+            best_ww = 0;
         for (const Shape &sh : shapes)
         for (int order : orders)
-        for (int fetch : {0, 1}) {
+        for (int fetch : {0, 1})
+        for (int ww : {0, 1}) {
+            if (ww && pass != LB_PASS_DIRECT) continue;
             WarpPass probe{};
             probe.S = &S;
             probe.pass = pass;
@@ -532,6 +535,7 @@ void autotune(lb_plan &p) {
                 w.near = sh.near;
                 w.occ = sh.occ;
                 w.work = fetch ? reinterpret_cast<unsigned int *>(p.counters.as<unsigned long long>() + 12) : nullptr;
+                w.warp_walk = ww;
                 float t = 0;
                 for (int rep = 0; rep < 2; rep++) {
                     ck(cudaEventRecord(e0, st), "autotune");
@@ -549,6 +553,7 @@ void autotune(lb_plan &p) {
                     best_near = sh.near;
                     best_occ = sh.occ;
                     best_fetch = fetch;
+                    best_ww = ww;
                 }
             }
         }
@@ -560,6 +565,7 @@ void autotune(lb_plan &p) {
             p.near_direct = best_near;
             p.occ_direct = best_occ;
             p.fetch_direct = best_fetch;
+            p.warp_walk = best_ww;
         } else {
             p.group_gather = best_order;
             p.blocks_gather = best_blocks;
@@ -572,7 +578,8 @@ void autotune(lb_plan &p) {
         report += std::string(pass == LB_PASS_DIRECT ? "direct" : "gather") + ": bvh " + std::to_string(best_bvh) +
                   ", refill " + std::to_string(best_refill) + ", near " + std::to_string(best_near) + ", order " +
                   std::to_string(best_order) + ", register cap " + std::to_string(best_occ) + ", fetch " +
-                  std::to_string(best_fetch) + ", " +
+                  std::to_string(best_fetch) + (pass == LB_PASS_DIRECT ? ", warp walk " + std::to_string(best_ww) : "") +
+                  ", " +
                   std::to_string(best_blocks / std::max(1, p.g->sms)) + " blocks/SM (" + std::to_string(best) +
                   " ms on " + std::to_string(sample.size()) + " texels); ";
     }
@@ -618,6 +625,7 @@ void capture(lb_plan &p) {
             w.near = p.near_direct;
             w.occ = p.occ_direct;
             w.work = p.fetch_direct ? reinterpret_cast<unsigned int *>(cnt + 12) : nullptr;
+            w.warp_walk = p.warp_walk;
             ck(lb_launch_pass_warp(w, st), "direct pass");
         }
         ck(lb_post_direct(a, int(h.lightmap.padding) + 4, s, st), "direct texel passes");
@@ -777,6 +785,7 @@ lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_
         p->refill_direct = p->refill_gather = g->refill;
         p->near_direct = p->near_gather = g->near;
         p->fetch_direct = p->fetch_gather = g->fetch;
+        p->warp_walk = g->warp_walk;
         // the gathers default to the 4-block register cap (fastest on B200 for the BVH2 gather walk)
         p->occ_direct = g->occ;
         p->occ_gather = g->occ ? g->occ : 4;

@@ -32,6 +32,8 @@ struct Scene {
     // 1 without vertices (the shader's tests, unchanged)
     const float4 *verts = nullptr;
     float grow = 1.0f;
+    // the most inner nodes on any root-to-leaf path of the BVH2 (0xffffffff: not known)
+    uint32_t depth = 0xffffffffu;
 };
 
 constexpr int STACK8 = 96;  // node groups the 8-wide walk can hold (depth x 7 at most)
@@ -298,6 +300,94 @@ __device__ __forceinline__ Hit trace_t(const Scene &S, float3 o, float3 d, float
         nhi = __ldg(&S.nodes[2 * n + 1]);
     }
     return hit;
+}
+
+// The BVH2 depth below which a per-ray walk never drops a child (its stack holds STACK entries and a walk
+// pushes at most one a level): the warp walk below gives the per-ray walk's answers only then.
+constexpr uint32_t WARP_WALK_DEPTH = STACK;
+
+// Any-hit rays of a warp walked together: one traversal of the BVH2 shared by the warp's lanes, each lane
+// with its own ray (`on`: it has one), a stack of (node, lanes) in shared memory (WARP_WALK_DEPTH entries).
+// At an inner node every lane tests its own ray against both children's boxes (trace.wgsl:74-80, the same
+// test as its own walk); the warp opens a child for the lanes whose rays enter it, the first child first,
+// and keeps the other with its lanes. At a leaf each of those lanes tests the triangles for its own ray; a
+// lane whose ray is stopped leaves the traversal. Returns whether the lane's ray escaped.
+//
+// The answer is each ray's own walk's (trace.wgsl:83-130 with `any`): both visit exactly the leaves whose
+// boxes, all the way down, the ray enters (no child is ever dropped: the tree is no deeper than
+// WARP_WALK_DEPTH, which the caller checks), and whether some triangle there stops the ray does not depend
+// on the order they are tested in (the opacity coin is keyed by triangle and ray). Only the order and
+// the work counters differ, so it runs without counting. For rays that start close together and head the
+// same way (a texel's sun rays) the lanes' paths nearly coincide and the warp walks them in step.
+template <bool WT>
+__device__ __forceinline__ bool escapes_warp(const Scene &S, float3 o, float3 d, float tmax, uint32_t ray,
+                                             uint32_t seed, bool on, uint32_t *st_node, uint32_t *st_mask, int lane,
+                                             Count &c) {
+    const unsigned me = 1u << lane;
+    float3 dd = mk(fabsf(d.x) < 1e-12f ? 1e-12f : d.x, fabsf(d.y) < 1e-12f ? 1e-12f : d.y,
+                   fabsf(d.z) < 1e-12f ? 1e-12f : d.z);
+    float3 inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+    if (on) c.rays++;
+    bool stopped = false;
+    unsigned alive = __ballot_sync(0xffffffffu, on);  // lanes with a ray not yet stopped
+    uint32_t node = 0;
+    unsigned mask = alive;
+    int sp = 0;
+    while (alive) {
+        const float4 nlo = __ldg(&S.nodes[2 * node]), nhi = __ldg(&S.nodes[2 * node + 1]);
+        const uint32_t first = __float_as_uint(nlo.w), count = __float_as_uint(nhi.w);
+        bool descend = false;
+        if (count > 0u) {
+            if ((mask & me) && !stopped) {
+                for (uint32_t i = first; i < first + count; i++) {
+                    float4 v0 = __ldg(&S.tris[3 * i]), e1 = __ldg(&S.tris[3 * i + 1]), e2 = __ldg(&S.tris[3 * i + 2]);
+                    float t;
+                    bool bk;
+                    if (!tri_hit<WT>(S, i, v0, e1, e2, o, d, t, bk)) continue;
+                    if (t > 1e-4f && t < tmax && stops<false>(S, i, v0.w, ray, seed, c)) {
+                        stopped = true;
+                        break;
+                    }
+                }
+            }
+            alive &= ~__ballot_sync(0xffffffffu, stopped);
+        } else if (first + 1u < S.n_nodes) {
+            const float4 alo = __ldg(&S.nodes[2 * first]), ahi = __ldg(&S.nodes[2 * first + 1]);
+            const float4 blo = __ldg(&S.nodes[2 * first + 2]), bhi = __ldg(&S.nodes[2 * first + 3]);
+            const bool in = (mask & me) && !stopped;
+            const bool ha = in && box<WT>(o, inv, alo, ahi, tmax, S.grow) < FAR;
+            const bool hb = in && box<WT>(o, inv, blo, bhi, tmax, S.grow) < FAR;
+            const unsigned ma = __ballot_sync(0xffffffffu, ha), mb = __ballot_sync(0xffffffffu, hb);
+            if (ma && mb) {
+                if (sp < int(WARP_WALK_DEPTH)) {
+                    if (lane == 0) {
+                        st_node[sp] = first + 1u;
+                        st_mask[sp] = mb;
+                    }
+                    sp++;
+                }
+                node = first;
+                mask = ma;
+                descend = true;
+            } else if (ma | mb) {
+                node = ma ? first : first + 1u;
+                mask = ma ? ma : mb;
+                descend = true;
+            }
+        }
+        if (descend) continue;
+        // the next kept child that still has a lane whose ray is not stopped
+        __syncwarp();
+        mask = 0;
+        while (sp > 0 && !mask) {
+            sp--;
+            node = st_node[sp];
+            mask = st_mask[sp] & alive;
+        }
+        __syncwarp();
+        if (!mask) break;
+    }
+    return on && !stopped;
 }
 
 template <bool COUNT, bool WT = false>

@@ -45,6 +45,8 @@ struct WarpPass {
     uint2 *rec;               // optional (gather): every ray's outcome, [item][ray] (lb_device.cuh gather_record)
     unsigned int *work;       // optional (direct, gather): a counter the launch zeroes, from which warps take
                               // their next item as they free up; null: a static stride over the items
+    int warp_walk;            // direct pass over the BVH2 without counting: a texel's sun rays walk the tree
+                              // together (lb_device.cuh escapes_warp), when the tree is shallow enough
 };
 // The gather records evaluated against a light atlas and theta (albedo 3 a material, zenith, horizon,
 // ground, sun scale; transport.cu): each item's gather result, its terms summed in ray order, equal to

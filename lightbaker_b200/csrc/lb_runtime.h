@@ -29,6 +29,7 @@ struct lb_gpu {
     int near = 1;    // the warp kernels' leaf list for occlusion rays (BVH2)
     int occ = 0;     // the warp kernels' register cap (WarpPass::occ)
     int fetch = 1;   // the warp kernels take items from a work counter (WarpPass::work)
+    int warp_walk = 1;  // the direct pass's sun rays walk the tree together (WarpPass::warp_walk)
     unsigned long long *counters = nullptr;       // device: rays, nodes, tris, mats
     unsigned long long *host_counters = nullptr;  // pinned copy, written by the stream
     lb_counters last = {};
@@ -50,6 +51,7 @@ struct lb_scene {
     uint32_t n_nodes = 0, n_tris = 0, n_mats = 0, n_charts = 0;
     void *nodes8 = nullptr, *tris8 = nullptr;  // the 8-wide BVH collapsed from the BVH2 (bvh8_build.cu)
     uint32_t n_nodes8 = 0, n_tris8 = 0;
+    uint32_t depth = 0xffffffffu;  // the most inner nodes on a root-to-leaf path of the BVH2
     void *verts = nullptr;  // exact vertices (lb_scene_set_vertices): the watertight triangle test
 };
 

@@ -164,18 +164,22 @@ template <int BVH, bool COUNT, int OCC = 1, int WALK = 0, bool WT = false>
 __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
                                                    unsigned long long *counters, int group, int refill, int near,
-                                                   unsigned int *work) {
+                                                   unsigned int *work, int warp_walk) {
     // each occlusion ray's term by ray index (0 for a miss: adding it to the sum changes no bit, as the sum
     // starts at +0 and every term is >= 0); before the rays, the ball query's scratch
     __shared__ float s_term[WARPS][AO_CAP];
     static_assert(sizeof(s_term[0]) >= 2 * BALL_FRONT * sizeof(uint32_t), "the ball query's scratch fits");
     __shared__ uint32_t s_list[WARPS][BALL_LEAVES];
     __shared__ float s_dist[WARPS][BALL_LEAVES];
+    // the sun rays' shared walk (escapes_warp): its stack of kept children and their lanes
+    constexpr int WW = (BVH == 2 && !COUNT) ? int(WARP_WALK_DEPTH) : 1;
+    __shared__ uint32_t s_ww_node[WARPS][WW], s_ww_mask[WARPS][WW];
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t n = n_dev ? *n_dev : n_host;
     const uint32_t seed = __float_as_uint(P.reach[3]);
+    const bool shared_sun = BVH == 2 && !COUNT && warp_walk && S.depth <= WARP_WALK_DEPTH;
     Count c;
     c.zero();
     const uint32_t first = work ? take_item(work, 0, 0, lane) : warp;
@@ -255,7 +259,24 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
             for (uint32_t s0 = 0; s0 < gg; s0 += 16) {
                 uint32_t s = s0 + uint32_t(lane & 15);
                 bool escaped = false;
-                if (s < gg) {
+                if (shared_sun) {
+                    // the 32 rays (16 cells' hard and soft rays) start within the texel and head within the sun's
+                    // disc: one walk of the BVH2 for the warp
+                    const bool on = s < gg;
+                    float3 o = at, d = sun;
+                    uint32_t ray = key + s;
+                    if (on) {
+                        float cx = ((__uint2float_rn(s % g) + 0.5f) / fg - 0.5f) * span;
+                        float cy = ((__uint2float_rn(s / g) + 0.5f) / fg - 0.5f) * span;
+                        o = add(add(add(at, scl(dx, cx)), scl(dy, cy)), lift);
+                        if (lane >= 16) {
+                            d = sun_disc(P, sf, (s + turn) % gg, gg);
+                            ray = key + s + 1000u;
+                        }
+                    }
+                    const int wi2 = int(threadIdx.x >> 5);
+                    escaped = escapes_warp<WT>(S, o, d, FAR, ray, seed, on, s_ww_node[wi2], s_ww_mask[wi2], lane, c);
+                } else if (s < gg) {
                     float cx = ((__uint2float_rn(s % g) + 0.5f) / fg - 0.5f) * span;
                     float cy = ((__uint2float_rn(s / g) + 0.5f) / fg - 0.5f) * span;
                     float3 o = add(add(add(at, scl(dx, cx)), scl(dy, cy)), lift);
@@ -710,7 +731,8 @@ void launch_walk(const WarpPass &w, int blocks, cudaStream_t stream) {
     switch (w.pass) {
     case LB_PASS_DIRECT:
         lbd::direct_warp<BVH, COUNT, OCC, WALK, WT><<<blocks, T, 0, stream>>>(
-            *w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base, w.out, w.counters, w.group, w.refill, w.near, w.work);
+            *w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base, w.out, w.counters, w.group, w.refill, w.near, w.work,
+            w.warp_walk);
         break;
     case LB_PASS_GATHER:
         lbd::gather_warp<BVH, COUNT, OCC, WALK, WT><<<blocks, T, 0, stream>>>(

@@ -117,6 +117,7 @@ struct lb_plan {
     int near_direct = 1, near_gather = 1;              // leaf lists (direct: occlusion rays; gather: near hits)
     int occ_direct = 0, occ_gather = 0;                // register caps (WarpPass::occ)
     int fetch_direct = 1, fetch_gather = 1;            // items taken from a work counter (WarpPass::work)
+    int warp_walk = 1;                                 // the direct pass's sun rays walk together (WarpPass)
     bool reuse = true;          // later bounces evaluate the first bounce's gather records
     bool keep_records = false;  // record the first bounce's gather rays whatever the bounce count
     uint64_t max_gathered = 0;  // a bound on the gathered texels (records are sized by it)

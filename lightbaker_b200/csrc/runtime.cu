@@ -8,6 +8,7 @@
 // allocated per call.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -243,6 +244,18 @@ lb_scene *lb_scene_upload(lb_gpu *g, const lb_node *nodes, size_t n_nodes, const
     s->n_tris = uint32_t(n_tris);
     s->n_mats = uint32_t(n_materials);
     s->n_charts = uint32_t(n_charts);
+    {
+        // the most inner nodes on a path (children follow their parent: lb_bvh_check), for the warp walks
+        std::vector<uint32_t> d(n_nodes, 0);
+        uint32_t most = 0;
+        for (size_t i = 0; i < n_nodes; i++) {
+            if (nodes[i].count > 0 || uint64_t(nodes[i].first) + 1 >= n_nodes) continue;
+            uint32_t here = d[i] + 1;
+            most = std::max(most, here);
+            d[nodes[i].first] = d[nodes[i].first + 1] = here;
+        }
+        s->depth = most;
+    }
     // the 8-wide BVH over the same triangles, collapsed on the device from the BVH2 just uploaded
     if (lb_bvh8_build(g, s) != LB_OK) {
         lb_scene_free(s);
@@ -260,6 +273,7 @@ lbd::Scene lb_scene_view(const lb_scene *s) {
     S.tris8 = (const float4 *)s->tris8;
     S.verts = (const float4 *)s->verts;
     S.grow = s->verts ? 1.0000004f : 1.0f;
+    S.depth = s->depth;
     return S;
 }
 
@@ -413,6 +427,12 @@ int lb_set_register_cap(lb_gpu *g, int blocks) {
     return LB_OK;
 }
 
+int lb_set_warp_walk(lb_gpu *g, int on) {
+    if (!g) return LB_EINVAL;
+    g->warp_walk = on != 0;
+    return LB_OK;
+}
+
 int lb_set_fetch(lb_gpu *g, int on) {
     if (!g) return LB_EINVAL;
     g->fetch = on != 0;
@@ -478,6 +498,7 @@ int lb_run_device(lb_gpu *g, lb_scene *s, int pass, const lb_params &P, const fl
         w.refill = g->refill;
         w.near = g->near;
         w.occ = g->occ;
+        w.warp_walk = g->warp_walk;
         // the work counter: the handle's counter slot 4 (slots 4..7 of its 8 are otherwise unused)
         w.work = g->fetch ? reinterpret_cast<unsigned int *>(g->counters + 4) : nullptr;
         LB_CUDA(lb_launch_pass_warp(w, g->stream), "pass launch");

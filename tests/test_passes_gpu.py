@@ -200,3 +200,33 @@ def test_dynamic_fetch_bit_exact(gpu, oracle_mod, name, limit, near):
         gpu.set_pass_kernel(0)
         gpu.set_near(1)
         buffers.close()
+
+
+@pytest.mark.parametrize("watertight", [False, True])
+@pytest.mark.parametrize("name,limit", [("small_map", 12000), ("map_100m", 4000), ("uneven_tiles", 4000)])
+def test_warp_walk_sun_rays_bit_exact(gpu, oracle_mod, name, limit, watertight):
+    """A texel's sun rays walked together by the warp (lb_set_warp_walk) give the same shadow bits as their own
+    walks: the direct records equal the oracle's, with the shader's triangle test and the watertight one."""
+    scene = scenes.WORKLOADS[name]() if name != "uneven_tiles" else scenes.uneven_tiles(seed=2, tiles=3)
+    P = lb.prepare(scene)
+    buffers = gpu.scene(P.nodes, P.tris, P.materials, P.charts)
+    if watertight:
+        buffers.set_vertices(P.verts)
+    sc = oracle_mod.Scene.of(P, watertight=watertight)
+    rng = np.random.default_rng(9)
+    items = P.covered_texels()
+    items = items[np.sort(rng.choice(len(items), size=min(limit, len(items)), replace=False))]
+    gpu.set_pass_kernel(1)
+    try:
+        for near in (0, 1):
+            gpu.set_near(near)
+            for ww in (True, False):
+                gpu.set_warp_walk(ww)
+                g = gpu.run(lb.Pass.DIRECT, buffers, P.params, items)
+                c, _ = oracle_mod.run(0, sc, P.params, items)
+                _compare(g, c, f"{name} direct, warp walk {ww}, near {near}")
+    finally:
+        gpu.set_warp_walk(True)
+        gpu.set_near(1)
+        gpu.set_pass_kernel(0)
+        buffers.close()
