@@ -351,6 +351,10 @@ def main():
     ap.add_argument("--items", type=int, default=262144)
     ap.add_argument("--walk", default="2,0,1,8",
                     help="kernel-only: bvh,refill,near,order[,register cap[,fetch[,warp walk]]]")
+    ap.add_argument("--split", action="store_true",
+                    help="N > 1: one map (seed 0) split over the ranks (lb_bake_options.exchange: each rank traces "
+                         "its share of every pass, the outputs summed over NCCL), strong scaling; prints the "
+                         "device bake's line and stops")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -367,7 +371,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
     import lightbaker_b200 as lb
-    scene, P, direct, gather, probes, light = load_workload(args.workload, rank_seed(rank))
+    scene, P, direct, gather, probes, light = load_workload(args.workload, 0 if args.split else rank_seed(rank))
     gpu = lb.Gpu.new(local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.ExternalStream(gpu.stream, device=dev)
@@ -377,7 +381,8 @@ def main():
         return reduce_max(x, dist, dev)
 
     # ---- the device-resident bake: graph replays, inputs resident ----
-    plan = lb.Plan(scene, gpu, autotune=True)
+    exchange = lb.Exchange() if args.split and world > 1 else None
+    plan = lb.Plan(scene, gpu, autotune=True, exchange=exchange)
     tuning = (lb._native.lib().lb_plan_tuning(plan._h) or b"").decode()
     plan.launch()
     gpu.sync()
@@ -410,12 +415,16 @@ def main():
     value = job_value(rays_job, ms_per_step)
     baked = plan.result()
     plan.close()
-    if args.device_only:
-        # for a profiler's launch list: the device bake's steps alone
+    if args.device_only or args.split:
+        # for a profiler's launch list: the device bake's steps alone; or one map split over the ranks (each
+        # step's time includes the sums between the graph's pieces)
         if rank == 0:
             print(json.dumps({"metric": "Grays/s", "value": value, "unit": "Grays/s", "n_gpus": world,
                               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-                              "device_only": True, "autotune": tuning, "graph_kernels": kernels}))
+                              "device_only": True, "autotune": tuning, "graph_kernels": kernels,
+                              "scaling": "strong" if args.split else "weak", "split": bool(args.split),
+                              "config": {"workload": args.workload, "seed": 0 if args.split else "rank"},
+                              "clocks": clock_info}))
         gpu.close()
         if dist is not None:
             dist.destroy_process_group()

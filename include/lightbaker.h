@@ -76,7 +76,8 @@ enum lb_status {
     LB_ENOMEM = -4,    /* device memory */
     /* -5 is not used: no kernel waits on another, and upload refuses a BVH2 a walk could loop in */
     LB_EIO = -6,       /* file or format error */
-    LB_ESCRATCH = -7   /* request larger than a fixed scratch area */
+    LB_ESCRATCH = -7,  /* request larger than a fixed scratch area */
+    LB_EEXCHANGE = -8  /* a split bake's sum (lb_exchange) failed */
 };
 
 typedef struct lb_gpu lb_gpu;
@@ -289,8 +290,9 @@ typedef struct lb_tracer {
                const float *light, size_t n_light, float *out, uint64_t *rays);
 } lb_tracer;
 
-/* How the ranks of a bake split over several processes (one a GPU) exchange what the others need: the
- * light atlas after each bounce, the probes, the atlases' pieces and some counts. No counterpart in the
+/* How the ranks of a bake split over several processes (one a GPU) exchange what the others need (the
+ * drop-in bake: the light atlas after each bounce, the probes, the atlases' pieces and some counts; the
+ * device-resident bake: each ray pass's outputs, in device memory). No counterpart in the
  * reference (one process bakes everything). `sum` adds `count` 32-bit words at `data` element-wise over
  * every rank, in place, as unsigned integers: every exchanged word is written by one rank and zero on
  * the others, so the sum carries that rank's bits exactly (floats included). device: 0 host memory, 1
@@ -314,9 +316,11 @@ typedef struct lb_bake_options {
                                                  * every pass; such tiles are cached apart (default 0: the
                                                  * shader's test) */
     const lb_exchange *exchange;                /* NULL: one process bakes every tile. Else this rank bakes its
-                                                 * share of the dirty tiles (contiguous in tile order, balanced
-                                                 * by their texels) and probe chunks, and every rank returns
-                                                 * the whole bake, equal to one process's bit for bit */
+                                                 * share (lb_bake_run: of the dirty tiles, contiguous in tile
+                                                 * order, balanced by their texels, and of the probe chunks;
+                                                 * lb_bake_device / lb_plan_create: of every ray pass's items,
+                                                 * contiguous, equal counts), and every rank returns the whole
+                                                 * bake, equal to one process's bit for bit */
 } lb_bake_options;
 
 typedef struct lb_bake lb_bake;
@@ -363,7 +367,9 @@ lb_bake *lb_bake_device(lb_gpu *gpu, const uint8_t *scene, size_t len, const lb_
 /* The same in steps, for a caller that rebakes the same dirty set: create (host work, uploads, the
  * graph captured), launch (the graph enqueued on the handle's stream; may be repeated), result (waits,
  * downloads, writes the cache; a bake handle). lb_plan_rays gives the rays of the last launch a pass:
- * direct, gather (all bounces), volume. */
+ * direct, gather (all bounces), volume (a split bake: this rank's). With an exchange the graph is cut
+ * after each ray pass and lb_plan_launch returns once the last piece is enqueued, having synchronised
+ * the stream and made the sums between the pieces (LB_EEXCHANGE when a sum fails). */
 typedef struct lb_plan lb_plan;
 lb_plan *lb_plan_create(lb_gpu *gpu, const uint8_t *scene, size_t len, const lb_bake_options *opts);
 int lb_plan_launch(lb_plan *plan);

@@ -446,11 +446,13 @@ def bake(scene: bytes, gpu: Gpu, cache=None, log=None, watertight: bool = False,
 
 
 def bake_device(scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False, trace_every_bounce=False,
-                watertight=False) -> Bake:
+                watertight=False, exchange: Exchange = None) -> Bake:
     """The device-resident bake: every dirty tile rebaked in one CUDA graph (same results as bake()).
     autotune: time the passes' ray order and grid on a sample of the texels first; trace_every_bounce:
-    trace the gather rays in every bounce instead of evaluating the first bounce's records (lb_bake_options)."""
-    opts, keep = _options(cache, log, autotune, trace_every_bounce, watertight)
+    trace the gather rays in every bounce instead of evaluating the first bounce's records (lb_bake_options);
+    exchange: this process is one rank of a bake split over several, which trace their shares of every pass
+    and sum the passes' outputs on the device (every rank gets the whole bake)."""
+    opts, keep = _options(cache, log, autotune, trace_every_bounce, watertight, exchange)
     h = N.lib().lb_bake_device(gpu.handle, scene, len(scene), C.byref(opts))
     del keep
     if not h:
@@ -463,8 +465,9 @@ class Plan:
     (the graph enqueued on gpu.stream; repeatable), `rays()`, `result()`."""
 
     def __init__(self, scene: bytes, gpu: Gpu, cache=None, log=None, autotune=False, trace_every_bounce=False,
-                 watertight=False):
-        self._opts, self._keep = _options(cache, log, autotune, trace_every_bounce, watertight)
+                 watertight=False, exchange: Exchange = None):
+        self._opts, self._keep = _options(cache, log, autotune, trace_every_bounce, watertight, exchange)
+        self._exchange = exchange  # its callback lives as long as the plan
         self._h = N.lib().lb_plan_create(gpu.handle, scene, len(scene), C.byref(self._opts))
         if not self._h:
             raise LightbakerError(N.last_error())

@@ -603,6 +603,24 @@ void capture(lb_plan &p) {
                   p.s_v4.as<float4>(), p.s_e0.as<float4>(), p.s_e1.as<float4>()};
     unsigned long long *cnt = p.counters.as<unsigned long long>();
 
+    // a split bake: each pass takes this rank's share of its items, into outputs cleared first; the graph is
+    // cut after the pass, where the launch sums the outputs over the ranks
+    const bool split = p.world > 1;
+    const uint32_t part = split ? uint32_t(p.rank) : 0, parts = split ? uint32_t(p.world) : 1;
+    auto finish = [&](std::vector<std::pair<void *, size_t>> sums) {
+        lb_plan::Piece pc;
+        ck(cudaStreamEndCapture(st, &pc.graph), "end capture");
+        pc.sums = std::move(sums);
+        p.pieces.push_back(pc);
+        ck(cudaGraphInstantiate(&p.pieces.back().exec, pc.graph, 0), "graph instantiate");
+    };
+    auto cut = [&](void *words, size_t count) {
+        if (!split || !count) return;
+        finish({{words, count}});
+        ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    };
+    // the gather outputs a bounce's sum covers: every slot a gathered texel can take
+    const size_t gather_slots = std::min<uint64_t>(p.max_gathered, p.n_cov);
     ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
         ck(cudaMemsetAsync(cnt, 0, 12 * 8, st), "counters");
@@ -610,6 +628,9 @@ void capture(lb_plan &p) {
         w.S = &S;
         w.sms = p.g->sms;
         w.full_count = false;
+        w.part = part;
+        w.parts = parts;
+        if (p.n_cov && split) ck(cudaMemsetAsync(p.direct_out.p, 0, size_t(p.n_cov) * 16, st), "clear");
         if (p.n_cov) {
             w.pass = LB_PASS_DIRECT;
             w.P = &params;
@@ -627,6 +648,7 @@ void capture(lb_plan &p) {
             w.work = p.fetch_direct ? reinterpret_cast<unsigned int *>(cnt + 12) : nullptr;
             w.warp_walk = p.warp_walk;
             ck(lb_launch_pass_warp(w, st), "direct pass");
+            cut(p.direct_out.p, size_t(p.n_cov) * 4);
         }
         ck(lb_post_direct(a, int(h.lightmap.padding) + 4, s, st), "direct texel passes");
         ck(lb_select_gathered(a, p.select_temp.p, p.select_bytes, p.gath_idx.as<uint32_t>(), p.gath_count.as<uint32_t>(),
@@ -653,26 +675,36 @@ void capture(lb_plan &p) {
             gw.near = p.near_gather;
             gw.occ = p.occ_gather;
             gw.work = p.fetch_gather ? reinterpret_cast<unsigned int *>(cnt + 13) : nullptr;
+            gw.part = part;
+            gw.parts = parts;
             bool replay = p.reuse && b.gi_bounces > 1, record = replay || p.keep_records;
+            if (split && gather_slots)
+                ck(cudaMemsetAsync(p.gather_out.p, 0, gather_slots * 16, st), "clear");
             if (replay && bounce > 0) {
                 // the same rays met the same surfaces: evaluate the first bounce's records against this
                 // bounce's atlas (the sums in ray order, as the pass sums them)
                 ck(lb_eval_records(p.records.as<uint2>(), p.gath_count.as<uint32_t>(), 0, params.counts[2],
                                    p.light.as<float4>(), p.aw * p.ah, p.theta0.as<float>(),
-                                   uint32_t(h.materials.size()), p.gather_out.as<float4>(), p.g->sms, st),
+                                   uint32_t(h.materials.size()), p.gather_out.as<float4>(), p.g->sms, st, part, parts),
                    "gather records");
             } else {
                 gw.rec = record && bounce == 0 ? p.records.as<uint2>() : nullptr;
                 ck(lb_launch_pass_warp(gw, st), "gather pass");
             }
+            cut(p.gather_out.p, gather_slots * 4);
             ck(lb_post_bounce(a, p.gather_out.as<float4>(), int(b.gi_filter * p.ds), p.wr.as<float>(),
                               int(h.lightmap.padding + 2 * p.ds + 2), s, st),
                "bounce texel passes");
         }
         if (p.has_volume) {
-            // the probes the cache holds, then the ones baked here (every launch starts from the same grid)
-            ck(cudaMemcpyAsync(p.probes.p, p.probes_init.p, size_t(p.n_probes) * 64, cudaMemcpyDeviceToDevice, st),
-               "probes");
+            // the probes the cache holds, then the ones baked here (every launch starts from the same grid; in a
+            // split bake rank 0 brings the cached probes and every rank its share of the rest, zero elsewhere)
+            if (!split || p.rank == 0)
+                ck(cudaMemcpyAsync(p.probes.p, p.probes_init.p, size_t(p.n_probes) * 64, cudaMemcpyDeviceToDevice,
+                                   st),
+                   "probes");
+            else
+                ck(cudaMemsetAsync(p.probes.p, 0, size_t(p.n_probes) * 64, st), "probes");
             if (p.n_todo) {
                 WarpPass vw{};
                 vw.pass = LB_PASS_VOLUME;
@@ -688,7 +720,10 @@ void capture(lb_plan &p) {
                 vw.sms = p.g->sms;
                 vw.blocks = p.blocks_volume;
                 vw.bvh = p.bvh_volume;
+                vw.part = part;
+                vw.parts = parts;
                 ck(lb_launch_pass_warp(vw, st), "volume pass");
+                cut(p.probes.p, size_t(p.n_probes) * 16);
             }
             ck(lb_volume_fill(p.probes.as<float4>(), p.probes_b.as<float4>(), p.pk_a.as<uint8_t>(), p.pk_b.as<uint8_t>(),
                               p.vsize[0], p.vsize[1], p.vsize[2], 8, st),
@@ -725,22 +760,26 @@ void capture(lb_plan &p) {
                                     p.enc_vol.as<uint8_t>(), st),
                    "volume bytes");
         }
+        finish({});
     } catch (...) {
-        cudaGraph_t g;
-        cudaStreamEndCapture(st, &g);
-        if (g) cudaGraphDestroy(g);
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(st, &g);
+            if (g) cudaGraphDestroy(g);
+        }
         throw;
     }
-    ck(cudaStreamEndCapture(st, &p.graph), "end capture");
-    ck(cudaGraphInstantiate(&p.exec, p.graph, 0), "graph instantiate");
-    size_t n_nodes = 0;
-    ck(cudaGraphGetNodes(p.graph, nullptr, &n_nodes), "graph nodes");
-    std::vector<cudaGraphNode_t> nodes(n_nodes);
-    ck(cudaGraphGetNodes(p.graph, nodes.data(), &n_nodes), "graph nodes");
     p.kernel_nodes = 0;
-    for (auto nd : nodes) {
-        cudaGraphNodeType t;
-        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) p.kernel_nodes++;
+    for (const lb_plan::Piece &pc : p.pieces) {
+        size_t n_nodes = 0;
+        ck(cudaGraphGetNodes(pc.graph, nullptr, &n_nodes), "graph nodes");
+        std::vector<cudaGraphNode_t> nodes(n_nodes);
+        ck(cudaGraphGetNodes(pc.graph, nodes.data(), &n_nodes), "graph nodes");
+        for (auto nd : nodes) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) p.kernel_nodes++;
+        }
     }
 }
 
@@ -774,9 +813,14 @@ lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_
         }
         p->opt.watertight = opts && opts->watertight;
         p->autotune = opts && opts->autotune;
-        if (opts && opts->exchange && opts->exchange->world > 1)
-            throw std::runtime_error("lb_plan_create: a bake split over ranks runs through lb_bake_run or "
-                                     "lb_bake_run_with (exchange set)");
+        if (opts && opts->exchange && opts->exchange->world > 1) {
+            const lb_exchange *ex = opts->exchange;
+            if (!ex->sum || ex->rank < 0 || ex->rank >= ex->world)
+                throw std::runtime_error("lb_exchange: bad rank or no sum");
+            p->ex = *ex;
+            p->rank = ex->rank;
+            p->world = ex->world;
+        }
         p->reuse = !(opts && opts->trace_every_bounce);
         p->keep_records = keep_records;
         p->group_direct = g->group_direct;
@@ -799,6 +843,9 @@ lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_
         capture(*p);
         double t_capture = since(t0);
         if (p->opt.log) {
+            if (p->world > 1)
+                p->opt.log("rank " + std::to_string(p->rank) + " of " + std::to_string(p->world) +
+                           ": its share of every pass's items, the outputs summed over the ranks after each pass");
             p->opt.log(std::to_string(p->dirty.size()) + " of " + std::to_string(p->P.layout.tiles.size()) +
                        " tiles to bake on the device, " + std::to_string(p->n_cov) + " texels, " +
                        std::to_string(p->n_todo) + " probes");
@@ -832,7 +879,18 @@ int lb_plan_launch(lb_plan *p) {
     for (cudaEvent_t &ev : p->ev)
         if (!ev && e == cudaSuccess) e = cudaEventCreate(&ev);
     if (e == cudaSuccess) e = cudaEventRecord(p->ev[0], p->g->stream);
-    if (e == cudaSuccess) e = cudaGraphLaunch(p->exec, p->g->stream);
+    for (const lb_plan::Piece &pc : p->pieces) {
+        if (e == cudaSuccess) e = cudaGraphLaunch(pc.exec, p->g->stream);
+        for (const auto &sum : pc.sums) {
+            // the piece's outputs are complete before the ranks sum them, in place, on the device
+            if (e == cudaSuccess) e = cudaStreamSynchronize(p->g->stream);
+            if (e != cudaSuccess) break;
+            if (p->ex.sum(p->ex.ctx, sum.first, sum.second, 1) != 0) {
+                lb_set_error("lb_plan_launch: the exchange's sum failed");
+                return LB_EEXCHANGE;
+            }
+        }
+    }
     if (e == cudaSuccess) e = cudaEventRecord(p->ev[1], p->g->stream);
     if (e != cudaSuccess) return lb_cuda_fail(e, "lb_plan_launch");
     return LB_OK;
@@ -944,7 +1002,10 @@ lb::Bake lb_plan_collect(lb_plan &p) {
         std::vector<float> dl = down<float>(p, p.dl, size_t(p.n_dirty_texels) * 4),
                            id = down<float>(p, p.ind, size_t(p.n_dirty_texels) * 4);
         ck(cudaStreamSynchronize(p.g->stream), "download");
+        // a split bake: every rank holds every tile's light, and writes its share of the tiles and chunks
+        auto mine = [&](size_t k, size_t n) { return p.world <= 1 || k * size_t(p.world) / n == size_t(p.rank); };
         for (size_t k = 0; k < p.dirty.size(); k++) {
+            if (!mine(k, p.dirty.size())) continue;
             const DTile &t = p.tiles_all[k];
             size_t n = size_t(t.w) * t.h;
             lb::TileLight l;
@@ -962,7 +1023,9 @@ lb::Bake lb_plan_collect(lb_plan &p) {
             cache.put("tile", p.hashes[p.dirty[k]], l.pack());
         }
         if (p.has_volume)
-            for (auto &kv : p.chunk_keys) {
+            for (size_t c = 0; c < p.chunk_keys.size(); c++) {
+                if (!mine(c, p.chunk_keys.size())) continue;
+                auto &kv = p.chunk_keys[c];
                 std::vector<uint8_t> bytes(kv.second.size() * 64);
                 for (size_t i = 0; i < kv.second.size(); i++)
                     std::memcpy(bytes.data() + i * 64, &probes[size_t(kv.second[i]) * 16], 64);

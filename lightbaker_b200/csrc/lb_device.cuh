@@ -44,6 +44,19 @@ struct Count {
     __device__ void zero() { rays = nodes = tris = mats = 0; }
 };
 
+// The share of a pass's items [0, n) that one rank of a split bake takes: [n part / parts, n (part + 1) /
+// parts), contiguous, the shares covering every item once (parts 0 or 1: all of them). An item keeps its
+// index, and so its key and its output slot, whichever rank takes it.
+__device__ __forceinline__ void item_part(uint32_t n, uint32_t part, uint32_t parts, uint32_t &lo, uint32_t &hi) {
+    if (parts <= 1) {
+        lo = 0;
+        hi = n;
+        return;
+    }
+    lo = uint32_t(uint64_t(n) * part / parts);
+    hi = uint32_t(uint64_t(n) * (part + 1) / parts);
+}
+
 __device__ __forceinline__ float3 mk(float x, float y, float z) { return make_float3(x, y, z); }
 __device__ __forceinline__ float3 add(float3 a, float3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
 __device__ __forceinline__ float3 sub(float3 a, float3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
@@ -784,6 +797,13 @@ __device__ __forceinline__ Hit walk(const Scene &S, float3 o, float3 d, float tm
                                     uint32_t seed, Count &c) {
     if (BVH == 8) return trace8_t<COUNT, WT>(S, o, d, tmax, any, ray, seed, c);
     return trace_t<COUNT, WT>(S, o, d, tmax, any, ray, seed, c);
+}
+// The BVH2 walk for the rare ray a leaf list leaves to the tree (a near tie), as a call: one copy of the
+// walk serves every such site instead of a copy inlined at each.
+template <bool COUNT, bool WT>
+__device__ __noinline__ Hit walk_apart(const Scene &S, float3 o, float3 d, float tmax, uint32_t ray, uint32_t seed,
+                                       Count &c) {
+    return trace_t<COUNT, WT>(S, o, d, tmax, false, ray, seed, c);
 }
 
 // A gather ray's outcome, all a bounce needs to evaluate it again against another light atlas:

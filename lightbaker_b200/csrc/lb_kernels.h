@@ -47,13 +47,16 @@ struct WarpPass {
                               // their next item as they free up; null: a static stride over the items
     int warp_walk;            // direct pass over the BVH2 without counting: a texel's sun rays walk the tree
                               // together (lb_device.cuh escapes_warp), when the tree is shallow enough
+    uint32_t part, parts;     // a split bake: this rank takes share `part` of `parts` of the items (item_part in
+                              // lb_device.cuh); parts 0 or 1: every item
 };
 // The gather records evaluated against a light atlas and theta (albedo 3 a material, zenith, horizon,
 // ground, sun scale; transport.cu): each item's gather result, its terms summed in ray order, equal to
 // what the gather pass gives for the same light.
+// part, parts: only that share of the items (item_part), as the gather pass that recorded them.
 cudaError_t lb_eval_records(const uint2 *rec, const uint32_t *n_dev, uint32_t n_host, uint32_t rays,
                             const float4 *light, uint32_t n_light, const float *theta, uint32_t n_mats, float4 *out,
-                            int sms, cudaStream_t stream);
+                            int sms, cudaStream_t stream, uint32_t part = 0, uint32_t parts = 1);
 cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream);
 // The persistent grid's size for a pass: SMs x resident blocks of 256 threads.
 int lb_warp_pass_blocks(const WarpPass &w);

@@ -121,7 +121,14 @@ __device__ __forceinline__ bool inside_list(const Scene &S, const lb_params &P, 
         Frame f = frame(n);
         uint32_t r = uint32_t(lane);
         float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
-        Hit h = trace_list<COUNT, WT>(S, list, dist2, nl, o, d, P.ground[3], key + r + 7000u, seed, c, shift);
+        bool tie;
+        Hit h = trace_list_t<COUNT, WT, true>(S, list, dist2, nl, o, d, P.ground[3], key + r + 7000u, seed, c, shift,
+                                              tie);
+        if (tie) {
+            // nearly coincident faces: the tree walk's own order decides which is the hit (and its face)
+            c.rays--;
+            h = walk_apart<COUNT, WT>(S, o, d, P.ground[3], key + r + 7000u, seed, c);
+        }
         back = h.tri != NONE && h.back;
     }
     float nb = __uint2float_rn(__popc(__ballot_sync(FULL, back)));
@@ -131,11 +138,12 @@ __device__ __forceinline__ bool inside_list(const Scene &S, const lb_params &P, 
 // The item a warp takes next. With a work counter (zeroed before the launch) every warp takes the next item
 // not yet taken as soon as it is free, so warps behind heavy items (texels whose inside tests retry, long
 // escaping rays) no longer hold up the pass's end; without one, a static stride. Called by the whole warp.
-__device__ __forceinline__ uint32_t take_item(unsigned int *work, uint32_t k, uint32_t step, int lane) {
+// `lo`: the first item of the launch's share (item_part), where the counter's count starts.
+__device__ __forceinline__ uint32_t take_item(unsigned int *work, uint32_t k, uint32_t step, uint32_t lo, int lane) {
     if (!work) return k + step;
     uint32_t v = 0;
     if (lane == 0) v = atomicAdd(work, 1u);
-    return __shfl_sync(FULL, v, 0);
+    return lo + __shfl_sync(FULL, v, 0);
 }
 
 template <bool COUNT>
@@ -164,7 +172,8 @@ template <int BVH, bool COUNT, int OCC = 1, int WALK = 0, bool WT = false>
 __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S, lb_params P, const float4 *tex, const uint32_t *idx,
                                                    const uint32_t *n_dev, uint32_t n_host, uint32_t base, float4 *out,
                                                    unsigned long long *counters, int group, int refill, int near,
-                                                   unsigned int *work, int warp_walk) {
+                                                   unsigned int *work, int warp_walk, uint32_t part,
+                                                   uint32_t parts) {
     // each occlusion ray's term by ray index (0 for a miss: adding it to the sum changes no bit, as the sum
     // starts at +0 and every term is >= 0); before the rays, the ball query's scratch
     __shared__ float s_term[WARPS][AO_CAP];
@@ -174,16 +183,20 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
     // the sun rays' shared walk (escapes_warp): its stack of kept children and their lanes
     constexpr int WW = (BVH == 2 && !COUNT) ? int(WARP_WALK_DEPTH) : 1;
     __shared__ uint32_t s_ww_node[WARPS][WW], s_ww_mask[WARPS][WW];
+    // the leaf lists' occlusion rays left to the tree walk (near ties), by ray index
+    constexpr int PW = (BVH == 2 && WALK == 1) ? WARPS : 1;
+    __shared__ uint16_t s_pend[PW][AO_CAP];
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t n = n_dev ? *n_dev : n_host;
+    uint32_t lo, n;
+    item_part(n_dev ? *n_dev : n_host, part, parts, lo, n);
     const uint32_t seed = __float_as_uint(P.reach[3]);
     const bool shared_sun = BVH == 2 && !COUNT && warp_walk && S.depth <= WARP_WALK_DEPTH;
     Count c;
     c.zero();
-    const uint32_t first = work ? take_item(work, 0, 0, lane) : warp;
-    for (uint32_t k = first; k < n; k = take_item(work, k, warps, lane)) {
+    const uint32_t first = work ? take_item(work, 0, 0, lo, lane) : lo + warp;
+    for (uint32_t k = first; k < n; k = take_item(work, k, warps, lo, lane)) {
         Item it = load_item(tex, idx, nullptr, k);
         float3 nrm = xyz(it.nrm), pos = xyz(it.pos), dx = xyz(it.dx), dy = xyz(it.dy);
         uint32_t key = (base + k) * 7919u;
@@ -315,21 +328,46 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
         }
         if (pick == 0u) listed_from(o, ao_shift);
         if (nl >= 0) {
-            uint32_t myback = 0;
+            uint32_t myback = 0, npend = 0;
+            const unsigned below = (1u << lane) - 1u;
+            auto term_of = [&](uint32_t r, const Hit &h) {
+                float term = 0.0f;
+                if (h.tri != NONE) {
+                    float kk = h.t / P.reach[0];
+                    term = 1.0f - kk * kk;
+                    if (h.back && h.t < P.ground[3]) myback++;
+                }
+                s_term[w][r] = term;
+            };
+            auto dir_of = [&](uint32_t r) {
+                return cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
+            };
             for (uint32_t r0 = 0; r0 < rays; r0 += 32) {
                 uint32_t r = ord.ray(r0 >> 5);
+                bool pend = false;
                 if (r < rays) {
-                    float3 d = cosine(fract((__uint2float_rn(r) + 0.5f) / frays + s1), fract(radical(r) + s2), f);
-                    Hit h = trace_list<COUNT, WT>(S, s_list[w], s_dist[w], nl, o, d, P.reach[0], key + r + 2000u, seed, c,
-                                              ao_shift);
-                    float term = 0.0f;
-                    bool hit = h.tri != NONE;
-                    if (hit) {
-                        float kk = h.t / P.reach[0];
-                        term = 1.0f - kk * kk;
-                        if (h.back && h.t < P.ground[3]) myback++;
+                    bool tie;
+                    Hit h = trace_list_t<COUNT, WT, true>(S, s_list[w], s_dist[w], nl, o, dir_of(r), P.reach[0],
+                                                          key + r + 2000u, seed, c, ao_shift, tie);
+                    if (tie) {
+                        pend = true;
+                        c.rays--;  // the tree walk counts it
+                    } else {
+                        term_of(r, h);
                     }
-                    s_term[w][r] = term;
+                }
+                const unsigned pm = __ballot_sync(FULL, pend);
+                if (pend) s_pend[PW == 1 ? 0 : w][npend + __popc(pm & below)] = uint16_t(r);
+                npend += __popc(pm);
+            }
+            // nearly coincident faces: the tree walk's t (its box test may pass over the nearer face's box
+            // when the entry rounds past the hit it holds), for the rays that met such a tie, 32 at a time
+            __syncwarp();
+            for (uint32_t b0 = 0; b0 < npend; b0 += 32) {
+                const uint32_t i = b0 + uint32_t(lane);
+                if (i < npend) {
+                    const uint32_t r = s_pend[PW == 1 ? 0 : w][i];
+                    term_of(r, walk_apart<COUNT, WT>(S, o, dir_of(r), P.reach[0], key + r + 2000u, seed, c));
                 }
             }
             for (int ofs = 16; ofs > 0; ofs >>= 1) myback += __shfl_down_sync(FULL, myback, ofs);
@@ -432,7 +470,7 @@ template <int BVH, bool COUNT, int OCC = 1, int WALK = 0, bool WT = false>
 __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) gather_warp(
     Scene S, lb_params P, const float4 *tex, const uint32_t *idx, const float4 *pos_override, const uint32_t *n_dev,
     uint32_t n_host, uint32_t base, const float4 *light, uint32_t n_light, float4 *out, unsigned long long *counters,
-    int group, int refill, uint2 *rec, unsigned int *work) {
+    int group, int refill, uint2 *rec, unsigned int *work, uint32_t part, uint32_t parts) {
     constexpr int LW = (BVH == 2 && WALK == 1) ? WARPS : 1;  // the leaf lists' shared memory, when used
     __shared__ float3 s_term[WARPS][GI_CAP];
     __shared__ uint8_t s_on[WARPS][GI_CAP];
@@ -442,12 +480,13 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) gather_warp(
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t n = n_dev ? *n_dev : n_host;
+    uint32_t lo, n;
+    item_part(n_dev ? *n_dev : n_host, part, parts, lo, n);
     const uint32_t seed = __float_as_uint(P.reach[3]);
     Count c;
     c.zero();
-    const uint32_t first = work ? take_item(work, 0, 0, lane) : warp;
-    for (uint32_t k = first; k < n; k = take_item(work, k, warps, lane)) {
+    const uint32_t first = work ? take_item(work, 0, 0, lo, lane) : lo + warp;
+    for (uint32_t k = first; k < n; k = take_item(work, k, warps, lo, lane)) {
         Item it = load_item(tex, idx, pos_override, k);
         float3 nrm = xyz(it.nrm), pos = xyz(it.pos), dx = xyz(it.dx), dy = xyz(it.dy);
         Frame f = frame(nrm);
@@ -622,16 +661,19 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) gather_warp(
 
 // trace.wgsl:272-324. `slot` (optional) scatters probe k's four records to 4 * slot[k].
 template <int BVH, bool COUNT, bool WT = false>
-__global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const float4 *tex, uint32_t n, const float4 *light,
-                                                   uint32_t n_light, float4 *out, const uint32_t *slot,
-                                                   unsigned long long *counters) {
+__global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const float4 *tex, uint32_t n_all,
+                                                   const float4 *light, uint32_t n_light, float4 *out,
+                                                   const uint32_t *slot, unsigned long long *counters, uint32_t part,
+                                                   uint32_t parts) {
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t seed = __float_as_uint(P.reach[3]);
     Count c;
     c.zero();
-    for (uint32_t k = warp; k < n; k += warps) {
+    uint32_t lo, n;
+    item_part(n_all, part, parts, lo, n);
+    for (uint32_t k = lo + warp; k < n; k += warps) {
         float3 o = xyz(__ldg(&tex[4 * k]));
         uint32_t key = __float_as_uint(__ldg(&tex[4 * k + 1]).w) * 7919u + 77u;
         uint32_t rays = P.counts[2];
@@ -732,16 +774,16 @@ void launch_walk(const WarpPass &w, int blocks, cudaStream_t stream) {
     case LB_PASS_DIRECT:
         lbd::direct_warp<BVH, COUNT, OCC, WALK, WT><<<blocks, T, 0, stream>>>(
             *w.S, *w.P, w.tex, w.idx, w.n_dev, w.n_host, w.base, w.out, w.counters, w.group, w.refill, w.near, w.work,
-            w.warp_walk);
+            w.warp_walk, w.part, w.parts);
         break;
     case LB_PASS_GATHER:
         lbd::gather_warp<BVH, COUNT, OCC, WALK, WT><<<blocks, T, 0, stream>>>(
             *w.S, *w.P, w.tex, w.idx, w.pos, w.n_dev, w.n_host, w.base, w.light, w.n_light, w.out, w.counters, w.group,
-            w.refill, w.rec, w.work);
+            w.refill, w.rec, w.work, w.part, w.parts);
         break;
     default:
         lbd::volume_warp<BVH, COUNT, WT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light,
-                                                                   w.out, w.slot, w.counters);
+                                                                   w.out, w.slot, w.counters, w.part, w.parts);
         break;
     }
 }
@@ -801,8 +843,10 @@ cudaError_t lb_launch_pass_warp(const WarpPass &w, cudaStream_t stream) {
     if (w.bvh == 8 && (w.S->nodes8 == nullptr || w.S->tris8 == nullptr)) return cudaErrorInvalidValue;
     int blocks = w.blocks > 0 ? w.blocks : lb_warp_pass_blocks(w);
     if (w.n_dev == nullptr) {
-        // no more warps than items
-        uint32_t need = (w.n_host + (T / 32) - 1) / (T / 32);
+        // no more warps than the share's items
+        const uint64_t parts = w.parts > 1 ? w.parts : 1, part = w.parts > 1 ? w.part : 0;
+        const uint32_t mine = uint32_t(uint64_t(w.n_host) * (part + 1) / parts - uint64_t(w.n_host) * part / parts);
+        uint32_t need = (mine + (T / 32) - 1) / (T / 32);
         if (need == 0) return cudaSuccess;
         if ((uint32_t)blocks > need) blocks = (int)need;
     }

@@ -124,16 +124,28 @@ struct lb_plan {
     lbplan::DBuf records, theta0;
     std::string tuned;  // what the autotuner picked
     std::string build_phases;  // the host build's phases, seconds since its start
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    // a bake split over ranks (lb_exchange): every pass traces this rank's share of its items (item_part), and
+    // the ranks sum the passes' outputs (one writer a word) before the texel passes that read them
+    int rank = 0, world = 1;
+    lb_exchange ex{};
+    // the graph in pieces: one, or (world > 1) cut after each pass whose outputs the ranks sum; the sums
+    // (device words) a launch makes after each piece
+    struct Piece {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        std::vector<std::pair<void *, size_t>> sums;
+    };
+    std::vector<Piece> pieces;
     cudaEvent_t ev[2] = {nullptr, nullptr};  // around the last lb_plan_launch: the graph's device time
     double t_prepare = 0;
     lb::Stats stats;
     ~lb_plan() {
         for (cudaEvent_t e : ev)
             if (e) cudaEventDestroy(e);
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
+        for (Piece &pc : pieces) {
+            if (pc.exec) cudaGraphExecDestroy(pc.exec);
+            if (pc.graph) cudaGraphDestroy(pc.graph);
+        }
         if (dscene) lb_scene_free(dscene);
     }
 };

@@ -64,11 +64,12 @@ constexpr uint32_t LIT_NONE = 0xffffffffu, UNLIT = 0xfffffffeu;
 // The records against the light and theta: each gathered texel's gather result, its terms summed in ray
 // order as the gather pass sums them (trace.wgsl:258-269); a thread an item, reading its records in turn.
 __global__ void k_eval(const uint2 *rec, const uint32_t *n_dev, uint32_t n_host, uint32_t rays, const float4 *light,
-                       uint32_t n_light, Theta th, float4 *out) {
-    const uint32_t n = n_dev ? *n_dev : n_host;
+                       uint32_t n_light, Theta th, float4 *out, uint32_t part, uint32_t parts) {
+    uint32_t lo, n;
+    item_part(n_dev ? *n_dev : n_host, part, parts, lo, n);
     const float frays = __uint2float_rn(rays);
     const float3 zen = th.zenith(), hor = th.horizon(), gro = th.ground(), fb = th.fallback();
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    for (uint32_t k = lo + blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint2 *rk = rec + size_t(k) * rays;
         float3 sum = mk(0.f, 0.f, 0.f);
         uint32_t nback = 0;
@@ -619,8 +620,9 @@ __global__ void __launch_bounds__(256) k_theta_final(const PartialSet *sets, int
 
 cudaError_t lb_eval_records(const uint2 *rec, const uint32_t *n_dev, uint32_t n_host, uint32_t rays,
                             const float4 *light, uint32_t n_light, const float *theta, uint32_t n_mats, float4 *out,
-                            int sms, cudaStream_t stream) {
-    lbd::k_eval<<<sms * 16, 128, 0, stream>>>(rec, n_dev, n_host, rays, light, n_light, lbd::Theta{theta, n_mats}, out);
+                            int sms, cudaStream_t stream, uint32_t part, uint32_t parts) {
+    lbd::k_eval<<<sms * 16, 128, 0, stream>>>(rec, n_dev, n_host, rays, light, n_light, lbd::Theta{theta, n_mats}, out,
+                                              part, parts);
     return cudaGetLastError();
 }
 
