@@ -620,18 +620,31 @@ __device__ __noinline__ int ball_leaves(const Scene &S, float3 o, float r, float
 // distance from it), and the ray starts within `shift` of that centre, so once a box lies farther than the
 // nearest hit so far plus shift (by a relative margin far above the rounding of t, |d| and the distance),
 // neither it nor any later box can hold a nearer hit and the walk ends: the same hit as the whole list.
-// TIES: set `tie` when another accepted triangle lies within NEAR_TIE of the returned t (coincident or
-// nearly coincident faces, a ray through a shared edge or vertex). Between such triangles the tree walk's
-// answer depends on the order it opens boxes in and on its box test culling one whose entry rounds past
-// the nearest hit it holds, so a caller that must match it walks the tree for such a ray. Without TIES
-// the nearest triangle found wins (the first in list order at an exact tie).
-__device__ __forceinline__ float near_tie(float t) { return t * 1.00001f + 1e-4f; }
-template <bool COUNT, bool WT, bool TIES>
+//
+// Near ties. The tree walk keeps the nearest hit among the boxes it opens, and it skips a box whose
+// entry is not below the hit it holds. So its answer differs from the list's nearest hit t only when
+// (a) another accepted triangle lies exactly at t (then the order boxes are opened in picks one), or
+// (b) a box on the tree's path to the hit has an entry that rounds up to t or past it, and another accepted
+// triangle lies just beyond t (the tree may hold that one first and skip the hit's box). Every box on that
+// path contains the hit's leaf box, so its entry is at most the leaf box's (in exact arithmetic; computed,
+// within a few units in the last place of it), and the triangle the tree holds instead lies between the
+// hit and that entry. With TIES the walk also opens boxes entered up to tie_reach past the hit (the larger
+// of the hit and its box's entry, widened by 1e-5), notes the accepted triangles there by facing, and sets
+// `tie` when the case can change what the caller reads; the caller then walks the tree for that ray:
+//   TIE_GATHER  the hit's triangle (material, chart, point): (a) any face, or (b) any face;
+//   TIE_OCC     t and the facing: (a) another facing, or (b) any face (another t);
+//   TIE_INSIDE  the facing alone: (a) or (b) with another facing.
+// Without TIES the nearest triangle found wins (the first in list order at an exact tie).
+constexpr int TIE_NONE = 0, TIE_GATHER = 1, TIE_OCC = 2, TIE_INSIDE = 3;
+// how far past a hit at t, whose box the walk entered at e, a triangle may lie and still decide a tie
+__device__ __forceinline__ float tie_reach(float t, float e) { return fmaxf(t, e) * 1.00001f; }
+template <bool COUNT, bool WT, int TIES>
 __device__ __forceinline__ Hit trace_list_t(const Scene &S, const uint32_t *list, const float *dist2, int nl, float3 o,
                                             float3 d, float tmax, uint32_t ray, uint32_t seed, Count &c, float shift,
                                             bool &tie) {
     Hit hit{tmax, NONE, false};
-    float other = FAR;  // TIES: the nearest accepted t but the hit's
+    // TIES: the nearest accepted t of each facing but the hit's, and the entry of the hit's box
+    float of_front = FAR, of_back = FAR, e_hit = 0.0f;
     c.rays++;
     float3 dd = mk(fabsf(d.x) < 1e-12f ? 1e-12f : d.x, fabsf(d.y) < 1e-12f ? 1e-12f : d.y,
                    fabsf(d.z) < 1e-12f ? 1e-12f : d.z);
@@ -643,8 +656,9 @@ __device__ __forceinline__ Hit trace_list_t(const Scene &S, const uint32_t *list
         float4 lo = __ldg(&S.nodes[2 * node]), hi = __ldg(&S.nodes[2 * node + 1]);
         if (COUNT) c.nodes++;
         const bool found = hit.tri != NONE;
-        // TIES: boxes entered up to NEAR_TIE past the nearest hit open too, to see the triangles near it
-        if (!(box<WT>(o, inv, lo, hi, TIES && found ? near_tie(hit.t) : hit.t, S.grow) < FAR)) continue;
+        // TIES: boxes entered up to tie_reach past the nearest hit open too, to see the triangles near it
+        const float eb = box<WT>(o, inv, lo, hi, TIES && found ? tie_reach(hit.t, e_hit) : hit.t, S.grow);
+        if (!(eb < FAR)) continue;
         const uint32_t first = __float_as_uint(lo.w);
         for (uint32_t m = entry >> LEAF_MASK_SHIFT; m; m &= m - 1u) {
             const uint32_t i = first + uint32_t(__ffs(int(m)) - 1);
@@ -653,18 +667,35 @@ __device__ __forceinline__ Hit trace_list_t(const Scene &S, const uint32_t *list
             float t;
             bool bk;
             if (!tri_hit<WT>(S, i, v0, e1, e2, o, d, t, bk)) continue;
-            if (t > 1e-4f && t < hit.t && stops<COUNT>(S, i, v0.w, ray, seed, c)) {
-                if (TIES && hit.tri != NONE) other = fminf(other, hit.t);
+            const bool nearer = t > 1e-4f && t < hit.t;
+            const bool close = TIES && !nearer && hit.tri != NONE && t > 1e-4f && t <= tie_reach(hit.t, e_hit);
+            if (!(nearer || close) || !stops<COUNT>(S, i, v0.w, ray, seed, c)) continue;
+            if (nearer) {
+                if (TIES && hit.tri != NONE) {
+                    if (hit.back) of_back = fminf(of_back, hit.t);
+                    else of_front = fminf(of_front, hit.t);
+                }
                 hit = Hit{t, i, bk};
+                e_hit = eb;
                 lim = (t + shift) * 1.0001f + 1e-5f;
                 lim2 = lim * lim;
-            } else if (TIES && hit.tri != NONE && t > 1e-4f && t <= near_tie(hit.t) &&
-                       stops<COUNT>(S, i, v0.w, ray, seed, c)) {
-                other = fminf(other, t);
+            } else if (bk) {
+                of_back = fminf(of_back, t);
+            } else {
+                of_front = fminf(of_front, t);
             }
         }
     }
-    tie = TIES && hit.tri != NONE && other <= near_tie(hit.t);
+    tie = false;
+    if (TIES != TIE_NONE && hit.tri != NONE) {
+        const float same = hit.back ? of_back : of_front, other = hit.back ? of_front : of_back;
+        // (b)'s first half: the hit's box entry, within rounding, at or past the hit
+        const bool edge = e_hit * 1.00001f >= hit.t;
+        const float w = tie_reach(hit.t, e_hit);
+        if (TIES == TIE_GATHER) tie = same == hit.t || other == hit.t || (edge && fminf(same, other) <= w);
+        else if (TIES == TIE_OCC) tie = other == hit.t || (edge && fminf(same, other) <= w);
+        else tie = other == hit.t || (edge && other <= w);
+    }
     return hit;
 }
 template <bool COUNT, bool WT = false>
@@ -672,7 +703,7 @@ __device__ __forceinline__ Hit trace_list(const Scene &S, const uint32_t *list, 
                                           float3 d, float tmax, uint32_t ray, uint32_t seed, Count &c,
                                           float shift = 0.0f) {
     bool tie;
-    return trace_list_t<COUNT, WT, false>(S, list, dist2, nl, o, d, tmax, ray, seed, c, shift, tie);
+    return trace_list_t<COUNT, WT, TIE_NONE>(S, list, dist2, nl, o, d, tmax, ray, seed, c, shift, tie);
 }
 
 // The same query over the 8-wide BVH: the nearest accepted hit within tmax (any: the first accepted),

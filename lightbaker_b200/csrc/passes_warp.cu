@@ -122,8 +122,8 @@ __device__ __forceinline__ bool inside_list(const Scene &S, const lb_params &P, 
         uint32_t r = uint32_t(lane);
         float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
         bool tie;
-        Hit h = trace_list_t<COUNT, WT, true>(S, list, dist2, nl, o, d, P.ground[3], key + r + 7000u, seed, c, shift,
-                                              tie);
+        Hit h = trace_list_t<COUNT, WT, TIE_INSIDE>(S, list, dist2, nl, o, d, P.ground[3], key + r + 7000u, seed, c,
+                                                    shift, tie);
         if (tie) {
             // nearly coincident faces: the tree walk's own order decides which is the hit (and its face)
             c.rays--;
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
                 bool pend = false;
                 if (r < rays) {
                     bool tie;
-                    Hit h = trace_list_t<COUNT, WT, true>(S, s_list[w], s_dist[w], nl, o, dir_of(r), P.reach[0],
+                    Hit h = trace_list_t<COUNT, WT, TIE_OCC>(S, s_list[w], s_dist[w], nl, o, dir_of(r), P.reach[0],
                                                           key + r + 2000u, seed, c, ao_shift, tie);
                     if (tie) {
                         pend = true;
@@ -542,7 +542,7 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) gather_warp(
                 if (nl >= 0 && dot3(v, nrm) >= front) {
                     const float shift = sqrtf(dot3(v, v)) * 1.001f + 1e-6f;
                     bool tie;
-                    Hit h = trace_list_t<COUNT, WT, true>(S, s_list[lw], s_dist[lw], nl, o, d, rnear, key + r + 4000u,
+                    Hit h = trace_list_t<COUNT, WT, TIE_GATHER>(S, s_list[lw], s_dist[lw], nl, o, d, rnear, key + r + 4000u,
                                                           seed, c, shift, tie);
                     if (h.tri != NONE && !tie) {
                         done = true;
