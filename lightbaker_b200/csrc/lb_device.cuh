@@ -221,7 +221,8 @@ __device__ __forceinline__ bool tri_hit(const Scene &S, uint32_t ref, float4 v0,
     float3 p = cross3(d, xyz(e2));
     float det = dot3(xyz(e1), p);
     if (fabsf(det) < 1e-12f) return false;
-    float id = 1.0f / det;
+    // 1 / det rounded to nearest: the same bits as the division (both are the correctly rounded reciprocal)
+    float id = __frcp_rn(det);
     float3 s = sub(o, xyz(v0));
     float u = dot3(s, p) * id;
     if (u < 0.0f || u > 1.0f) return false;
@@ -650,14 +651,15 @@ __device__ __forceinline__ Hit trace_list_t(const Scene &S, const uint32_t *list
                    fabsf(d.z) < 1e-12f ? 1e-12f : d.z);
     float3 inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
     float lim = (tmax + shift) * 1.0001f + 1e-5f, lim2 = lim * lim;
+    // boxes open while entered before `cull`: the nearest hit; TIES: tie_reach past it, so that boxes entered
+    // just past the hit open too, to see the triangles near it
+    float cull = tmax;
     for (int k = 0; k < nl; k++) {
         if (dist2[k] > lim2) break;
         const uint32_t entry = list[k], node = entry & LEAF_NODE;
         float4 lo = __ldg(&S.nodes[2 * node]), hi = __ldg(&S.nodes[2 * node + 1]);
         if (COUNT) c.nodes++;
-        const bool found = hit.tri != NONE;
-        // TIES: boxes entered up to tie_reach past the nearest hit open too, to see the triangles near it
-        const float eb = box<WT>(o, inv, lo, hi, TIES && found ? tie_reach(hit.t, e_hit) : hit.t, S.grow);
+        const float eb = box<WT>(o, inv, lo, hi, cull, S.grow);
         if (!(eb < FAR)) continue;
         const uint32_t first = __float_as_uint(lo.w);
         for (uint32_t m = entry >> LEAF_MASK_SHIFT; m; m &= m - 1u) {
@@ -677,6 +679,7 @@ __device__ __forceinline__ Hit trace_list_t(const Scene &S, const uint32_t *list
                 }
                 hit = Hit{t, i, bk};
                 e_hit = eb;
+                cull = TIES ? tie_reach(t, eb) : t;
                 lim = (t + shift) * 1.0001f + 1e-5f;
                 lim2 = lim * lim;
             } else if (bk) {
