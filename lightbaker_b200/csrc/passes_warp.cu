@@ -241,23 +241,19 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
                 return inside_list<COUNT, WT>(S, P, seed, s_list[wi], s_dist[wi], nl, o, nrm, k, lane, c, shift);
             return inside_warp<BVH, COUNT, WT>(S, P, seed, o, nrm, k, lane, c);
         };
-        if (inside_at(c0, key)) {
-            for (uint32_t q = 1u; q < 9u; q++) {
-                float3 p = candidate(q);
-                if (!inside_at(add(p, lift), key + q * 31u)) {
-                    at = p;
-                    pick = q;
-                    span = 0.4f;
-                    break;
-                }
-            }
-            if (pick == 0u) {
-                float3 p = candidate(9u);
-                if (!inside_at(add(p, lift), key + 331u)) {
-                    at = p;
-                    pick = 9u;
-                    span = 0.4f;
-                }
+        // trace.wgsl:186-210: the texel's own point, then (when it is inside) the candidates 1..8 and the
+        // pushed point 9 in order, until one is not inside; one call site, so the walks are inlined once
+#pragma unroll 1
+        for (uint32_t q = 0u; q <= 9u; q++) {
+            const float3 p = q == 0u ? pos : candidate(q);
+            const bool in = inside_at(add(p, lift), q == 0u ? key : (q == 9u ? key + 331u : key + q * 31u));
+            if (q == 0u) {
+                if (!in) break;
+            } else if (!in) {
+                at = p;
+                pick = q;
+                span = 0.4f;
+                break;
             }
         }
         float soft = 0.0f;
@@ -293,12 +289,11 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
                     float cx = ((__uint2float_rn(s % g) + 0.5f) / fg - 0.5f) * span;
                     float cy = ((__uint2float_rn(s / g) + 0.5f) / fg - 0.5f) * span;
                     float3 o = add(add(add(at, scl(dx, cx)), scl(dy, cy)), lift);
-                    if (lane < 16) {
-                        escaped = walk<BVH, COUNT, WT>(S, o, sun, FAR, true, key + s, seed, c).tri == NONE;
-                    } else {
-                        float3 d = sun_disc(P, sf, (s + turn) % gg, gg);
-                        escaped = walk<BVH, COUNT, WT>(S, o, d, FAR, true, key + s + 1000u, seed, c).tri == NONE;
-                    }
+                    // lanes 0..15 the hard ray toward the sun, 16..31 the soft one (one walk call site)
+                    const bool hard_ray = lane < 16;
+                    const float3 d = hard_ray ? sun : sun_disc(P, sf, (s + turn) % gg, gg);
+                    escaped = walk<BVH, COUNT, WT>(S, o, d, FAR, true, hard_ray ? key + s : key + s + 1000u, seed, c).tri ==
+                              NONE;
                 }
                 unsigned m = __ballot_sync(FULL, escaped);
                 hard |= (m & 0xffffu) << (s0 & 31u);  // the shader shifts modulo 32
