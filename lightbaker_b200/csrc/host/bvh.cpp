@@ -48,25 +48,69 @@ inline void run_of(size_t n, int k, int parts, size_t &lo, size_t &hi) {
     hi = n * size_t(k + 1) / size_t(parts);
 }
 
-// bvh.rs:119-151: the axis and plane of the cheapest binned split, if one beats a leaf
-bool best_split(const Prim *p, size_t n, int &axis_out, float &at_out) {
-    Vec3 cmin = Vec3::splat(INFINITY), cmax = Vec3::splat(-INFINITY), pmin = cmin, pmax = cmax;
-    const int parts = n >= PARALLEL_BINS ? std::max(1, std::min(omp_get_max_threads(), MAX_PARTS)) : 1;
-    {
-        // fixed arrays: this runs once for every node of the tree, most of them small
-        Vec3 a[MAX_PARTS], b[MAX_PARTS], c[MAX_PARTS], d[MAX_PARTS];
-        for (int k = 0; k < parts; k++) {
-            a[k] = c[k] = Vec3::splat(INFINITY);
-            b[k] = d[k] = Vec3::splat(-INFINITY);
+// One axis's bins: bounds and counts.
+struct Bins {
+    Vec3 mn[BINS], mx[BINS];
+    uint32_t n[BINS];
+    void clear() {
+        for (size_t b = 0; b < BINS; b++) {
+            mn[b] = Vec3::splat(INFINITY);
+            mx[b] = Vec3::splat(-INFINITY);
+            n[b] = 0;
         }
-#pragma omp parallel for schedule(static, 1) if (parts > 1)
+    }
+};
+
+// A node's centres' bounds and its bounds over p[lo, hi), each folded in order (into locals: the callers'
+// slots for several threads' runs share cache lines).
+inline void gather_bounds(const Prim *p, size_t lo, size_t hi, Vec3 &cmin_out, Vec3 &cmax_out, Vec3 &pmin_out,
+                          Vec3 &pmax_out) {
+    Vec3 cmin = cmin_out, cmax = cmax_out, pmin = pmin_out, pmax = pmax_out;
+    for (size_t i = lo; i < hi; i++) {
+        bounds_add(cmin, cmax, p[i].centre, p[i].centre);
+        bounds_add(pmin, pmax, p[i].min, p[i].max);
+    }
+    cmin_out = cmin, cmax_out = cmax, pmin_out = pmin, pmax_out = pmax;
+}
+
+// p[lo, hi) into the bins of every axis that is binned (use[axis]), in order (bvh.rs:127-133)
+inline void gather_bins(const Prim *p, size_t lo, size_t hi, const bool use[3], const Vec3 &cmin, const float ext[3],
+                        Bins out[3]) {
+    Bins bins[3] = {out[0], out[1], out[2]};
+    for (size_t i = lo; i < hi; i++) {
+        for (int axis = 0; axis < 3; axis++) {
+            if (!use[axis]) continue;
+            float f = (p[i].centre[axis] - cmin[axis]) / ext[axis] * float(BINS);
+            size_t b = f > 0.0f ? size_t(f) : 0;  // Rust `as usize`: truncation, saturating at 0
+            if (b > BINS - 1) b = BINS - 1;
+            Bins &q = bins[axis];
+            q.mn[b] = q.mn[b].min(p[i].min);
+            q.mx[b] = q.mx[b].max(p[i].max);
+            q.n[b]++;
+        }
+    }
+    for (int axis = 0; axis < 3; axis++) out[axis] = bins[axis];
+}
+
+// bvh.rs:119-151: the axis and plane of the cheapest binned split, if one beats a leaf, and the node's
+// bounds (pmin, pmax: the fold bvh.rs:66-67 makes, the same bits, gathered here once). The three axes
+// are binned in one pass over the primitives; from PARALLEL_BINS primitives on, every thread takes one
+// contiguous run and the runs' bounds and bins are merged in run order. (The per-run arrays are sized to
+// the runs: most calls are for nodes of a few primitives, for which clearing arrays sized for 64 runs
+// cost more than the binning.)
+bool best_split(const Prim *p, size_t n, int &axis_out, float &at_out, Vec3 &pmin, Vec3 &pmax) {
+    Vec3 cmin = Vec3::splat(INFINITY), cmax = Vec3::splat(-INFINITY);
+    pmin = cmin, pmax = cmax;
+    const int parts = n >= PARALLEL_BINS ? std::max(1, std::min(omp_get_max_threads(), MAX_PARTS)) : 1;
+    if (parts == 1) {
+        gather_bounds(p, 0, n, cmin, cmax, pmin, pmax);
+    } else {
+        std::vector<Vec3> a(parts, Vec3::splat(INFINITY)), b(parts, Vec3::splat(-INFINITY)), c = a, d = b;
+#pragma omp parallel for schedule(static, 1)
         for (int k = 0; k < parts; k++) {
             size_t lo, hi;
             run_of(n, k, parts, lo, hi);
-            for (size_t i = lo; i < hi; i++) {
-                bounds_add(a[k], b[k], p[i].centre, p[i].centre);
-                bounds_add(c[k], d[k], p[i].min, p[i].max);
-            }
+            gather_bounds(p, lo, hi, a[k], b[k], c[k], d[k]);
         }
         for (int k = 0; k < parts; k++) {
             bounds_add(cmin, cmax, a[k], b[k]);
@@ -74,47 +118,41 @@ bool best_split(const Prim *p, size_t n, int &axis_out, float &at_out) {
         }
     }
     float leaf_cost = float(n) * area(pmin, pmax);
+    bool use[3];
+    float ext[3];
+    for (int axis = 0; axis < 3; axis++) {
+        ext[axis] = cmax[axis] - cmin[axis];
+        use[axis] = !(ext[axis] < 1e-6f);
+    }
+    Bins bins[3];
+    for (auto &q : bins) q.clear();
+    if (parts == 1) {
+        gather_bins(p, 0, n, use, cmin, ext, bins);
+    } else {
+        std::vector<Bins> runs(size_t(parts) * 3);
+        for (auto &q : runs) q.clear();
+#pragma omp parallel for schedule(static, 1)
+        for (int k = 0; k < parts; k++) {
+            size_t lo, hi;
+            run_of(n, k, parts, lo, hi);
+            gather_bins(p, lo, hi, use, cmin, ext, &runs[size_t(k) * 3]);
+        }
+        for (int k = 0; k < parts; k++)
+            for (int axis = 0; axis < 3; axis++)
+                for (size_t b = 0; b < BINS; b++) {
+                    const Bins &r = runs[size_t(k) * 3 + axis];
+                    bins[axis].mn[b] = bins[axis].mn[b].min(r.mn[b]);
+                    bins[axis].mx[b] = bins[axis].mx[b].max(r.mx[b]);
+                    bins[axis].n[b] += r.n[b];
+                }
+    }
     bool have = false;
     float best_cost = 0, best_at = 0;
     int best_axis = 0;
     for (int axis = 0; axis < 3; axis++) {
-        float extent = cmax[axis] - cmin[axis];
-        if (extent < 1e-6f) continue;
-        Vec3 bmin[BINS], bmax[BINS];
-        uint32_t bn[BINS];
-        for (size_t b = 0; b < BINS; b++) {
-            bmin[b] = Vec3::splat(INFINITY);
-            bmax[b] = Vec3::splat(-INFINITY);
-            bn[b] = 0;
-        }
-        Vec3 tmin[MAX_PARTS * BINS], tmax[MAX_PARTS * BINS];
-        uint32_t tn[MAX_PARTS * BINS];
-        for (size_t q = 0; q < size_t(parts) * BINS; q++) {
-            tmin[q] = Vec3::splat(INFINITY);
-            tmax[q] = Vec3::splat(-INFINITY);
-            tn[q] = 0;
-        }
-#pragma omp parallel for schedule(static, 1) if (parts > 1)
-        for (int k = 0; k < parts; k++) {
-            size_t lo, hi;
-            run_of(n, k, parts, lo, hi);
-            Vec3 *mn = &tmin[size_t(k) * BINS], *mx = &tmax[size_t(k) * BINS];
-            uint32_t *cn = &tn[size_t(k) * BINS];
-            for (size_t i = lo; i < hi; i++) {
-                float f = (p[i].centre[axis] - cmin[axis]) / extent * float(BINS);
-                size_t b = f > 0.0f ? size_t(f) : 0;  // Rust `as usize`: truncation, saturating at 0
-                if (b > BINS - 1) b = BINS - 1;
-                mn[b] = mn[b].min(p[i].min);
-                mx[b] = mx[b].max(p[i].max);
-                cn[b]++;
-            }
-        }
-        for (int k = 0; k < parts; k++)
-            for (size_t b = 0; b < BINS; b++) {
-                bmin[b] = bmin[b].min(tmin[size_t(k) * BINS + b]);
-                bmax[b] = bmax[b].max(tmax[size_t(k) * BINS + b]);
-                bn[b] += tn[size_t(k) * BINS + b];
-            }
+        if (!use[axis]) continue;
+        const float extent = ext[axis];
+        const Bins &q = bins[axis];
         // the bins' bounds and counts below and from each plane, swept once each way: min and max give the
         // reference's per-plane folds (bvh.rs:135-137) up to the sign of a zero, which no area changes
         // (max - min and its clamp at 0 are the same for either zero), so every cost compares the same
@@ -125,21 +163,20 @@ bool best_split(const Prim *p, size_t n, int &axis_out, float &at_out) {
             uint32_t c = 0;
             for (size_t b = 0; b < BINS; b++) {
                 lo_min[b] = mn, lo_max[b] = mx, lo_n[b] = c;  // bins [0, b)
-                bounds_add(mn, mx, bmin[b], bmax[b]);
-                c += bn[b];
+                bounds_add(mn, mx, q.mn[b], q.mx[b]);
+                c += q.n[b];
             }
             mn = Vec3::splat(INFINITY), mx = Vec3::splat(-INFINITY), c = 0;
             for (size_t b = BINS; b-- > 0;) {
-                bounds_add(mn, mx, bmin[b], bmax[b]);
-                c += bn[b];
+                bounds_add(mn, mx, q.mn[b], q.mx[b]);
+                c += q.n[b];
                 hi_min[b] = mn, hi_max[b] = mx, hi_n[b] = c;  // bins [b, BINS)
             }
         }
         for (size_t s = 1; s < BINS; s++) {
             uint32_t ln = lo_n[s], rn = hi_n[s];
-            Vec3 lmin = lo_min[s], lmax = lo_max[s], rmin = hi_min[s], rmax = hi_max[s];
             if (ln == 0 || rn == 0) continue;
-            float cost = float(ln) * area(lmin, lmax) + float(rn) * area(rmin, rmax);
+            float cost = float(ln) * area(lo_min[s], lo_max[s]) + float(rn) * area(hi_min[s], hi_max[s]);
             if (!have || cost < best_cost) {
                 have = true;
                 best_cost = cost;
@@ -179,10 +216,12 @@ void build_subtree(std::vector<Prim> &prims, size_t start0, size_t end0, std::ve
         Prim *slice = prims.data() + start;
         size_t n = end - start;
         Vec3 bmin = Vec3::splat(INFINITY), bmax = Vec3::splat(-INFINITY);
-        for (size_t i = 0; i < n; i++) bounds_add(bmin, bmax, slice[i].min, slice[i].max);
         int axis;
         float at;
-        bool split = n > LEAF && best_split(slice, n, axis, at);
+        bool split = false;
+        if (n > LEAF) split = best_split(slice, n, axis, at, bmin, bmax);
+        else
+            for (size_t i = 0; i < n; i++) bounds_add(bmin, bmax, slice[i].min, slice[i].max);
         if (!split) {
             set(ni, bmin, uint32_t(start), bmax, uint32_t(n));
             continue;
@@ -205,25 +244,60 @@ void build_subtree(std::vector<Prim> &prims, size_t start0, size_t end0, std::ve
 
 // bvh.rs:50-106
 Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)> &chart) {
-    std::vector<Prim> prims;
-    std::vector<Source> sources;
+    // bvh.rs:51-74: every casting triangle that is not degenerate, in mesh and triangle order. Done in
+    // parallel: each thread's contiguous run of the scene's triangles is counted, then written from the
+    // count of the runs before it (the same order and ids as one pass).
+    std::vector<size_t> mesh_first(scene.header.meshes.size() + 1, 0);
     for (size_t mi = 0; mi < scene.header.meshes.size(); mi++) {
         const MeshInfo &m = scene.header.meshes[mi];
-        if (!scene.header.materials[m.material].casts) continue;
+        const size_t nt = scene.header.materials[m.material].casts ? scene.positions[mi].size() / 3 : 0;
+        mesh_first[mi + 1] = mesh_first[mi] + nt;
+    }
+    const size_t n_all = mesh_first.back();
+    auto locate = [&](size_t g, size_t &mi, size_t &t) {
+        mi = size_t(std::upper_bound(mesh_first.begin(), mesh_first.end(), g) - mesh_first.begin()) - 1;
+        t = g - mesh_first[mi];
+    };
+    auto keeps = [&](size_t mi, size_t t) {
         const std::vector<Vec3> &p = scene.positions[mi];
-        for (size_t t = 0; t < p.size() / 3; t++) {
+        Vec3 a = p[t * 3], b = p[t * 3 + 1], c = p[t * 3 + 2];
+        return !((b - a).cross(c - a).length_squared() < 1e-14f);
+    };
+    const int runs_n = std::max(1, std::min(omp_get_max_threads() * 4, int((n_all + 4095) / 4096)));
+    std::vector<size_t> kept(size_t(runs_n) + 1, 0);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 0; k < runs_n; k++) {
+        size_t lo, hi, mi, t, c = 0;
+        run_of(n_all, k, runs_n, lo, hi);
+        for (size_t g = lo; g < hi; g++) {
+            locate(g, mi, t);
+            c += keeps(mi, t) ? 1 : 0;
+        }
+        kept[size_t(k) + 1] = c;
+    }
+    for (int k = 0; k < runs_n; k++) kept[size_t(k) + 1] += kept[size_t(k)];
+    std::vector<Prim> prims(kept.back());
+    std::vector<Source> sources(kept.back());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 0; k < runs_n; k++) {
+        size_t lo, hi, mi, t, at = kept[size_t(k)];
+        run_of(n_all, k, runs_n, lo, hi);
+        for (size_t g = lo; g < hi; g++) {
+            locate(g, mi, t);
+            if (!keeps(mi, t)) continue;
+            const MeshInfo &m = scene.header.meshes[mi];
+            const std::vector<Vec3> &p = scene.positions[mi];
             Vec3 a = p[t * 3], b = p[t * 3 + 1], c = p[t * 3 + 2];
             Vec3 e1 = b - a, e2 = c - a;
-            if (e1.cross(e2).length_squared() < 1e-14f) continue;
-            Prim q;
+            Prim &q = prims[at];
             q.min = a.min(b).min(c);
             q.max = a.max(b).max(c);
             q.centre = (a + b + c) / 3.0f;
-            q.id = uint32_t(sources.size());
-            sources.push_back(Source{lb_tri{{a.x, a.y, a.z, u2f(m.material)}, {e1.x, e1.y, e1.z, u2f(chart(mi, t))},
-                                            {e2.x, e2.y, e2.z, 0.0f}},
-                                     uint32_t(mi), uint32_t(t)});
-            prims.push_back(q);
+            q.id = uint32_t(at);
+            sources[at] = Source{lb_tri{{a.x, a.y, a.z, u2f(m.material)}, {e1.x, e1.y, e1.z, u2f(chart(mi, t))},
+                                        {e2.x, e2.y, e2.z, 0.0f}},
+                                 uint32_t(mi), uint32_t(t)};
+            at++;
         }
     }
     Bvh out;
@@ -267,12 +341,14 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
         }
         Prim *slice = prims.data() + start;
         Vec3 bmin = Vec3::splat(INFINITY), bmax = Vec3::splat(-INFINITY);
-        for (size_t i = 0; i < n; i++) bounds_add(bmin, bmax, slice[i].min, slice[i].max);
-        top[id].bmin = bmin;
-        top[id].bmax = bmax;
         int axis;
         float at;
-        bool split = n > LEAF && best_split(slice, n, axis, at);
+        bool split = false;
+        if (n > LEAF) split = best_split(slice, n, axis, at, bmin, bmax);
+        else
+            for (size_t i = 0; i < n; i++) bounds_add(bmin, bmax, slice[i].min, slice[i].max);
+        top[id].bmin = bmin;
+        top[id].bmax = bmax;
         size_t mid = 0;
         if (split) {
             mid = start + partition(slice, n, axis, at);
@@ -323,11 +399,13 @@ Bvh Bvh::build(const Scene &scene, const std::function<uint32_t(size_t, size_t)>
             stack.emplace_back(left, t.left);
         }
     }
-    out.tris.reserve(prims.size());
-    for (auto &p : prims) out.tris.push_back(sources[p.id].tri);
+    out.tris.resize(prims.size());
     out.source.resize(prims.size());
     out.verts.resize(prims.size() * 9);
-    for (size_t i = 0; i < prims.size(); i++) {
+#pragma omp parallel for schedule(static)
+    for (long long ii = 0; ii < (long long)prims.size(); ii++) {
+        const size_t i = size_t(ii);
+        out.tris[i] = sources[prims[i].id].tri;
         const Source &src = sources[prims[i].id];
         out.source[i] = {src.mesh, src.index};
         const std::vector<Vec3> &p = scene.positions[src.mesh];

@@ -19,7 +19,7 @@ struct Bvh {
     std::vector<float> verts;
     // each triangle's mesh and its index there, in `tris` order
     std::vector<std::array<uint32_t, 2>> source;
-    // chart(mesh, triangle): the triangle's chart (0xffffffff: none)
+    // chart(mesh, triangle): the triangle's chart (0xffffffff: none); called from several threads at once
     static Bvh build(const Scene &scene, const std::function<uint32_t(size_t, size_t)> &chart);
     // the triangles' chart bits (e1.w) written again from chart(mesh, triangle): a BVH built before the layout
     // (the tree does not depend on them) gets the bits a build after it would have written

@@ -4,14 +4,31 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 
 namespace lb {
 
 // std::fmin / std::fmax as the C library computes them (the non-NaN argument when one is NaN, the first
 // of two equal values, so +0 or -0 as given), written out so that the compiler inlines them: the BVH
-// build and the layout call them for every primitive of every node.
+// build and the layout call them for every primitive of every node. On x86 the choice is made with
+// SSE masks rather than branches (a box's bound moves with no pattern a branch predictor can follow).
+#if defined(__SSE2__)
+inline float fmin_(float a, float b) {
+    const __m128 va = _mm_set_ss(a), vb = _mm_set_ss(b);
+    const __m128 take_b = _mm_or_ps(_mm_cmplt_ss(vb, va), _mm_cmpunord_ss(va, va));
+    return _mm_cvtss_f32(_mm_or_ps(_mm_and_ps(take_b, vb), _mm_andnot_ps(take_b, va)));
+}
+inline float fmax_(float a, float b) {
+    const __m128 va = _mm_set_ss(a), vb = _mm_set_ss(b);
+    const __m128 take_b = _mm_or_ps(_mm_cmpgt_ss(vb, va), _mm_cmpunord_ss(va, va));
+    return _mm_cvtss_f32(_mm_or_ps(_mm_and_ps(take_b, vb), _mm_andnot_ps(take_b, va)));
+}
+#else
 inline float fmin_(float a, float b) { return (b < a || a != a) ? b : a; }
 inline float fmax_(float a, float b) { return (b > a || a != a) ? b : a; }
+#endif
 
 struct Vec2 {
     float x = 0, y = 0;
