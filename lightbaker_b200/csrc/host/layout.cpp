@@ -5,6 +5,7 @@
 #include <cmath>
 #include <map>
 #include <stdexcept>
+#include <string>
 #include <unordered_map>
 
 namespace lb {
@@ -48,43 +49,89 @@ struct Key3Hash {
 };
 
 // layout.rs:129-171: charts by region growing across shared vertices, neighbours facing within `cos` of
-// the seed and in its tile (by the centre of the triangle's box); each group in triangle order
+// the seed and in its tile (by the centre of the triangle's box); each group in triangle order, the groups
+// in the order of their seeds (each the lowest triangle not yet taken).
+//
+// A group never leaves its seed's tile, so the tiles are grown apart, in parallel: a tile's groups depend
+// only on its own triangles (their seeds, in index order, are the ones the whole-mesh walk meets there),
+// and each group's first triangle is its seed, so sorting all groups by their first triangle gives the
+// whole-mesh walk's order.
 std::vector<std::vector<uint32_t>> grow(const std::vector<Vec3> &pos, float cosv, float tile) {
-    size_t n = pos.size() / 3;
+    const size_t n = pos.size() / 3;
     std::vector<Vec3> normals(n);
     std::vector<TileKey> keys(n);
-    for (size_t t = 0; t < n; t++) {
-        normals[t] = face_normal(pos, t);
-        keys[t] = tile_of(box_centre(pos, t), tile);
+#pragma omp parallel for schedule(static)
+    for (long long ti = 0; ti < (long long)n; ti++) {
+        normals[ti] = face_normal(pos, size_t(ti));
+        keys[ti] = tile_of(box_centre(pos, size_t(ti)), tile);
+    }
+    // the triangles of each tile, in index order
+    std::map<TileKey, uint32_t> tile_id;
+    std::vector<uint32_t> id_of(n), count;
+    {
+        TileKey last{INT32_MIN, INT32_MIN};
+        uint32_t last_id = 0;
+        for (size_t t = 0; t < n; t++) {
+            if (t == 0 || keys[t] != last) {
+                auto it = tile_id.emplace(keys[t], uint32_t(tile_id.size())).first;
+                last = keys[t];
+                last_id = it->second;
+                if (last_id == count.size()) count.push_back(0);
+            }
+            id_of[t] = last_id;
+            count[last_id]++;
+        }
+    }
+    const size_t nt = count.size();
+    std::vector<size_t> first(nt + 1, 0);
+    for (size_t k = 0; k < nt; k++) first[k + 1] = first[k] + count[k];
+    std::vector<uint32_t> members(n);
+    {
+        std::vector<size_t> at = first;
+        for (size_t t = 0; t < n; t++) members[at[id_of[t]]++] = uint32_t(t);
     }
     auto key = [](Vec3 v) {
         return Key3{{as_i64(std::round(v.x * 1e4f)), as_i64(std::round(v.y * 1e4f)), as_i64(std::round(v.z * 1e4f))}};
     };
-    std::unordered_map<Key3, std::vector<uint32_t>, Key3Hash> at;
-    at.reserve(n * 2);
-    for (size_t t = 0; t < n; t++)
-        for (int k = 0; k < 3; k++) at[key(pos[t * 3 + k])].push_back(uint32_t(t));
+    // (a triangle is in one tile, so the tiles' threads write disjoint flags)
     std::vector<char> taken(n, 0);
-    std::vector<std::vector<uint32_t>> out;
-    for (size_t seed = 0; seed < n; seed++) {
-        if (taken[seed]) continue;
-        taken[seed] = 1;
-        std::vector<uint32_t> group{uint32_t(seed)};
-        Vec3 sn = normals[seed];
-        TileKey sk = keys[seed];
-        for (size_t i = 0; i < group.size(); i++) {
-            size_t t = group[i];
-            for (int k = 0; k < 3; k++) {
-                for (uint32_t o : at[key(pos[t * 3 + k])]) {
-                    if (taken[o] || keys[o] != sk || normals[o].dot(sn) < cosv) continue;
-                    taken[o] = 1;
-                    group.push_back(o);
+    std::vector<std::vector<std::vector<uint32_t>>> per_tile(nt);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long k = 0; k < (long long)nt; k++) {
+        const uint32_t *tris = members.data() + first[k];
+        const size_t m = first[k + 1] - first[k];
+        std::unordered_map<Key3, std::vector<uint32_t>, Key3Hash> at;
+        at.reserve(m * 2);
+        for (size_t i = 0; i < m; i++)
+            for (int c = 0; c < 3; c++) at[key(pos[size_t(tris[i]) * 3 + c])].push_back(tris[i]);
+        auto &out = per_tile[k];
+        for (size_t i = 0; i < m; i++) {
+            const uint32_t seed = tris[i];
+            if (taken[seed]) continue;
+            taken[seed] = 1;
+            std::vector<uint32_t> group{seed};
+            Vec3 sn = normals[seed];
+            TileKey sk = keys[seed];
+            for (size_t j = 0; j < group.size(); j++) {
+                size_t t = group[j];
+                for (int c = 0; c < 3; c++) {
+                    for (uint32_t o : at[key(pos[t * 3 + c])]) {
+                        if (taken[o] || keys[o] != sk || normals[o].dot(sn) < cosv) continue;
+                        taken[o] = 1;
+                        group.push_back(o);
+                    }
                 }
             }
+            std::sort(group.begin(), group.end());
+            out.push_back(std::move(group));
         }
-        std::sort(group.begin(), group.end());
-        out.push_back(std::move(group));
     }
+    std::vector<std::vector<uint32_t>> out;
+    for (auto &v : per_tile)
+        for (auto &g : v) out.push_back(std::move(g));
+    std::sort(out.begin(), out.end(), [](const std::vector<uint32_t> &a, const std::vector<uint32_t> &b) {
+        return a[0] < b[0];
+    });
     return out;
 }
 
@@ -294,15 +341,35 @@ Layout Layout::build(const Scene &scene) {
     for (size_t mi = 0; mi < scene.header.meshes.size(); mi++) {
         const MeshInfo &m = scene.header.meshes[mi];
         if (!scene.header.materials[m.material].receives) continue;
-        for (auto &group : grow(scene.positions[mi], cosv, s.tile_size)) {
-            Chart c = make_chart(scene.positions[mi], uint32_t(mi), group, s.tile_size, L.density, L.padding);
+        std::vector<std::vector<uint32_t>> groups = grow(scene.positions[mi], cosv, s.tile_size);
+        // each group's chart on its own (in parallel), numbered in group order
+        std::vector<Chart> made(groups.size());
+#pragma omp parallel for schedule(dynamic, 64)
+        for (long long g = 0; g < (long long)groups.size(); g++)
+            made[g] = make_chart(scene.positions[mi], uint32_t(mi), std::move(groups[g]), s.tile_size, L.density,
+                                 L.padding);
+        for (Chart &c : made) {
             for (uint32_t t : c.tris) L.tri_chart[mi][t] = uint32_t(L.charts.size());
             L.charts.push_back(std::move(c));
         }
     }
     std::map<TileKey, std::vector<uint32_t>> by_tile;
     for (size_t i = 0; i < L.charts.size(); i++) by_tile[L.charts[i].tile].push_back(uint32_t(i));
-    for (auto &kv : by_tile) L.tiles.push_back(pack_tile(kv.first, kv.second, L.charts));
+    // the tiles packed apart (in parallel: a tile's packing reads and moves only its own charts), kept in
+    // tile order
+    std::vector<std::pair<TileKey, std::vector<uint32_t>>> todo(by_tile.begin(), by_tile.end());
+    L.tiles.resize(todo.size());
+    std::vector<std::string> failed(todo.size());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long k = 0; k < (long long)todo.size(); k++) {
+        try {
+            L.tiles[k] = pack_tile(todo[k].first, todo[k].second, L.charts);
+        } catch (const std::exception &e) {
+            failed[k] = e.what();
+        }
+    }
+    for (const std::string &f : failed)
+        if (!f.empty()) throw std::runtime_error(f);
     L.height = shelve(L.tiles, s.atlas_width);
     L.width = s.atlas_width;
     return L;
