@@ -316,7 +316,8 @@ class Stats:
 
 class Bake:
     """A bake's results (bake.rs:36-47): `direct` (h, w, 2) field and occlusion, `indirect` (ih, iw, 3),
-    `validity` (h, w), `volume` (probes, 4, 4) or None, `stats`."""
+    `validity` (h, w), `volume` (probes, 4, 4) or None, `stats`. The results are in host memory when the
+    bake returns (in the handle); each array is copied out of it on first access."""
 
     def __init__(self, handle: int):
         self._h = handle
@@ -325,29 +326,53 @@ class Bake:
         self.info = info
         w, h, iw, ih = info.width, info.height, info.indirect_width, info.indirect_height
         self.width, self.height, self.indirect_size = w, h, (iw, ih)
-        self.direct = np.zeros((h, w, 2), np.float32)
-        N.check(N.lib().lb_bake_get_direct(handle, N.ptr(self.direct)), "direct")
-        self.indirect = np.zeros((ih, iw, 3), np.float32)
-        N.check(N.lib().lb_bake_get_indirect(handle, N.ptr(self.indirect)), "indirect")
-        self.validity = np.zeros((h, w), np.uint8)
-        N.check(N.lib().lb_bake_get_validity(handle, N.ptr(self.validity)), "validity")
-        self.volume = None
+        self._arrays = {}
         if info.has_volume:
-            nx, ny, nz = info.volume_size
-            self.volume = np.zeros((nx * ny * nz, 4, 4), np.float32)
-            N.check(N.lib().lb_bake_get_volume(handle, N.ptr(self.volume)), "volume")
-            self.volume_size = (nx, ny, nz)
+            self.volume_size = tuple(info.volume_size)
             self.volume_origin = tuple(info.volume_origin)
             self.volume_step = info.volume_step
-        self.charts = np.zeros((info.n_charts, 8), np.float32)
-        if info.n_charts:
-            N.check(N.lib().lb_bake_get_charts(handle, N.ptr(self.charts)), "charts")
-        self.tri_charts = np.zeros(info.n_triangles, np.uint32)
-        if info.n_triangles:
-            N.check(N.lib().lb_bake_get_tri_charts(handle, N.ptr(self.tri_charts)), "triangle charts")
         self.stats = Stats(info.tiles, info.tiles_baked, info.texels_baked, info.chunks, info.chunks_baked,
                            info.seconds, info.rays_direct, info.rays_gather, info.rays_volume, info.t_layout,
                            info.t_direct, info.t_bounces, info.t_volume, info.t_composite)
+
+    def _array(self, name, shape, dtype, getter):
+        a = self._arrays.get(name)
+        if a is None:
+            if not self._h:
+                raise LightbakerError("the bake is closed")
+            a = np.zeros(shape, dtype)
+            if a.size:
+                N.check(getter(self._h, N.ptr(a)), name)
+            self._arrays[name] = a
+        return a
+
+    @property
+    def direct(self) -> np.ndarray:
+        return self._array("direct", (self.height, self.width, 2), np.float32, N.lib().lb_bake_get_direct)
+
+    @property
+    def indirect(self) -> np.ndarray:
+        iw, ih = self.indirect_size
+        return self._array("indirect", (ih, iw, 3), np.float32, N.lib().lb_bake_get_indirect)
+
+    @property
+    def validity(self) -> np.ndarray:
+        return self._array("validity", (self.height, self.width), np.uint8, N.lib().lb_bake_get_validity)
+
+    @property
+    def volume(self):
+        if not self.info.has_volume:
+            return None
+        nx, ny, nz = self.volume_size
+        return self._array("volume", (nx * ny * nz, 4, 4), np.float32, N.lib().lb_bake_get_volume)
+
+    @property
+    def charts(self) -> np.ndarray:
+        return self._array("charts", (self.info.n_charts, 8), np.float32, N.lib().lb_bake_get_charts)
+
+    @property
+    def tri_charts(self) -> np.ndarray:
+        return self._array("tri_charts", (self.info.n_triangles,), np.uint32, N.lib().lb_bake_get_tri_charts)
 
     @property
     def device_encoded(self) -> bool:

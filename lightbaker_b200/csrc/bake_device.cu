@@ -963,9 +963,20 @@ lb::Bake lb_plan_collect(lb_plan &p) {
     if (lb_plan_rays(&p, rays) != LB_OK) throw std::runtime_error(lb_last_error());
     const double t_down = since(t0);
     const float *ind = (const float *)(stage + o_ind), *probes = (const float *)(stage + o_pr);
+    // out of the staging buffer by all host threads (tens of MB: one thread's copy is the collection's
+    // largest host cost)
+    auto copy = [](void *dst, const void *src, size_t bytes) {
+        const size_t piece = size_t(1) << 20, n = (bytes + piece - 1) / piece;
+#pragma omp parallel for schedule(static) if (n > 4)
+        for (long long k = 0; k < (long long)n; k++) {
+            const size_t at = size_t(k) * piece;
+            std::memcpy((char *)dst + at, (const char *)src + at, std::min(piece, bytes - at));
+        }
+    };
     out.direct.resize(A);
-    std::memcpy(out.direct.data(), stage, A * 8);
-    out.validity.assign((const uint8_t *)stage + o_val, (const uint8_t *)stage + o_val + A);
+    copy(out.direct.data(), stage, A * 8);
+    out.validity.resize(A);
+    copy(out.validity.data(), stage + o_val, A);
     out.indirect.resize(n_ind);
     auto *oi = out.indirect.data();
 #pragma omp parallel for schedule(static)
@@ -974,9 +985,10 @@ lb::Bake lb_plan_collect(lb_plan &p) {
     out.ih = p.ih;
     if (p.aw % 4 == 0 && p.ah % 4 == 0) {
         lb::Encoded enc;
-        enc.bc5.assign((const uint8_t *)stage + o_bc5, (const uint8_t *)stage + o_bc5 + A);
+        enc.bc5.resize(A);
+        copy(enc.bc5.data(), stage + o_bc5, A);
         enc.rgb9e5.resize(n_ind);
-        std::memcpy(enc.rgb9e5.data(), stage + o_rgb, n_ind * 4);
+        copy(enc.rgb9e5.data(), stage + o_rgb, n_ind * 4);
         if (p.has_volume) {
             enc.volume.assign((const uint8_t *)stage + o_vb, (const uint8_t *)stage + o_vb + size_t(p.n_probes) * 16);
             std::memcpy(&enc.volume_scale, stage + o_sc, 4);
@@ -989,7 +1001,7 @@ lb::Bake lb_plan_collect(lb_plan &p) {
         v.step = h.volume->step;
         v.size = p.vsize;
         v.probes.resize(p.n_probes);
-        std::memcpy(v.probes.data(), probes, n_pr * 4);
+        copy(v.probes.data(), probes, n_pr * 4);
         v.chunks = p.n_chunks;
         v.chunks_baked = p.chunk_keys.size();
         out.volume = std::move(v);

@@ -1,6 +1,9 @@
 #include "blake3.h"
 
+#include <algorithm>
+#include <array>
 #include <cstring>
+#include <vector>
 
 namespace lb {
 
@@ -169,10 +172,61 @@ std::string Blake3::hex() const {
     return to_hex(h, 32);
 }
 
+namespace {
+// chunk `index` of `data` (1 to 1024 bytes): its chaining value, or (root) the root output's first words
+void chunk_cv(const uint8_t *p, size_t bytes, uint64_t index, bool root, uint32_t out[8]) {
+    uint32_t cv[8], w[16], o[16];
+    std::memcpy(cv, IV, 32);
+    const size_t blocks = bytes == 0 ? 1 : (bytes + 63) / 64;
+    for (size_t b = 0; b < blocks; b++) {
+        const size_t blen = b + 1 < blocks ? 64 : bytes - b * 64;
+        uint8_t block[64] = {0};
+        std::memcpy(block, p + b * 64, blen);
+        words(block, w);
+        const uint32_t flags =
+            (b == 0 ? CHUNK_START : 0) | (b + 1 == blocks ? CHUNK_END : 0) | (root && b + 1 == blocks ? ROOT : 0);
+        compress(cv, w, index, uint32_t(blen), flags, o);
+        std::memcpy(cv, o, 32);
+    }
+    std::memcpy(out, cv, 32);
+}
+}  // namespace
+
+// One call over the whole input. From 64 KiB on, the chunks' chaining values are computed in parallel
+// and merged pair by pair, level by level (an odd last node goes up as it is): that builds the same
+// left-balanced tree the incremental hasher folds (every left subtree the largest power of two of chunks
+// below the node's count), so the digest is the same.
 void blake3_hash(const void *data, size_t len, uint8_t out[32]) {
-    Blake3 h;
-    h.update(data, len);
-    h.finalize(out);
+    const size_t chunks = (len + CHUNK - 1) / CHUNK;
+    if (len < (size_t(64) << 10) || chunks < 2) {
+        Blake3 h;
+        h.update(data, len);
+        h.finalize(out);
+        return;
+    }
+    const uint8_t *p = (const uint8_t *)data;
+    std::vector<std::array<uint32_t, 8>> level(chunks);
+#pragma omp parallel for schedule(static)
+    for (long long c = 0; c < (long long)chunks; c++) {
+        const size_t at = size_t(c) * CHUNK;
+        chunk_cv(p + at, std::min(CHUNK, len - at), uint64_t(c), false, level[size_t(c)].data());
+    }
+    while (level.size() > 2) {
+        std::vector<std::array<uint32_t, 8>> up((level.size() + 1) / 2);
+#pragma omp parallel for schedule(static) if (level.size() > 4096)
+        for (long long k = 0; k < (long long)(level.size() / 2); k++)
+            parent_cv(level[2 * size_t(k)].data(), level[2 * size_t(k) + 1].data(), 0, up[size_t(k)].data());
+        if (level.size() % 2) up.back() = level.back();
+        level.swap(up);
+    }
+    uint32_t root[8];
+    parent_cv(level[0].data(), level[1].data(), ROOT, root);
+    for (int k = 0; k < 8; k++) {
+        out[4 * k] = uint8_t(root[k]);
+        out[4 * k + 1] = uint8_t(root[k] >> 8);
+        out[4 * k + 2] = uint8_t(root[k] >> 16);
+        out[4 * k + 3] = uint8_t(root[k] >> 24);
+    }
 }
 
 }  // namespace lb
