@@ -1,7 +1,9 @@
 #include "raster.h"
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstring>
 
 namespace lb {
 
@@ -95,6 +97,56 @@ std::vector<RasterTri> raster_triangles(const Scene &scene, const Layout &layout
                                     s.x0, s.y0, s.x1, s.y1, ci, tile_index, 0});
         }
     }
+    return out;
+}
+
+std::vector<RasterTri> raster_triangles(const Scene &scene, const Layout &layout, const std::vector<size_t> &tiles) {
+    // every (tile, chart) in order, with the count of (chart, triangle) pairs before it
+    struct Span {
+        uint32_t tile_k, chart;
+        size_t first;
+    };
+    std::vector<Span> spans;
+    size_t total = 0;
+    for (size_t k = 0; k < tiles.size(); k++)
+        for (uint32_t ci : layout.tiles[tiles[k]].charts) {
+            spans.push_back(Span{uint32_t(k), ci, total});
+            total += layout.charts[ci].tris.size();
+        }
+    const size_t RUN = 16384, runs = (total + RUN - 1) / RUN;
+    std::vector<std::vector<RasterTri>> part(runs);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long r = 0; r < (long long)runs; r++) {
+        const size_t lo = size_t(r) * RUN, hi = std::min(total, lo + RUN);
+        // the span holding pair `lo`, then on in order
+        size_t si = size_t(std::upper_bound(spans.begin(), spans.end(), lo,
+                                            [](size_t v, const Span &sp) { return v < sp.first; }) -
+                           spans.begin()) -
+                    1;
+        std::vector<RasterTri> &out = part[size_t(r)];
+        out.reserve(hi - lo);
+        for (size_t at = lo; at < hi; si++) {
+            const Span &sp = spans[si];
+            const Tile &tile = layout.tiles[tiles[sp.tile_k]];
+            const Chart &c = layout.charts[sp.chart];
+            const std::vector<Vec3> &pos = scene.positions[c.mesh];
+            for (size_t j = at - sp.first; j < c.tris.size() && at < hi; j++, at++) {
+                Setup s;
+                if (!setup(layout, c, pos, c.tris[j], int32_t(tile.w), int32_t(tile.h), s)) continue;
+                out.push_back(RasterTri{{s.ua.x, s.ua.y}, {s.ub.x, s.ub.y}, {s.uc.x, s.uc.y}, s.det,
+                                        {s.pa.x, s.pa.y, s.pa.z}, {s.pb.x, s.pb.y, s.pb.z}, {s.pc.x, s.pc.y, s.pc.z},
+                                        {s.n.x, s.n.y, s.n.z}, {s.dx.x, s.dx.y, s.dx.z}, {s.dy.x, s.dy.y, s.dy.z},
+                                        s.x0, s.y0, s.x1, s.y1, sp.chart, sp.tile_k, 0});
+            }
+        }
+    }
+    std::vector<size_t> first(runs + 1, 0);
+    for (size_t r = 0; r < runs; r++) first[r + 1] = first[r] + part[r].size();
+    std::vector<RasterTri> out(first.back());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long r = 0; r < (long long)runs; r++)
+        if (!part[size_t(r)].empty())
+            std::memcpy(out.data() + first[size_t(r)], part[size_t(r)].data(), part[size_t(r)].size() * sizeof(RasterTri));
     return out;
 }
 

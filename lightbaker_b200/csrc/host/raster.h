@@ -33,5 +33,9 @@ namespace lb {
 // The tile's triangles in the order rasterize() visits them (charts in tile order, each chart's
 // triangles in order), set up with the same arithmetic; degenerate ones (|det| < 1e-12) left out.
 std::vector<RasterTri> raster_triangles(const Scene &scene, const Layout &layout, const Tile &tile, uint32_t tile_index);
+// The same for several tiles, concatenated in list order (tile k's triangles carry tile index k): the work
+// is split into equal runs of (chart, triangle) pairs across the tiles, set up by all host threads, so one
+// large tile does not hold up the rest.
+std::vector<RasterTri> raster_triangles(const Scene &scene, const Layout &layout, const std::vector<size_t> &tiles);
 
 }  // namespace lb
