@@ -181,12 +181,14 @@ int lb_set_ray_order(lb_gpu *gpu, int direct, int gather);
 /* Leaf lists for the warp kernels' direct pass over the BVH2 (default on): a warp gathers once for a
  * texel the leaves within the occlusion reach (widened by its farthest candidate point) of its own point,
  * on its front side, nearest first, and its inside-test and occlusion rays test that list instead of
- * walking the tree. Same hits (between triangles at exactly equal distance the first found in list
- * order). */
+ * walking the tree. Same results: a ray whose list walk meets a tie the tree walk could settle another
+ * way (an exact tie, or a near one where the hit's box entry rounds up to the hit) walks the tree. */
 int lb_set_near(lb_gpu *gpu, int on);
 /* Register cap of the warp kernels over the BVH2 (direct and gather, without counting): 0 (default) the
  * compiler's own budget; 3 or 4 registers capped so that this many 256-thread blocks share an SM (more
- * warps in flight, some values spilled). Same results. */
+ * warps in flight, some values spilled). Same results. With 0, lb_bake_device and lb_plan_create without
+ * autotuning use their own shapes: the 3-block cap without the shared sun walk (lb_set_warp_walk) for the
+ * direct pass, the 4-block cap for the gathers; with 3 or 4 they use the handle's cap and walk. */
 int lb_set_register_cap(lb_gpu *gpu, int blocks);
 /* Lane refill in the warp kernels' occlusion and gather rays over the BVH2 (default off): a lane whose
  * ray has ended starts the item's next one instead of waiting for its round. Same results. */
