@@ -594,7 +594,8 @@ def main():
                    "checkpoint_bytes": {"every_bounce": int(shape.checkpoint_bytes), "one": int(one_bytes)},
                    "bounces": int(shape.bounces), "params": int(shape.n_params), "records": int(shape.records),
                    "lit_records": int(shape.lit_records),
-                   "fallback_texels_not_differentiated": fallback_texels,
+                   "fallback_texels": fallback_texels,
+                   "volume_records": int(len(tr.export("volume_records"))),
                    "gradient_check": {"loss": "L2 to a target baked at theta0 + N(0, 0.05)", "h": h,
                                       "max_rel_err": max(c["rel_err"] for c in checks), "params": checks},
                    "note": "device time of one forward (theta on the device to the indirect atlas) and one "

@@ -392,8 +392,10 @@ void lb_plan_free(lb_plan *plan);
  * horizon and ground (rgb each, scene.rs:53-60), and the sun's intensity as a scale on its irradiance
  * (1 = the scene's own). lb_transport_theta0 gives the scene's own theta; forward at it gives the
  * device bake's indirect atlas bit for bit. Visibility does not depend on theta: create traces every
- * gather ray once and records what it met. Texels lit by the volume's fallback (validity 5) keep their
- * light at the scene's own theta.
+ * gather ray once and records what it met. Texels lit by the volume's fallback (validity 5,
+ * bake.rs:335-359) take their light from the probes, which the transport evaluates from its own last
+ * bounce's light and theta (create records every volume ray too), then fills and interpolates as the
+ * bake does; the adjoint runs those steps transposed (the cosine lobe's clamp at 0 as in the forward).
  *
  * create bakes the scene once on the device (every tile, no cache) and keeps what the transport reads;
  * max_checkpoints bounds the light atlases the forward keeps for the backward (0: one a bounce); with
@@ -422,7 +424,9 @@ int lb_transport_bake_indirect(lb_transport *t, float *indirect);
  * "light_flags", "tiles", "smooth_weights", "shape"; and the bake's arrays as it left them: "direct_records"
  * (the direct pass's record of each covered texel), "valid", "field", "ao", "direct" and "indirect_light"
  * (float4 a texel), "gather_out" (the last bounce's gather results), "light" (the last light atlas),
- * "probes"): its size in bytes when out is NULL, else the bytes copied (0 on error). */
+ * "probes"; and the volume's share, empty when no texel takes the fallback: "volume_records",
+ * "volume_items", "volume_slots", "volume_raw" (the probes before the fill), "volume_grid"): its size in
+ * bytes when out is NULL, else the bytes copied (0 on error). */
 size_t lb_transport_export(lb_transport *t, const char *name, void *out, size_t cap);
 void lb_transport_free(lb_transport *t);
 

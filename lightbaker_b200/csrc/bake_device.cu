@@ -421,6 +421,9 @@ void build(lb_plan &p) {
     p.theta0.alloc(theta.size() * 4);
     bool recording = (p.reuse && b.gi_bounces > 1) || (p.keep_records && b.gi_bounces > 0);
     p.records.alloc(recording ? p.max_gathered * p.P.params.counts[2] * 8 : 16);
+    const bool vrecording = p.keep_records && h.volume && p.n_todo;
+    p.vrecords.alloc(vrecording ? size_t(p.n_todo) * h.volume->rays * 8 : 16);
+    p.vraw.alloc(vrecording ? size_t(p.n_probes) * 64 : 16);
 
     mark("allocations");
     auto up = [&](DBuf &d, const void *src, size_t bytes) {
@@ -727,8 +730,12 @@ void capture(lb_plan &p) {
                 vw.bvh = p.bvh_volume;
                 vw.part = part;
                 vw.parts = parts;
+                vw.rec = p.keep_records ? p.vrecords.as<uint2>() : nullptr;
                 ck(lb_launch_pass_warp(vw, st), "volume pass");
                 cut(p.probes.p, size_t(p.n_probes) * 16);
+                if (p.keep_records)
+                    ck(cudaMemcpyAsync(p.vraw.p, p.probes.p, size_t(p.n_probes) * 64, cudaMemcpyDeviceToDevice, st),
+                       "raw probes");
             }
             ck(lb_volume_fill(p.probes.as<float4>(), p.probes_b.as<float4>(), p.pk_a.as<uint8_t>(), p.pk_b.as<uint8_t>(),
                               p.vsize[0], p.vsize[1], p.vsize[2], 8, st),

@@ -135,6 +135,17 @@ __device__ __forceinline__ float3 sun_disc(const lb_params &P, const Frame &sf, 
     sincos32(a, &s, &c);
     return norm3(add(add(xyz(P.sun_dir), scl(scl(sf.t, c), r)), scl(scl(sf.b, s), r)));
 }
+// trace.wgsl:289-295: volume ray r of a probe whose seeds are s1, s2 (of frays rays), uniform over the sphere
+__device__ __forceinline__ float3 volume_ray(uint32_t r, float frays, float s1, float s2) {
+    float u = fract((__uint2float_rn(r) + 0.5f) / frays + s1);
+    float v = fract(radical(r) + s2);
+    float z = 1.0f - 2.0f * u;
+    float rr = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    float a = v * 2.0f * PI;
+    float sa, ca;
+    sincos32(a, &sa, &ca);
+    return mk(rr * ca, z, rr * sa);
+}
 // trace.wgsl:152-156
 __device__ __forceinline__ float2 offset(uint32_t q) {
     if (q <= 4u) return make_float2((q & 1u) ? 0.3f : -0.3f, q > 2u ? 0.3f : -0.3f);

@@ -42,7 +42,8 @@ struct WarpPass {
     int near;                 // BVH2 occlusion rays: test a leaf list gathered once an item (lb_device.cuh)
     int occ;                  // BVH2 direct and gather passes without counting: 3 or 4 caps registers so that
                               // this many 256-thread blocks fit an SM; else the compiler's own budget
-    uint2 *rec;               // optional (gather): every ray's outcome, [item][ray] (lb_device.cuh gather_record)
+    uint2 *rec;               // optional (gather, volume): every ray's outcome, [item][ray] (lb_device.cuh
+                              // gather_record)
     unsigned int *work;       // optional (direct, gather): a counter the launch zeroes, from which warps take
                               // their next item as they free up; null: a static stride over the items
     int warp_walk;            // direct pass over the BVH2 without counting: a texel's sun rays walk the tree

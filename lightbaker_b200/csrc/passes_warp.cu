@@ -659,7 +659,7 @@ template <int BVH, bool COUNT, bool WT = false>
 __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const float4 *tex, uint32_t n_all,
                                                    const float4 *light, uint32_t n_light, float4 *out,
                                                    const uint32_t *slot, unsigned long long *counters, uint32_t part,
-                                                   uint32_t parts) {
+                                                   uint32_t parts, uint2 *rec) {
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -681,20 +681,14 @@ __global__ void __launch_bounds__(256) volume_warp(Scene S, lb_params P, const f
             bool on = r < rays, bk = false;
             float3 t0 = mk(0.f, 0.f, 0.f), tx = t0, ty = t0, tz = t0;
             if (on) {
-                float u = fract((__uint2float_rn(r) + 0.5f) / frays + s1);
-                float v = fract(radical(r) + s2);
-                float z = 1.0f - 2.0f * u;
-                float rr = sqrtf(fmaxf(0.0f, 1.0f - z * z));
-                float a = v * 2.0f * PI;
-                float sa, ca;
-                sincos32(a, &sa, &ca);
-                float3 d = mk(rr * ca, z, rr * sa);
+                float3 d = volume_ray(r, frays, s1, s2);
                 Hit h = walk<BVH, COUNT, WT>(S, o, d, P.reach[1], false, key + r, seed, c);
                 float3 l = sky(P, d);
                 if (h.tri != NONE) {
                     bk = h.back;
                     l = h.back ? mk(0.f, 0.f, 0.f) : bounced(S, P, light, n_light, o, d, h);
                 }
+                if (rec) rec[size_t(k) * rays + r] = gather_record(S, P, n_light, o, d, h);
                 t0 = scl(l, 0.282095f);
                 float3 lw = scl(l, 0.488603f);
                 tx = scl(lw, d.x);
@@ -778,7 +772,7 @@ void launch_walk(const WarpPass &w, int blocks, cudaStream_t stream) {
         break;
     default:
         lbd::volume_warp<BVH, COUNT, WT><<<blocks, T, 0, stream>>>(*w.S, *w.P, w.tex, w.n_host, w.light, w.n_light,
-                                                                   w.out, w.slot, w.counters, w.part, w.parts);
+                                                                   w.out, w.slot, w.counters, w.part, w.parts, w.rec);
         break;
     }
 }

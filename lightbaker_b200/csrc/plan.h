@@ -122,6 +122,9 @@ struct lb_plan {
     bool keep_records = false;  // record the first bounce's gather rays whatever the bounce count
     uint64_t max_gathered = 0;  // a bound on the gathered texels (records are sized by it)
     lbplan::DBuf records, theta0;
+    // with keep_records and a volume: every volume ray's outcome ([probe item][ray], gather_record) and the
+    // probes as the volume pass wrote them, before the fill
+    lbplan::DBuf vrecords, vraw;
     std::string tuned;  // what the autotuner picked
     std::string build_phases;  // the host build's phases, seconds since its start
     // a bake split over ranks (lb_exchange): every pass traces this rank's share of its items (item_part), and

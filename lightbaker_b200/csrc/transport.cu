@@ -11,12 +11,14 @@
 //   res_b        = eval(records, light_b, theta)                  trace.wgsl:258-269, bounced :133-148
 //   e_b          = fill(smooth(scatter(res_b)))                   bake.rs:309-323
 //   light_{b+1}  = write_light(s * dl0 + e_b)                     bake.rs:324-328
+//   probes       = fill(project(vrecords, light_B, theta))        trace.wgsl:272-324, volume.rs:88-121
+//   fallback     = irradiance(probes) at the validity-5 texels    bake.rs:335-359, volume.rs:125-147
 //   indirect     = dilate(dilate(composite(e_{B-1} | fallback)))  bake.rs:364-421
 //
-// where dl0 is the direct light at the scene's irradiance (linear in it: bake.rs:247-252 and the fills).
-// At theta0 (the scene's own values) every step is the device bake's own kernel on the same inputs, so
-// the result is the bake's indirect atlas bit for bit. Texels that take the volume's fallback
-// (bake.rs:335-359, validity 5) keep their theta0 light: the volume pass is not part of the transport.
+// where dl0 is the direct light at the scene's irradiance (linear in it: bake.rs:247-252 and the fills)
+// and vrecords what each volume ray met (recorded once, as the gather rays). At theta0 (the scene's own
+// values) every step is the device bake's own arithmetic on the same inputs, so the result is the bake's
+// indirect atlas bit for bit. The volume's share runs only when some texel takes the fallback.
 //
 // The adjoint runs the steps transposed, the last bounce first. Every sum runs in a fixed order (no
 // floating-point atomics; theta's sums in double), so a gradient is the same bits call after call and
@@ -179,12 +181,13 @@ __global__ void k_record_offsets(const uint32_t *keys, uint64_t n, uint32_t n_li
 // ---- transposes: a thread writes its own texel's gradient, summing what it fed in a fixed order ----
 
 // the composite's block average (bake.rs:364-391): a texel's share of its block's gradient; the fallback
-// texels' light is fixed
-__global__ void k_composite_t(PostArgs a, CompositeArgs c, const float4 *g_blocks, float4 *g_ind) {
+// texels' share too when the volume is differentiated (`fallback`; k_vfallback_t takes it from there),
+// else their light is fixed and gets none
+__global__ void k_composite_t(PostArgs a, CompositeArgs c, const float4 *g_blocks, float4 *g_ind, int fallback) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n_texels) return;
     float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (c.known[i] != 0 && c.state[i] != 5) {
+    if (c.known[i] != 0 && (c.state[i] != 5 || fallback)) {
         const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, i)];
         uint32_t li = i - t.off, ax = t.x + li % t.w, ay = t.y + li / t.w;
         uint32_t bx = ax / c.ds, by = ay / c.ds;
@@ -616,6 +619,234 @@ __global__ void __launch_bounds__(256) k_theta_final(const PartialSet *sets, int
     if (threadIdx.x == 0) g_theta[j] = float(part[0]);
 }
 
+// ---- the volume's share: the probes the fallback texels read (bake.rs:335-359, volume.rs:86-147) ----
+
+// The volume records against the last bounce's light and theta: each probe's L1 harmonics, its terms
+// summed in ray order as the volume pass sums them (trace.wgsl:272-324), a thread a probe; the sun's share
+// and the back-face share (geometry alone) as the bake wrote them (`raw`).
+__global__ void k_veval(const uint2 *rec, const float4 *items, const uint32_t *slot, uint32_t n, uint32_t rays,
+                        uint32_t seed, const float4 *light, uint32_t n_light, Theta th, const float4 *raw,
+                        float4 *probes) {
+    const float frays = __uint2float_rn(rays);
+    const float3 zen = th.zenith(), hor = th.horizon(), gro = th.ground(), fb = th.fallback();
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t key = __float_as_uint(items[4 * k + 1].w) * 7919u + 77u;
+        const float s1 = rnd(key, 29u, seed), s2 = rnd(key, 31u, seed);
+        float3 l0 = mk(0.f, 0.f, 0.f), l1x = l0, l1y = l0, l1z = l0;
+        const uint2 *rk = rec + size_t(k) * rays;
+        for (uint32_t r = 0; r < rays; r++) {
+            const float3 d = volume_ray(r, frays, s1, s2);
+            const uint2 q = __ldg(&rk[r]);
+            const uint32_t kind = q.x >> 30;
+            float3 l = mk(0.f, 0.f, 0.f);
+            if (kind == KIND_SKY) {
+                l = d.y < 0.0f ? gro : add(scl(hor, 1.0f - d.y), scl(zen, d.y));  // trace.wgsl:63-66
+            } else if (kind == KIND_SURFACE) {
+                const uint32_t m = q.x & 0x3fffffffu;
+                const float3 al = m < th.M ? th.albedo(m) : mk(0.f, 0.f, 0.f);
+                float3 e = fb;
+                if (q.y < n_light) {
+                    const float4 L = __ldg(&light[q.y]);
+                    if (L.w > 0.5f) e = mk(L.x, L.y, L.z);
+                }
+                l = mulv(mk(al.x / PI, al.y / PI, al.z / PI), e);  // trace.wgsl:133-148
+            }
+            const float3 lw = scl(l, 0.488603f);
+            l0 = add(l0, scl(l, 0.282095f));
+            l1x = add(l1x, scl(lw, d.x));
+            l1y = add(l1y, scl(lw, d.y));
+            l1z = add(l1z, scl(lw, d.z));
+        }
+        const float w = 4.0f * PI / frays;
+        const uint32_t dst = slot[k];
+        const float3 a[4] = {scl(l0, w), scl(l1x, w), scl(l1y, w), scl(l1z, w)};
+        for (int c = 0; c < 4; c++)
+            probes[4 * dst + c] = make_float4(a[c].x, a[c].y, a[c].z, raw[4 * dst + c].w);
+    }
+}
+
+// The trilinear corners a fallback texel reads (volume.rs:125-137), as the fallback computes them.
+struct VolumeGrid {
+    float3 origin;
+    float step;
+    uint32_t nx, ny, nz;
+};
+__device__ __forceinline__ void fallback_corners(const PostArgs &a, uint32_t i, const VolumeGrid &v, uint32_t j[8],
+                                                 float w[8]) {
+    const float4 n4 = a.tex[4 * i + 1];
+    float3 q = mk(a.posg[i].x + n4.x * 0.15f, a.posg[i].y + n4.y * 0.15f, a.posg[i].z + n4.z * 0.15f);
+    float fx = (q.x - v.origin.x) / v.step, fy = (q.y - v.origin.y) / v.step, fz = (q.z - v.origin.z) / v.step;
+    fx = fminf(fmaxf(fx, 0.0f), float(v.nx - 1));
+    fy = fminf(fmaxf(fy, 0.0f), float(v.ny - 1));
+    fz = fminf(fmaxf(fz, 0.0f), float(v.nz - 1));
+    uint32_t x0 = min(uint32_t(fx), v.nx - 2), y0 = min(uint32_t(fy), v.ny - 2), z0 = min(uint32_t(fz), v.nz - 2);
+    float tx = fx - float(x0), ty = fy - float(y0), tz = fz - float(z0);
+    for (int k = 0; k < 8; k++) {
+        int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+        w[k] = ((dx ? tx : 1.0f - tx) * (dy ? ty : 1.0f - ty)) * (dz ? tz : 1.0f - tz);
+        j[k] = ((y0 + dy) * v.nz + (z0 + dz)) * v.nx + (x0 + dx);
+    }
+}
+
+// The fallback texels' light from the filled probes (bake.rs:337-359 through volume.rs:125-147), the
+// arithmetic of the bake's own fallback, a thread a fallback texel.
+__global__ void k_vfallback(PostArgs a, const uint32_t *f5, uint32_t n5, const float4 *probes, VolumeGrid v,
+                            float4 *ind) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n5) return;
+    const uint32_t i = f5[q];
+    uint32_t j[8];
+    float w[8];
+    fallback_corners(a, i, v, j, w);
+    float p4[16] = {0};
+    for (int k = 0; k < 8; k++)
+        for (int c = 0; c < 4; c++) {
+            float4 pv = probes[4 * j[k] + c];
+            p4[4 * c] += pv.x * w[k], p4[4 * c + 1] += pv.y * w[k], p4[4 * c + 2] += pv.z * w[k], p4[4 * c + 3] += pv.w * w[k];
+        }
+    const float4 n4 = a.tex[4 * i + 1];
+    const float PI32 = 3.14159274101257324f;
+    float a0 = PI32 * 0.282095f, a1 = 2.0f * PI32 / 3.0f * 0.488603f;
+    float e[3];
+    for (int c = 0; c < 3; c++)
+        e[c] = 0.5f * a0 * p4[c] + 0.5f * fmaxf(a0 * p4[c] + a1 * ((p4[4 + c] * n4.x + p4[8 + c] * n4.y) + p4[12 + c] * n4.z), 0.0f);
+    ind[i] = make_float4(e[0], e[1], e[2], 0.0f);
+}
+
+// The fallback transposed, a thread a fallback texel: its indirect's gradient (taken out of g_ind, where
+// the composite's transpose left it) into the gradient of the four interpolated coefficients (rgb each),
+// the cosine lobe's clamp at 0 read from the forward's probes.
+__global__ void k_vfallback_t(PostArgs a, const uint32_t *f5, uint32_t n5, const float4 *probes, VolumeGrid v,
+                              float4 *g_ind, float4 *gp) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n5) return;
+    const uint32_t i = f5[q];
+    const float4 g = g_ind[i];
+    g_ind[i] = make_float4(0.f, 0.f, 0.f, 0.f);  // a fallback texel's light is not the bounces'
+    uint32_t j[8];
+    float w[8];
+    fallback_corners(a, i, v, j, w);
+    float p4[16] = {0};
+    for (int k = 0; k < 8; k++)
+        for (int c = 0; c < 4; c++) {
+            float4 pv = probes[4 * j[k] + c];
+            p4[4 * c] += pv.x * w[k], p4[4 * c + 1] += pv.y * w[k], p4[4 * c + 2] += pv.z * w[k], p4[4 * c + 3] += pv.w * w[k];
+        }
+    const float4 n4 = a.tex[4 * i + 1];
+    const float PI32 = 3.14159274101257324f;
+    const float a0 = PI32 * 0.282095f, a1 = 2.0f * PI32 / 3.0f * 0.488603f;
+    const float gc[3] = {g.x, g.y, g.z};
+    float o[4][3];
+    for (int c = 0; c < 3; c++) {
+        const float arg = a0 * p4[c] + a1 * ((p4[4 + c] * n4.x + p4[8 + c] * n4.y) + p4[12 + c] * n4.z);
+        const float on = arg > 0.0f ? 1.0f : 0.0f;
+        o[0][c] = gc[c] * (0.5f * a0 + on * 0.5f * a0);
+        o[1][c] = gc[c] * on * 0.5f * a1 * n4.x;
+        o[2][c] = gc[c] * on * 0.5f * a1 * n4.y;
+        o[3][c] = gc[c] * on * 0.5f * a1 * n4.z;
+    }
+    for (int k = 0; k < 4; k++) gp[4 * size_t(q) + k] = make_float4(o[k][0], o[k][1], o[k][2], 0.f);
+}
+
+// The interpolation transposed, a thread a probe: the corner weights of the fallback texels that read it
+// (listed at create, in texel order) times their coefficients' gradients.
+__global__ void k_vprobe_t(const uint32_t *off, const uint32_t *who, const float *wt, uint32_t n_probes,
+                           const float4 *gp, float4 *g_probes) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n_probes) return;
+    float3 s[4] = {mk(0.f, 0.f, 0.f), mk(0.f, 0.f, 0.f), mk(0.f, 0.f, 0.f), mk(0.f, 0.f, 0.f)};
+    for (uint32_t e = off[j]; e < off[j + 1]; e++) {
+        const uint32_t q = who[e];
+        const float w = wt[e];
+        for (int k = 0; k < 4; k++) s[k] = add(s[k], scl(xyz(gp[4 * size_t(q) + k]), w));
+    }
+    for (int k = 0; k < 4; k++) g_probes[4 * size_t(j) + k] = make_float4(s[k].x, s[k].y, s[k].z, 0.f);
+}
+
+// One ring of the volume's fill (volume.rs:88-121) transposed, a thread a probe: a probe known before the
+// ring keeps its own value and feeds each unknown neighbour that the ring fills (an average of its known
+// neighbours); an unknown probe the ring leaves unknown keeps its own. `was`: the known flags before it.
+__global__ void k_vfill_t(const uint8_t *was, const float4 *g_dst, float4 *g_src, uint32_t nx, uint32_t ny,
+                          uint32_t nz) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t total = nx * ny * nz;
+    if (j >= total) return;
+    const int D[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    auto neighbour = [&](uint32_t k, int d, uint32_t &out) {
+        int x = int(k % nx), z = int((k / nx) % nz), y = int(k / (nx * nz));
+        int xx = x + D[d][0], yy = y + D[d][1], zz = z + D[d][2];
+        if (xx < 0 || yy < 0 || zz < 0 || xx >= int(nx) || yy >= int(ny) || zz >= int(nz)) return false;
+        out = (uint32_t(yy) * nz + uint32_t(zz)) * nx + uint32_t(xx);
+        return true;
+    };
+    auto known_count = [&](uint32_t k) {
+        int c = 0;
+        uint32_t m;
+        for (int d = 0; d < 6; d++)
+            if (neighbour(k, d, m) && was[m]) c++;
+        return c;
+    };
+    float4 g[4];
+    const bool keeps = was[j] || known_count(j) == 0;
+    for (int q = 0; q < 4; q++) g[q] = keeps ? g_dst[4 * j + q] : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (was[j])
+        for (int d = 0; d < 6; d++) {
+            uint32_t k;
+            if (!neighbour(j, d, k) || was[k]) continue;
+            const int c = known_count(k);
+            if (c == 0) continue;
+            const float f = float(c);
+            for (int q = 0; q < 4; q++) {
+                float4 v = g_dst[4 * k + q];
+                g[q] = make_float4(g[q].x + v.x / f, g[q].y + v.y / f, g[q].z + v.z / f, 0.f);
+            }
+        }
+    for (int q = 0; q < 4; q++) g_src[4 * j + q] = g[q];
+}
+
+// The probes each fallback texel reads and their weights (8 a texel, corner order), for the per-probe lists.
+__global__ void k_vcorners(PostArgs a, const uint32_t *f5, uint32_t n5, VolumeGrid v, uint32_t *j8, float *w8) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n5) return;
+    fallback_corners(a, f5[q], v, j8 + 8 * size_t(q), w8 + 8 * size_t(q));
+}
+
+// The L1 projection transposed, a thread a volume ray: the gradient of the ray's radiance from its probe's
+// coefficient gradients (w * basis(d)), divided by pi: as the gather's records weigh their terms (pi / rays),
+// so the records' transposes (k_lit_t, k_unlit_t with one ray an item) give the volume rays' gradients.
+__global__ void k_vrec_t(const float4 *items, const uint32_t *slot, uint32_t n, uint32_t rays, uint32_t seed,
+                         const float4 *g_probes, float4 *vg) {
+    const uint64_t total = uint64_t(n) * rays;
+    const float frays = __uint2float_rn(rays), w = 4.0f * PI / frays;
+    for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < total; q += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t k = uint32_t(q / rays), r = uint32_t(q % rays);
+        const uint32_t key = __float_as_uint(items[4 * k + 1].w) * 7919u + 77u;
+        const float3 d = volume_ray(r, frays, rnd(key, 29u, seed), rnd(key, 31u, seed));
+        const uint32_t j = slot[k];
+        const float3 g0 = xyz(g_probes[4 * j]), gx = xyz(g_probes[4 * j + 1]), gy = xyz(g_probes[4 * j + 2]),
+                     gz = xyz(g_probes[4 * j + 3]);
+        const float3 g1 = add(add(scl(gx, d.x), scl(gy, d.y)), scl(gz, d.z));
+        const float3 gl = scl(add(scl(g0, 0.282095f), scl(g1, 0.488603f)), w / PI);
+        vg[q] = make_float4(gl.x, gl.y, gl.z, 0.f);
+    }
+}
+
+// write_light transposed for the last bounce's light, which only the volume reads: added to the direct
+// light's gradient and to the last bounce's indirect's (the composite's transpose wrote it first).
+__global__ void k_light_add_t(PostArgs a, const uint8_t *kb, const float4 *g_light, float4 *g_dl, float4 *g_ind) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_texels || kb[i] < 1) return;
+    const DTile t = a.tiles[find_tile(a.tiles, a.n_tiles, i)];
+    uint32_t li = i - t.off;
+    const float4 g = g_light[size_t(t.y + li / t.w) * a.aw + t.x + li % t.w];
+    float4 d = g_dl[i];
+    g_dl[i] = make_float4(d.x + g.x, d.y + g.y, d.z + g.z, 0.f);
+    if (g_ind) {
+        float4 e = g_ind[i];
+        g_ind[i] = make_float4(e.x + g.x, e.y + g.y, e.z + g.z, 0.f);
+    }
+}
+
 }  // namespace lbd
 
 cudaError_t lb_eval_records(const uint2 *rec, const uint32_t *n_dev, uint32_t n_host, uint32_t rays,
@@ -652,6 +883,15 @@ struct lb_transport {
         ind, out_atlas, out_tmp, out_has, out_has_b, out_direct, out_validity;
     DBuf g_in, g_blocks_a, g_blocks_b, g_ind, g_a, g_b, g_res, g_light, g_dl, partials, sun_partials, sets_d, g_theta;
     std::vector<lbd::PartialSet> sets;
+    // the volume's share (a scene with a volume and texels it lights, state 5): the fallback texels' light
+    // through the probes from the last bounce's light and theta (build())
+    bool vol = false;
+    uint32_t vrays = 0, n_vitems = 0, n_probes = 0, n5 = 0, vseed = 0;
+    uint64_t n_vrec = 0, vunlit0 = 0, n_vunlit = 0;
+    lbd::VolumeGrid grid{};
+    static constexpr int VRINGS = 8;  // the fill's rings (bake_device.cu, volume.rs:88)
+    DBuf light_last, vprobes, vprobes_b, vka, vkb, fb_ind, f5, vflags, vcsr_off, vcsr_who, vcsr_w, gp, g_vp_a, g_vp_b, vg,
+        vsorted, voffs, g_vlight;
     cudaGraphExec_t fwd = nullptr, bwd = nullptr;
     bool forward_done = false;
     ~lb_transport() {
@@ -686,6 +926,60 @@ void light0(lb_transport &t, float4 *light, cudaStream_t st) {
     ck(cudaGetLastError(), "transport light");
 }
 
+// the volume's share of the forward: the probes from the last bounce's light (the volume records), the
+// fill, the fallback texels' light
+void volume_forward(lb_transport &t, cudaStream_t st) {
+    lb_plan &p = *t.plan;
+    lbd::k_veval<<<tg(t.n_vitems), 256, 0, st>>>(p.vrecords.as<uint2>(), p.probe_items.as<float4>(),
+                                                 p.probe_slot.as<uint32_t>(), t.n_vitems, t.vrays, t.vseed,
+                                                 t.light_last.as<float4>(), t.n_light, t.th(), p.vraw.as<float4>(),
+                                                 t.vprobes.as<float4>());
+    ck(cudaGetLastError(), "volume records");
+    ck(lb_volume_fill(t.vprobes.as<float4>(), t.vprobes_b.as<float4>(), t.vka.as<uint8_t>(), t.vkb.as<uint8_t>(),
+                      t.grid.nx, t.grid.ny, t.grid.nz, lb_transport::VRINGS, st),
+       "volume fill");
+    lbd::k_vfallback<<<tg(t.n5), 256, 0, st>>>(t.a, t.f5.as<uint32_t>(), t.n5, t.vprobes.as<float4>(), t.grid,
+                                               t.fb_ind.as<float4>());
+    ck(cudaGetLastError(), "fallback");
+}
+
+// the volume's share of the adjoint (before the bounces'): the fallback texels' gradient into the probes,
+// the fill and the projection transposed, the volume records as one-ray items, and the last bounce's light
+// gradient into the direct light's and the last bounce's indirect's
+void volume_backward(lb_transport &t, cudaStream_t st, size_t smem, int &set) {
+    lb_plan &p = *t.plan;
+    lbd::k_vfallback_t<<<tg(t.n5), 256, 0, st>>>(t.a, t.f5.as<uint32_t>(), t.n5, t.vprobes.as<float4>(), t.grid,
+                                                 t.g_ind.as<float4>(), t.gp.as<float4>());
+    lbd::k_vprobe_t<<<tg(t.n_probes), 256, 0, st>>>(t.vcsr_off.as<uint32_t>(), t.vcsr_who.as<uint32_t>(),
+                                                    t.vcsr_w.as<float>(), t.n_probes, t.gp.as<float4>(),
+                                                    t.g_vp_a.as<float4>());
+    float4 *cur = t.g_vp_a.as<float4>(), *other = t.g_vp_b.as<float4>();
+    for (int q = lb_transport::VRINGS - 1; q >= 0; q--) {
+        lbd::k_vfill_t<<<tg(t.n_probes), 256, 0, st>>>(t.vflags.as<uint8_t>() + size_t(q) * t.n_probes, cur, other,
+                                                       t.grid.nx, t.grid.ny, t.grid.nz);
+        std::swap(cur, other);
+    }
+    lbd::k_vrec_t<<<t.g->sms * 8, 256, 0, st>>>(p.probe_items.as<float4>(), p.probe_slot.as<uint32_t>(), t.n_vitems,
+                                                t.vrays, t.vseed, cur, t.vg.as<float4>());
+    ck(cudaGetLastError(), "volume^T");
+    for (uint32_t m0 = 0, first = 1; m0 < std::max(t.M, 1u); m0 += t.mc, first = 0) {
+        uint32_t mc = std::min(t.mc, std::max(t.M, 1u) - m0);
+        lbd::k_lit_t<<<t.blocks, T_THREADS, smem, st>>>(t.voffs.as<uint64_t>(), t.vsorted.as<uint2>(), t.n_light,
+                                                        t.light_last.as<float4>(), t.th(), m0, mc, 1u, t.vg.as<float4>(),
+                                                        t.g_vlight.as<float4>(), int(first),
+                                                        const_cast<double *>(t.sets[set].p));
+        set++;
+        lbd::k_unlit_t<<<t.blocks, T_THREADS, smem, st>>>(t.vsorted.as<uint2>() + t.vunlit0, t.n_vunlit, t.th(), m0,
+                                                          mc, 1u, t.vg.as<float4>(), int(first),
+                                                          const_cast<double *>(t.sets[set].p));
+        set++;
+    }
+    if (t.n_tex)
+        lbd::k_light_add_t<<<tg(t.n_tex), 256, 0, st>>>(t.a, t.kb.as<uint8_t>(), t.g_vlight.as<float4>(),
+                                                        t.g_dl.as<float4>(), t.B > 0 ? t.g_ind.as<float4>() : nullptr);
+    ck(cudaGetLastError(), "volume records^T");
+}
+
 // the forward, from theta (on the device) to the indirect atlas in out_atlas
 void record_forward(lb_transport &t, cudaStream_t st) {
     bool all = t.K >= t.B;
@@ -700,14 +994,19 @@ void record_forward(lb_transport &t, cudaStream_t st) {
                    "checkpoint");
                 next_ck++;
             }
-            float4 *nxt = b + 1 < t.B ? (all ? t.slot(b + 1) : cur) : nullptr;
+            // the last bounce writes the light the volume reads
+            float4 *nxt = b + 1 < t.B ? (all ? t.slot(b + 1) : cur) : t.vol ? t.light_last.as<float4>() : nullptr;
             bounce(t, cur, b, nxt, st, &filled);
             if (nxt) cur = nxt;
         }
+    } else if (t.vol) {
+        light0(t, t.light_last.as<float4>(), st);
     }
+    if (t.vol) volume_forward(t, st);
     if (t.n_tex)
         lbd::k_final_ind<<<tg(t.n_tex), 256, 0, st>>>(t.n_tex, t.plan->state.as<uint8_t>(), filled,
-                                                      t.fixed_ind.as<float4>(), t.ind.as<float4>());
+                                                      t.vol ? t.fb_ind.as<float4>() : t.fixed_ind.as<float4>(),
+                                                      t.ind.as<float4>());
     ck(lb_composite(t.c, t.out_tmp.as<float4>(), t.out_has_b.as<uint8_t>(), st), "transport composite");
 }
 
@@ -722,11 +1021,13 @@ void record_backward(lb_transport &t, cudaStream_t st) {
     lbd::k_dilate_t<<<tg(nb), 256, 0, st>>>(t.has0.as<uint8_t>(), t.g_blocks_a.as<float4>(), t.g_blocks_b.as<float4>(),
                                             t.iw, t.ih);
     if (t.n_tex)
-        lbd::k_composite_t<<<tg(t.n_tex), 256, 0, st>>>(a, t.c, t.g_blocks_b.as<float4>(), t.g_ind.as<float4>());
+        lbd::k_composite_t<<<tg(t.n_tex), 256, 0, st>>>(a, t.c, t.g_blocks_b.as<float4>(), t.g_ind.as<float4>(),
+                                                        int(t.vol));
     ck(cudaGetLastError(), "transport composite^T");
     bool all = t.K >= t.B;
     size_t smem = size_t(3 * t.mc) * lbd::TW * sizeof(double);
     int set = 0;
+    if (t.vol) volume_backward(t, st, smem, set);
     for (int32_t b = int32_t(t.B) - 1; b >= 0; b--) {
         // the light this bounce read: kept, or recomputed from the nearest earlier checkpoint
         float4 *light;
@@ -804,6 +1105,135 @@ cudaGraphExec_t capture(lb_transport &t, void (*rec)(lb_transport &, cudaStream_
 template <class T> void up(DBuf &d, const std::vector<T> &v, cudaStream_t st) {
     d.alloc(v.size() * sizeof(T));
     if (!v.empty()) ck(cudaMemcpyAsync(d.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st), "upload");
+}
+
+// The volume's share, when the bake lit texels from the volume (state 5): their list, the fill's known flags
+// ring by ring, each probe's list of the fallback texels that read it (with the corner weights), the
+// volume records in the adjoint's order (as the gather's, one ray an item) and the adjoint's arrays.
+void volume_setup(lb_transport &t, cudaStream_t st) {
+    lb_plan &p = *t.plan;
+    t.vol = false;
+    if (!p.has_volume || !p.n_todo || !t.n_tex) return;
+    std::vector<uint8_t> state(t.n_tex);
+    ck(cudaMemcpy(state.data(), p.state.p, t.n_tex, cudaMemcpyDeviceToHost), "state");
+    std::vector<uint32_t> f5;
+    for (uint32_t i = 0; i < t.n_tex; i++)
+        if (state[i] == 5) f5.push_back(i);
+    if (f5.empty()) return;
+    const lb::VolumeSettings &v = *p.scene.header.volume;
+    t.vol = true;
+    t.n5 = uint32_t(f5.size());
+    up(t.f5, f5, st);
+    t.vrays = v.rays;
+    t.n_vitems = p.n_todo;
+    t.n_probes = p.n_probes;
+    std::memcpy(&t.vseed, &p.P.params.reach[3], 4);
+    t.n_vrec = uint64_t(t.n_vitems) * t.vrays;
+    if (t.n_vrec >= (1ull << 30)) throw std::runtime_error("lb_transport_create: too many volume rays");
+    t.grid = lbd::VolumeGrid{make_float3(v.min[0], v.min[1], v.min[2]), v.step, p.vsize[0], p.vsize[1], p.vsize[2]};
+    if (t.grid.nx < 2 || t.grid.ny < 2 || t.grid.nz < 2)
+        throw std::runtime_error("lb_transport_create: a volume needs two probes along each axis");
+    const size_t N = std::max<size_t>(t.n_tex, 1);
+    t.light_last.alloc(size_t(t.n_light) * 16);
+    ck(cudaMemsetAsync(t.light_last.p, 0, t.light_last.bytes, st), "light");
+    t.vprobes.alloc(size_t(t.n_probes) * 64);
+    t.vprobes_b.alloc(size_t(t.n_probes) * 64);
+    t.vka.alloc(t.n_probes);
+    t.vkb.alloc(t.n_probes);
+    t.fb_ind.alloc(N * 16);
+    ck(cudaMemcpyAsync(t.fb_ind.p, t.fixed_ind.p, N * 16, cudaMemcpyDeviceToDevice, st), "fallback light");
+    // the fill's known flags before each ring (volume.rs:88-121: known where the back-face share is at most
+    // half, then every unknown probe with a known neighbour, ring by ring)
+    {
+        std::vector<float> raw(size_t(t.n_probes) * 16);
+        ck(cudaMemcpy(raw.data(), p.vraw.p, raw.size() * 4, cudaMemcpyDeviceToHost), "raw probes");
+        const uint32_t nx = t.grid.nx, ny = t.grid.ny, nz = t.grid.nz;
+        std::vector<uint8_t> flags(size_t(lb_transport::VRINGS) * t.n_probes), was(t.n_probes);
+        for (uint32_t k = 0; k < t.n_probes; k++) was[k] = raw[size_t(k) * 16 + 7] <= 0.5f;
+        const int D[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+        for (int q = 0; q < lb_transport::VRINGS; q++) {
+            std::copy(was.begin(), was.end(), flags.begin() + size_t(q) * t.n_probes);
+            std::vector<uint8_t> now = was;
+            for (uint32_t k = 0; k < t.n_probes; k++) {
+                if (was[k]) continue;
+                int x = int(k % nx), z = int((k / nx) % nz), y = int(k / (nx * nz));
+                for (int d = 0; d < 6; d++) {
+                    int xx = x + D[d][0], yy = y + D[d][1], zz = z + D[d][2];
+                    if (xx < 0 || yy < 0 || zz < 0 || xx >= int(nx) || yy >= int(ny) || zz >= int(nz)) continue;
+                    if (was[(uint32_t(yy) * nz + uint32_t(zz)) * nx + uint32_t(xx)]) {
+                        now[k] = 1;
+                        break;
+                    }
+                }
+            }
+            was.swap(now);
+        }
+        up(t.vflags, flags, st);
+    }
+    // each probe's fallback texels (index in f5) and weights, in texel order
+    {
+        DBuf j8, w8;
+        j8.alloc(size_t(t.n5) * 8 * 4);
+        w8.alloc(size_t(t.n5) * 8 * 4);
+        lbd::k_vcorners<<<tg(t.n5), 256, 0, st>>>(t.a, t.f5.as<uint32_t>(), t.n5, t.grid, j8.as<uint32_t>(),
+                                                  w8.as<float>());
+        ck(cudaGetLastError(), "corners");
+        std::vector<uint32_t> hj(size_t(t.n5) * 8);
+        std::vector<float> hw(size_t(t.n5) * 8);
+        ck(cudaMemcpy(hj.data(), j8.p, hj.size() * 4, cudaMemcpyDeviceToHost), "corners");
+        ck(cudaMemcpy(hw.data(), w8.p, hw.size() * 4, cudaMemcpyDeviceToHost), "corners");
+        std::vector<uint32_t> off(size_t(t.n_probes) + 1, 0), who(hj.size());
+        std::vector<float> wt(hj.size());
+        for (uint32_t j : hj) off[size_t(j) + 1]++;
+        for (uint32_t k = 0; k < t.n_probes; k++) off[k + 1] += off[k];
+        std::vector<uint32_t> at(off.begin(), off.end() - 1);
+        for (size_t e = 0; e < hj.size(); e++) {
+            uint32_t pos = at[hj[e]]++;
+            who[pos] = uint32_t(e / 8);
+            wt[pos] = hw[e];
+        }
+        up(t.vcsr_off, off, st);
+        up(t.vcsr_who, who, st);
+        up(t.vcsr_w, wt, st);
+        ck(cudaStreamSynchronize(st), "corner lists");
+    }
+    // the volume records in the adjoint's order: lit by atlas texel (the bake's last light tells which texels
+    // hold light), then sky and fallback-lit, then none
+    t.vsorted.alloc(t.n_vrec * 8);
+    t.voffs.alloc(size_t(t.n_light + 3) * 8);
+    {
+        DBuf keys, vals, keys2, vals2, temp;
+        size_t n = std::max<uint64_t>(t.n_vrec, 1);
+        keys.alloc(n * 4);
+        vals.alloc(n * 4);
+        keys2.alloc(n * 4);
+        vals2.alloc(n * 4);
+        lbd::k_record_keys<<<t.g->sms * 8, 256, 0, st>>>(p.vrecords.as<uint2>(), t.n_vrec, p.light.as<float4>(),
+                                                        t.n_light, t.M, keys.as<uint32_t>(), vals.as<uint32_t>());
+        size_t tb = 0;
+        ck(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.as<uint32_t>(), keys2.as<uint32_t>(), vals.as<uint32_t>(),
+                                           vals2.as<uint32_t>(), int(t.n_vrec), 0, 32, st),
+           "sort size");
+        temp.alloc(tb);
+        ck(cub::DeviceRadixSort::SortPairs(temp.p, tb, keys.as<uint32_t>(), keys2.as<uint32_t>(), vals.as<uint32_t>(),
+                                           vals2.as<uint32_t>(), int(t.n_vrec), 0, 32, st),
+           "sort");
+        lbd::k_record_sorted<<<t.g->sms * 8, 256, 0, st>>>(p.vrecords.as<uint2>(), vals2.as<uint32_t>(), t.n_vrec, 1u,
+                                                          t.vsorted.as<uint2>());
+        lbd::k_record_offsets<<<tg(t.n_light + 3), 256, 0, st>>>(keys2.as<uint32_t>(), t.n_vrec, t.n_light,
+                                                                 t.voffs.as<uint64_t>());
+        ck(cudaGetLastError(), "volume record order");
+        std::vector<uint64_t> tail(3);
+        ck(cudaMemcpyAsync(tail.data(), t.voffs.as<uint64_t>() + t.n_light, 24, cudaMemcpyDeviceToHost, st), "offsets");
+        ck(cudaStreamSynchronize(st), "volume record order");
+        t.vunlit0 = tail[0];
+        t.n_vunlit = tail[2] - tail[0];
+    }
+    t.gp.alloc(size_t(t.n5) * 64);
+    t.g_vp_a.alloc(size_t(t.n_probes) * 64);
+    t.g_vp_b.alloc(size_t(t.n_probes) * 64);
+    t.vg.alloc(std::max<uint64_t>(t.n_vrec, 1) * 16);
+    t.g_vlight.alloc(size_t(t.n_light) * 16);
 }
 
 void build(lb_transport &t, uint32_t max_checkpoints) {
@@ -943,6 +1373,7 @@ void build(lb_transport &t, uint32_t max_checkpoints) {
         t.unlit0 = tail[0];
         t.n_unlit = tail[2] - tail[0];
     }
+    volume_setup(t, st);
     // checkpoints: every bounce's light when the budget allows, else K spread evenly (the first is bounce 0)
     t.K = max_checkpoints == 0 ? t.B : std::min(max_checkpoints, t.B);
     t.ck_bounce.clear();
@@ -976,7 +1407,7 @@ void build(lb_transport &t, uint32_t max_checkpoints) {
     ck(cudaFuncSetAttribute(lbd::k_unlit_t, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem");
     uint32_t chunks = (std::max(t.M, 1u) + t.mc - 1) / t.mc;
     size_t per_set = size_t(t.blocks) * (3 * t.mc + lbd::FIXED_SLOTS);
-    size_t n_sets = size_t(t.B) * chunks * 2;
+    size_t n_sets = size_t(t.B + (t.vol ? 1 : 0)) * chunks * 2;
     t.partials.alloc(std::max<size_t>(n_sets, 1) * per_set * sizeof(double));
     t.sun_partials.alloc(size_t(t.sun_blocks) * sizeof(double));
     t.sets.clear();
@@ -1142,6 +1573,25 @@ size_t lb_transport_export(lb_transport *t, const char *name, void *out, size_t 
     else if (n == "gather_out") dev(p.gather_out, size_t(t->n_gath) * 16);
     else if (n == "light") dev(p.light, size_t(t->n_light) * 16);
     else if (n == "probes") dev(p.probes, p.has_volume ? size_t(p.n_probes) * 64 : 0);
+    // the volume's share (empty when the transport does not differentiate the volume): every volume ray's
+    // outcome, the probe items and their slots, the probes as the volume pass wrote them, the grid
+    else if (n == "volume_records") dev(p.vrecords, t->vol ? t->n_vrec * 8 : 0);
+    else if (n == "volume_items") dev(p.probe_items, t->vol ? size_t(t->n_vitems) * 64 : 0);
+    else if (n == "volume_slots") dev(p.probe_slot, t->vol ? size_t(t->n_vitems) * 4 : 0);
+    else if (n == "volume_raw") dev(p.vraw, t->vol ? size_t(t->n_probes) * 64 : 0);
+    else if (n == "volume_grid") {
+        // nx, ny, nz, rays, items, the sample seed (bits), origin xyz and step (bits); empty without the share
+        if (t->vol) {
+            uint32_t v[10] = {t->grid.nx, t->grid.ny, t->grid.nz, t->vrays, t->n_vitems, t->vseed, 0, 0, 0, 0};
+            std::memcpy(&v[6], &t->grid.origin.x, 4);
+            std::memcpy(&v[7], &t->grid.origin.y, 4);
+            std::memcpy(&v[8], &t->grid.origin.z, 4);
+            std::memcpy(&v[9], &t->grid.step, 4);
+            host.resize(sizeof v);
+            std::memcpy(host.data(), v, sizeof v);
+            bytes = sizeof v;
+        }
+    }
     else if (n == "light_flags") {
         // the atlas's known flags (w of the light atlas)
         std::vector<float> l(size_t(t->n_light) * 4);

@@ -27,6 +27,8 @@ _EXPORT_DTYPES = {
     "direct_records": (np.float32, 4), "valid": (np.uint8, 1), "field": (np.float32, 1), "ao": (np.float32, 1),
     "direct": (np.float32, 4), "indirect_light": (np.float32, 4), "gather_out": (np.float32, 4),
     "light": (np.float32, 4), "probes": (np.float32, 16),
+    "volume_records": (np.uint32, 2), "volume_items": (np.float32, 16), "volume_slots": (np.uint32, 1),
+    "volume_raw": (np.float32, 16), "volume_grid": (np.uint32, 1),
 }
 
 

@@ -7,7 +7,9 @@ the product's adjoint (lb_transport_backward). The forward follows the reference
   each gather result            crates/lightbaker/src/gpu/trace.wgsl:245-270 (bounced :133-148, sky :63-66)
   the bounce's texel work       crates/lightbaker/src/bake.rs:303-328 with filter.rs:20-53 (smooth) and
                                 filter.rs:58-94 (fill)
-  the fallback texels           crates/lightbaker/src/bake.rs:335-359 (held at their own values)
+  the volume's probes           crates/lightbaker/src/gpu/trace.wgsl:272-324 (L1 projection of the recorded
+                                volume rays against the last bounce's light), volume.rs:88-121 (the fill)
+  the fallback texels           crates/lightbaker/src/bake.rs:335-359 with volume.rs:125-147 (irradiance)
   the indirect atlas            crates/lightbaker/src/bake.rs:364-421 (block average, two dilations)
 
 Every linear step is a scipy sparse matrix built from the fixed arrays the transport exports (texel
@@ -165,6 +167,58 @@ def dilate_pass(has: np.ndarray, iw: int, ih: int):
     return m, has | fill
 
 
+def _pcg(v):
+    """trace.wgsl:41-45 on uint32 arrays."""
+    v = np.asarray(v, np.uint64) & 0xFFFFFFFF
+    s = (v * 747796405 + 2891336453) & 0xFFFFFFFF
+    w = (((s >> ((s >> 28) + 4)) ^ s) * 277803737) & 0xFFFFFFFF
+    return ((w >> 22) ^ w) & 0xFFFFFFFF
+
+
+def _rnd(a, b, seed):
+    """trace.wgsl:46: a uniform float in [0, 1) from two keys and the seed."""
+    return _pcg(np.asarray(a, np.uint64) ^ _pcg(np.uint64(b) + np.uint64(seed))).astype(np.float32) * np.float32(2.0 ** -32)
+
+
+def _radical(i):
+    """trace.wgsl:49: the bits of i reversed, over 2^32."""
+    i = np.asarray(i, np.uint64)
+    r = np.zeros_like(i)
+    for k in range(32):
+        r |= ((i >> k) & 1) << (31 - k)
+    return r.astype(np.float32) * np.float32(2.0 ** -32)
+
+
+def fill_probe_rings(known, nx, ny, nz, rings):
+    """volume.rs:88-121: each ring, an unknown probe with known neighbours becomes their mean (and known);
+    the others keep their values. Returns the rings' matrices, first first."""
+    n = nx * ny * nz
+    k = np.arange(n)
+    x, z, y = k % nx, (k // nx) % nz, k // (nx * nz)
+    out = []
+    was = known.copy()
+    for _ in range(rings):
+        rows, cols, vals = [], [], []
+        cnt = np.zeros(n, np.int64)
+        nb = []
+        for dx, dy, dz in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+            xx, yy, zz = x + dx, y + dy, z + dz
+            ok = (xx >= 0) & (yy >= 0) & (zz >= 0) & (xx < nx) & (yy < ny) & (zz < nz)
+            j = np.where(ok, (yy * nz + zz) * nx + xx, 0)
+            ok &= was[j]
+            nb.append((ok, j))
+            cnt += ok
+        filled = ~was & (cnt > 0)
+        keep = ~filled
+        rows.append(k[keep]), cols.append(k[keep]), vals.append(np.ones(keep.sum()))
+        for ok, j in nb:
+            m = filled & ok
+            rows.append(k[m]), cols.append(j[m]), vals.append(1.0 / cnt[m])
+        out.append(sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n)))
+        was = was | filled
+    return out
+
+
 def _torch_sparse(m):
     import torch
     m = m.tocoo()
@@ -225,6 +279,66 @@ class TransportRef:
         self.surf, self.lit = surf, lit
         self.sky_up = (kind == 0) & (self.y >= 0)
         self.sky_down = (kind == 0) & (self.y < 0)
+        # the volume's share, when the transport has one (some texel takes the fallback)
+        grid = arrays.get("volume_grid")
+        self.vol = grid is not None and len(grid) == 10
+        if self.vol:
+            self._volume(arrays, grid, n_tex)
+
+    def _volume(self, arrays, grid, n_tex):
+        nx, ny, nz, vrays, nv, seed = (int(v) for v in grid[:6])
+        origin = grid[6:9].astype(np.uint32).view(np.float32)
+        step = grid[9:10].astype(np.uint32).view(np.float32)[0]
+        items = arrays["volume_items"].reshape(nv, 16)
+        self.vslots = arrays["volume_slots"].astype(np.int64)
+        raw = arrays["volume_raw"].reshape(-1, 4, 4)
+        self.n_probes = nx * ny * nz
+        # every ray's direction (trace.wgsl:278-295), in float64 from the float32 seeds
+        key = (items[:, 7].view(np.uint32).astype(np.uint64) * 7919 + 77) & 0xFFFFFFFF
+        s1, s2 = _rnd(key, 29, seed).astype(np.float64), _rnd(key, 31, seed).astype(np.float64)
+        r = np.arange(vrays, dtype=np.float64)
+        u = (r[None, :] + 0.5) / vrays + s1[:, None]
+        u -= np.floor(u)
+        v = _radical(np.arange(vrays)).astype(np.float64)[None, :] + s2[:, None]
+        v -= np.floor(v)
+        zc = 1.0 - 2.0 * u
+        rr = np.sqrt(np.maximum(0.0, 1.0 - zc * zc))
+        a = v * 2.0 * math.pi
+        self.vdir = np.stack([rr * np.cos(a), zc, rr * np.sin(a)], axis=-1)
+        self.vw = 4.0 * math.pi / vrays
+        rec = arrays["volume_records"].reshape(nv, vrays, 2)
+        kind = rec[:, :, 0] >> 30
+        self.vmat = (rec[:, :, 0] & 0x3FFFFFFF).astype(np.int64)
+        self.vli = rec[:, :, 1].astype(np.int64)
+        self.vy = np.where(kind == 0, rec[:, :, 1].view(np.float32).astype(np.float64), 0.0)
+        surf = (kind == 2) & (self.vmat < self.M)
+        lit = surf & (rec[:, :, 1] != NONE)
+        lit[lit] = self.light_flag[self.vli[lit]]
+        self.vsurf, self.vlit = surf, lit
+        self.vsky_up = (kind == 0) & (self.vy >= 0)
+        self.vsky_down = (kind == 0) & (self.vy < 0)
+        # the fill (volume.rs:88-121), its known flags from the back-face share
+        self.vfill = [_torch_sparse(m) for m in fill_probe_rings(raw[:, 1, 3] <= np.float32(0.5), nx, ny, nz, 8)]
+        # the fallback texels' trilinear corners (volume.rs:125-137, in float32 as the bake computes them)
+        f5 = np.nonzero(self.state == 5)[0]
+        self.f5 = f5
+        pos = arrays["sample_points"][f5, :3].astype(np.float32)
+        nrm = arrays["texels"][f5, 4:7].astype(np.float32)
+        q = pos + nrm * np.float32(0.15)
+        f = (q - origin[None, :]) / step
+        dims = np.array([nx, ny, nz])
+        f = np.minimum(np.maximum(f, np.float32(0.0)), (dims - 1).astype(np.float32)[None, :])
+        c0 = np.minimum(f.astype(np.int64), dims[None, :] - 2)
+        t = (f - c0.astype(np.float32)).astype(np.float32)
+        rows, cols, vals = [], [], []
+        for k in range(8):
+            dx, dy, dz = k & 1, (k >> 1) & 1, (k >> 2) & 1
+            w = ((t[:, 0] if dx else 1 - t[:, 0]) * (t[:, 1] if dy else 1 - t[:, 1])) * (t[:, 2] if dz else 1 - t[:, 2])
+            j = ((c0[:, 1] + dy) * nz + (c0[:, 2] + dz)) * nx + (c0[:, 0] + dx)
+            rows.append(np.arange(len(f5))), cols.append(j), vals.append(w.astype(np.float64))
+        self.vinterp = _torch_sparse(sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                                                   shape=(len(f5), self.n_probes)))
+        self.vnormal = nrm.astype(np.float64)
 
     def forward(self, theta):
         """theta: a float64 torch tensor (3 M + 10) -> the indirect atlas (ih * iw, 3)."""
@@ -257,6 +371,31 @@ class TransportRef:
         fallback = torch.from_numpy(self.state == 5)[:, None]
         fixed = torch.from_numpy(self.fixed)
         ind = torch.where(fallback, fixed, e if e is not None else torch.zeros_like(fixed))
+        if self.vol:
+            # the light the volume reads: the last bounce's (trace.wgsl:296-306 reads the atlas after it)
+            last = torch.sparse.mm(self.write, dl + e) if self.B > 0 else light
+            vy = torch.from_numpy(self.vy)[..., None]
+            vsky = torch.where(torch.from_numpy(self.vsky_down)[..., None], gro.expand(*vy.shape[:2], 3),
+                               hor * (1.0 - vy) + zen * vy)
+            vsky = vsky * torch.from_numpy(self.vsky_up | self.vsky_down)[..., None]
+            vmat = torch.from_numpy(np.where(self.vsurf, self.vmat, 0))
+            vli = torch.from_numpy(np.where(self.vlit, self.vli, 0))
+            vhit = torch.where(torch.from_numpy(self.vlit)[..., None], last[vli], fb.expand(*vli.shape, 3))
+            l = torch.where(torch.from_numpy(self.vsurf)[..., None], al[vmat] / math.pi * vhit, vsky) if M else vsky
+            d = torch.from_numpy(self.vdir)
+            coef = torch.stack([(l * 0.282095).sum(1)] + [(l * 0.488603 * d[..., a:a + 1]).sum(1) for a in range(3)],
+                               dim=1) * self.vw  # (items, 4, 3)
+            probes = torch.zeros((self.n_probes, 4, 3), dtype=torch.float64)
+            probes = probes.index_put((torch.from_numpy(self.vslots),), coef)
+            p = probes.reshape(self.n_probes, 12)
+            for f in self.vfill:
+                p = torch.sparse.mm(f, p)
+            p4 = torch.sparse.mm(self.vinterp, p).reshape(-1, 4, 3)
+            n = torch.from_numpy(self.vnormal)
+            a0, a1 = math.pi * 0.282095, 2.0 * math.pi / 3.0 * 0.488603
+            arg = a0 * p4[:, 0] + a1 * (p4[:, 1] * n[:, 0:1] + p4[:, 2] * n[:, 1:2] + p4[:, 3] * n[:, 2:3])
+            e5 = 0.5 * a0 * p4[:, 0] + 0.5 * torch.relu(arg)
+            ind = ind.index_put((torch.from_numpy(self.f5),), e5)
         return torch.sparse.mm(self.atlas, ind)
 
     def gradient(self, theta: np.ndarray, g_indirect: np.ndarray):

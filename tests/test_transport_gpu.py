@@ -2,7 +2,8 @@
 
 - every recorded gather ray equals the oracle's trace of the same ray (trace.wgsl:245-270), bit for bit;
 - the forward at the scene's own theta is the device bake's indirect atlas, bit for bit, and at edited
-  albedos and sky it is the bake of the edited scene, bit for bit;
+  albedos and sky it is the bake of the edited scene, bit for bit, the texels lit by the volume's
+  fallback included;
 - the gradient equals the float64 restatement's autograd gradient (oracle/transport_ref.py) and central
   differences of the forward (h = 1e-3);
 - fewer checkpoints than bounces (recomputation) give the same bits, and so does a second call.
@@ -19,7 +20,8 @@ from oracle import transport_ref as T
 pytestmark = pytest.mark.gpu
 
 EXPORTS = ["shape", "tiles", "texels", "chart", "gathered", "known", "known_bounce", "state", "direct_light",
-           "fixed_indirect", "owner", "gathered_index", "records", "smooth_weights"]
+           "fixed_indirect", "owner", "gathered_index", "records", "smooth_weights", "sample_points",
+           "volume_grid", "volume_items", "volume_slots", "volume_raw", "volume_records"]
 
 
 @pytest.fixture(scope="module")
@@ -33,6 +35,17 @@ def small(gpu):
 @pytest.fixture(scope="module")
 def reftest(gpu):
     scene = scenes.reference_test()
+    tr = lb.Transport(scene, gpu)
+    yield scene, tr
+    tr.close()
+
+
+@pytest.fixture(scope="module")
+def inside(gpu):
+    """Boxes sunk into each other and into the ground: texels inside solids lit by the volume's fallback, and
+    probes inside solids that the volume's fill gives light."""
+    from edge_scenes import EDGE_SCENES
+    scene = EDGE_SCENES["inside"]()
     tr = lb.Transport(scene, gpu)
     yield scene, tr
     tr.close()
@@ -68,7 +81,7 @@ def test_records_are_the_oracle_rays(which, request):
     assert surf.any() and sky.any()
 
 
-@pytest.mark.parametrize("which", ["small", "reftest"])
+@pytest.mark.parametrize("which", ["small", "reftest", "inside"])
 def test_forward_at_theta0_is_the_bake(which, request, gpu):
     scene, tr = request.getfixturevalue(which)
     got = tr.forward(tr.theta0())
@@ -99,7 +112,48 @@ def test_forward_is_the_bake_of_the_edited_scene(reftest, gpu):
     np.testing.assert_allclose(tr.forward(th2), want, rtol=1e-5, atol=1e-6)
 
 
-@pytest.mark.parametrize("which", ["small", "reftest"])
+@pytest.mark.parametrize("which", ["small", "inside"])
+def test_forward_with_the_volume_is_the_bake_of_the_edited_scene(which, request, gpu):
+    """Texels lit by the volume's fallback (validity 5) take their light from the probes, which the transport
+    evaluates from its last bounce's light and theta, fills and interpolates: at edited albedos and sky the
+    forward is the bake of the edited scene bit for bit, those texels included."""
+    scene, tr = request.getfixturevalue(which)
+    assert (tr.export("state") == 5).sum() > 0 and len(tr.export("volume_grid")) == 10
+    rng = np.random.default_rng(5)
+    th = tr.theta0()
+    M = tr.n_materials
+    th[:3 * M] = rng.uniform(0.1, 0.9, 3 * M).astype(np.float32)
+    th[3 * M:3 * M + 9] = rng.uniform(0.05, 0.6, 9).astype(np.float32)
+    edited = scenes.with_light(scene, albedo=th[:3 * M], zenith=th[3 * M:3 * M + 3], horizon=th[3 * M + 3:3 * M + 6],
+                               ground=th[3 * M + 6:3 * M + 9])
+    want = np.asarray(lb.bake_device(edited, gpu).indirect, np.float32).reshape(tr.ih, tr.iw, 3)
+    got = tr.forward(th)
+    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_fallback_texels_have_a_gradient(inside):
+    """On a scene whose fallback texels are lit through filled probes, the gradient of a loss on the whole
+    atlas (the fallback texels' share reaching the sky and the albedos through the probes) equals central
+    differences of the forward."""
+    scene, tr = inside
+    th = tr.theta0()
+    state = tr.export("state")
+    tr.forward(th)
+    # the composite spreads a texel over its block: weigh the whole atlas, the fallback texels' blocks most
+    g = np.full((tr.ih, tr.iw, 3), 0.1, np.float32)
+    grad = tr.backward(g)
+    M = tr.n_materials
+    h = 1e-3
+    for j in [3 * M, 3 * M + 4, 3 * M + 7, 0, 4]:
+        tp, tm = th.copy(), th.copy()
+        tp[j] += h
+        tm[j] -= h
+        fd = ((tr.forward(tp).astype(np.float64) * g).sum() - (tr.forward(tm).astype(np.float64) * g).sum()) / (2 * h)
+        assert abs(fd - grad[j]) <= 2e-3 * max(abs(grad[j]), 1e-3 * np.abs(grad).max()), (j, fd, grad[j])
+    assert (state == 5).sum() > 0
+
+
+@pytest.mark.parametrize("which", ["small", "reftest", "inside"])
 def test_gradient_is_the_float64_reference(which, request):
     scene, tr = request.getfixturevalue(which)
     ref = T.TransportRef(_arrays(tr))
