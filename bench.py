@@ -578,10 +578,10 @@ def main():
             gj = float(grad[j])
             checks.append({"param": j, "adjoint": gj, "central_difference": float(fd),
                            "rel_err": float(abs(fd - gj) / max(abs(gj), 1e-30))})
-        # texels the volume's fallback lit (validity 5) keep their light at theta0 in the transport: the volume
-        # pass is not differentiated, so their share of d(loss)/d(theta) is left out (weight 1e-3 in a block
-        # that also holds texels with light of their own)
+        # texels the volume's fallback lit (validity 5): the transport carries them through the probes, whose
+        # rays it recorded at create
         fallback_texels = int((tr.export("state") == 5).sum())
+        volume_records = int(len(tr.export("volume_records")))
         tr.close()
         one = lb.Transport(scene, gpu, max_checkpoints=1)
         one.forward_async(th.data_ptr(), out_t.data_ptr())
@@ -595,7 +595,7 @@ def main():
                    "bounces": int(shape.bounces), "params": int(shape.n_params), "records": int(shape.records),
                    "lit_records": int(shape.lit_records),
                    "fallback_texels": fallback_texels,
-                   "volume_records": int(len(tr.export("volume_records"))),
+                   "volume_records": volume_records,
                    "gradient_check": {"loss": "L2 to a target baked at theta0 + N(0, 0.05)", "h": h,
                                       "max_rel_err": max(c["rel_err"] for c in checks), "params": checks},
                    "note": "device time of one forward (theta on the device to the indirect atlas) and one "

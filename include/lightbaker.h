@@ -426,7 +426,8 @@ int lb_transport_bake_indirect(lb_transport *t, float *indirect);
  * (float4 a texel), "gather_out" (the last bounce's gather results), "light" (the last light atlas),
  * "probes"; and the volume's share, empty when no texel takes the fallback: "volume_records",
  * "volume_items", "volume_slots", "volume_raw" (the probes before the fill), "volume_grid"): its size in
- * bytes when out is NULL, else the bytes copied (0 on error). */
+ * bytes when out is NULL, else the bytes copied (0 on error, with lb_last_error set; 0 with it empty: an
+ * empty array). */
 size_t lb_transport_export(lb_transport *t, const char *name, void *out, size_t cap);
 void lb_transport_free(lb_transport *t);
 

@@ -1541,7 +1541,12 @@ int lb_transport_bake_indirect(lb_transport *t, float *indirect) {
 }
 
 size_t lb_transport_export(lb_transport *t, const char *name, void *out, size_t cap) {
-    if (!t || !name) return 0;
+    // an empty array returns 0 too: the error text tells the two apart, so none is left from an earlier call
+    lb_set_error("");
+    if (!t || !name) {
+        lb_set_error("lb_transport_export: bad arguments");
+        return 0;
+    }
     lb_plan &p = *t->plan;
     const void *src = nullptr;
     size_t bytes = 0;
