@@ -93,46 +93,35 @@ __device__ __forceinline__ Item load_item(const float4 *tex, const uint32_t *idx
     return it;
 }
 
-// trace.wgsl:159-168 with lanes 0..15 each tracing one of the 16 rays; true on every lane when more than
-// insideShare of them meet back faces. The count of back faces is exact, as the shader's float sum of ones.
+// One ray of an inside test (trace.wgsl:159-168): ray r of the 16 from o about the normal n, and whether
+// it meets a back face. Over the texel's leaf list when o may use it (`listed`; the ray starts within
+// `shift` of the list's centre, heads into the same hemisphere and reaches no farther than the list),
+// else the tree walk. Per lane: the two halves of a warp may test two points.
 template <int BVH, bool COUNT, bool WT>
-__device__ __forceinline__ bool inside_warp(const Scene &S, const lb_params &P, uint32_t seed, float3 o, float3 n,
-                                            uint32_t key, int lane, Count &c) {
-    bool back = false;
-    if (lane < 16) {
-        Frame f = frame(n);
-        uint32_t r = uint32_t(lane);
-        float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
-        Hit h = walk<BVH, COUNT, WT>(S, o, d, P.ground[3], false, key + r + 7000u, seed, c);
-        back = h.tri != NONE && h.back;
-    }
-    float nb = __uint2float_rn(__popc(__ballot_sync(FULL, back)));
-    return nb / 16.0f > __uint_as_float(P.atlas[3]);
-}
-
-// The same test over the texel's leaf list (a list that holds every leaf the test's rays can meet: they
-// start within `shift` of its centre, head into the same hemisphere and reach no farther than the list).
-template <bool COUNT, bool WT>
-__device__ __forceinline__ bool inside_list(const Scene &S, const lb_params &P, uint32_t seed, const uint32_t *list,
-                                            const float *dist2, int nl, float3 o, float3 n, uint32_t key, int lane,
-                                            Count &c, float shift) {
-    bool back = false;
-    if (lane < 16) {
-        Frame f = frame(n);
-        uint32_t r = uint32_t(lane);
-        float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
+__device__ __forceinline__ bool inside_ray(const Scene &S, const lb_params &P, uint32_t seed, const uint32_t *list,
+                                           const float *dist2, int nl, bool listed, float shift, float3 o, float3 n,
+                                           uint32_t key, uint32_t r, Count &c) {
+    Frame f = frame(n);
+    float3 d = cosine((__uint2float_rn(r) + 0.5f) / 16.0f, radical(r), f);
+    Hit h;
+    if (listed) {
         bool tie;
-        Hit h = trace_list_t<COUNT, WT, TIE_INSIDE>(S, list, dist2, nl, o, d, P.ground[3], key + r + 7000u, seed, c,
-                                                    shift, tie);
+        h = trace_list_t<COUNT, WT, TIE_INSIDE>(S, list, dist2, nl, o, d, P.ground[3], key + r + 7000u, seed, c,
+                                                shift, tie);
         if (tie) {
             // nearly coincident faces: the tree walk's own order decides which is the hit (and its face)
             c.rays--;
             h = walk_apart<COUNT, WT>(S, o, d, P.ground[3], key + r + 7000u, seed, c);
         }
-        back = h.tri != NONE && h.back;
+    } else {
+        h = walk<BVH, COUNT, WT>(S, o, d, P.ground[3], false, key + r + 7000u, seed, c);
     }
-    float nb = __uint2float_rn(__popc(__ballot_sync(FULL, back)));
-    return nb / 16.0f > __uint_as_float(P.atlas[3]);
+    return h.tri != NONE && h.back;
+}
+// The test's verdict from the count of its 16 rays that met back faces: more than insideShare of them.
+// The count is exact, as the shader's float sum of ones.
+__device__ __forceinline__ bool inside_of(const lb_params &P, unsigned backs) {
+    return __uint2float_rn(__popc(backs)) / 16.0f > __uint_as_float(P.atlas[3]);
 }
 
 // The item a warp takes next. With a work counter (zeroed before the launch) every warp takes the next item
@@ -235,23 +224,34 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
             shift = sqrtf(dot3(v, v)) * 1.001f + 1e-6f;
             return nl >= 0 && dot3(v, nrm) >= front;
         };
-        auto inside_at = [&](float3 o, uint32_t k) -> bool {
-            float shift;
-            if (listed_from(o, shift))
-                return inside_list<COUNT, WT>(S, P, seed, s_list[wi], s_dist[wi], nl, o, nrm, k, lane, c, shift);
-            return inside_warp<BVH, COUNT, WT>(S, P, seed, o, nrm, k, lane, c);
-        };
         // trace.wgsl:186-210: the texel's own point, then (when it is inside) the candidates 1..8 and the
-        // pushed point 9 in order, until one is not inside; one call site, so the walks are inlined once
+        // pushed point 9 in order, until one is not inside. Points are tested two at a time, lanes 0..15
+        // the first, 16..31 the next (a half warp is all one test takes): the first point not inside is the
+        // sequential loop's, and a second point's test past it is not counted as traced. With COUNT one
+        // point at a time (exact node and triangle counts). One call site, so the walks are inlined once.
+        constexpr uint32_t STEP = COUNT ? 1u : 2u;
 #pragma unroll 1
-        for (uint32_t q = 0u; q <= 9u; q++) {
-            const float3 p = q == 0u ? pos : candidate(q);
-            const bool in = inside_at(add(p, lift), q == 0u ? key : (q == 9u ? key + 331u : key + q * 31u));
-            if (q == 0u) {
-                if (!in) break;
-            } else if (!in) {
-                at = p;
-                pick = q;
+        for (uint32_t q = 0u; q <= 9u; q += STEP) {
+            const uint32_t mine = q + (STEP == 2u ? uint32_t(lane >> 4) : 0u);
+            bool back = false;
+            if ((STEP == 2u || lane < 16) && mine <= 9u) {
+                const float3 o = add(mine == 0u ? pos : candidate(mine), lift);
+                const uint32_t k = mine == 0u ? key : (mine == 9u ? key + 331u : key + mine * 31u);
+                float shift;
+                const bool lst = listed_from(o, shift);
+                back = inside_ray<BVH, COUNT, WT>(S, P, seed, s_list[wi], s_dist[wi], nl, lst, shift, o, nrm, k,
+                                                  uint32_t(lane & 15), c);
+            }
+            const unsigned m = __ballot_sync(FULL, back);
+            const bool in0 = inside_of(P, m & 0xffffu);
+            const bool in1 = inside_of(P, m >> 16);
+            // the point that is not inside, if any (10: both are)
+            const uint32_t out = !in0 ? q : (STEP == 2u && q + 1u <= 9u && !in1 ? q + 1u : 10u);
+            if (STEP == 2u && out == q && q + 1u <= 9u && lane >= 16) c.rays--;
+            if (out == 0u) break;
+            if (out <= 9u) {
+                at = candidate(out);
+                pick = out;
                 span = 0.4f;
                 break;
             }
