@@ -260,14 +260,18 @@ __device__ __forceinline__ float min3(float a, float b, float c) {
 }
 
 // trace.wgsl:74-80; the watertight walks (WT) scale the exit distance by `grow`
+// `skip` > 0: a box the ray leaves before skip counts as missed (for a caller that knows no hit lies
+// that close).
 template <bool WT = false>
-__device__ __forceinline__ float box(float3 o, float3 inv, float4 mn, float4 mx, float tmax, float grow = 1.0f) {
+__device__ __forceinline__ float box(float3 o, float3 inv, float4 mn, float4 mx, float tmax, float grow = 1.0f,
+                                     float skip = 0.0f) {
     float ax = (mn.x - o.x) * inv.x, ay = (mn.y - o.y) * inv.y, az = (mn.z - o.z) * inv.z;
     float bx = (mx.x - o.x) * inv.x, by = (mx.y - o.y) * inv.y, bz = (mx.z - o.z) * inv.z;
     float lo = max3(fminf(ax, bx), fminf(ay, by), fminf(az, bz));
     float hi = min3(fmaxf(ax, bx), fmaxf(ay, by), fmaxf(az, bz));
     if (WT) hi = hi * grow;
     float l0 = fmaxf(lo, 0.0f);
+    if (skip > 0.0f && hi < skip) return FAR;
     return (hi >= l0 && lo < tmax) ? l0 : FAR;
 }
 
@@ -275,10 +279,13 @@ __device__ __forceinline__ float box(float3 o, float3 inv, float4 mn, float4 mx,
 // a 48-entry stack; a far child that finds it full is dropped as in the shader. Child records are
 // carried into the next step instead of being read again; a popped node is read once. The root's box
 // is never tested (the shader starts at its children). An inner node whose children lie past the
-// array ends the walk (the reference's one-node BVH of an empty scene).
+// array ends the walk (the reference's one-node BVH of an empty scene). skip > 0 passes over the boxes the
+// ray leaves before skip: for a ray known to have no accepted hit that close, in a tree no deeper than the
+// stack (so no child is ever dropped), the walk opens the same other boxes in the same order and holds the
+// same hits, so it returns the full walk's hit.
 template <bool COUNT, bool WT>
 __device__ __forceinline__ Hit trace_t(const Scene &S, float3 o, float3 d, float tmax, bool any, uint32_t ray,
-                                       uint32_t seed, Count &c) {
+                                       uint32_t seed, Count &c, float skip = 0.0f) {
     Hit hit{tmax, NONE, false};
     c.rays++;
     if (COUNT) c.nodes++;
@@ -307,8 +314,8 @@ __device__ __forceinline__ Hit trace_t(const Scene &S, float3 o, float3 d, float
             if (COUNT) c.nodes += 2;
             float4 alo = __ldg(&S.nodes[2 * first]), ahi = __ldg(&S.nodes[2 * first + 1]);
             float4 blo = __ldg(&S.nodes[2 * first + 2]), bhi = __ldg(&S.nodes[2 * first + 3]);
-            float ta = box<WT>(o, inv, alo, ahi, hit.t, S.grow);
-            float tb = box<WT>(o, inv, blo, bhi, hit.t, S.grow);
+            float ta = box<WT>(o, inv, alo, ahi, hit.t, S.grow, skip);
+            float tb = box<WT>(o, inv, blo, bhi, hit.t, S.grow, skip);
             bool a_near = ta <= tb;
             float tn = fminf(ta, tb), tf = fmaxf(ta, tb);
             if (tn < FAR) {
@@ -839,9 +846,9 @@ __device__ __forceinline__ Hit trace8_t(const Scene &S, float3 o, float3 d, floa
 // (the kernels are built for both and the launch picks by whether the scene has vertices).
 template <int BVH, bool COUNT, bool WT = false>
 __device__ __forceinline__ Hit walk(const Scene &S, float3 o, float3 d, float tmax, bool any, uint32_t ray,
-                                    uint32_t seed, Count &c) {
+                                    uint32_t seed, Count &c, float skip = 0.0f) {
     if (BVH == 8) return trace8_t<COUNT, WT>(S, o, d, tmax, any, ray, seed, c);
-    return trace_t<COUNT, WT>(S, o, d, tmax, any, ray, seed, c);
+    return trace_t<COUNT, WT>(S, o, d, tmax, any, ray, seed, c, skip);
 }
 // The BVH2 walk for the rare ray a leaf list leaves to the tree (a near tie), as a call: one copy of the
 // walk serves every such site instead of a copy inlined at each.

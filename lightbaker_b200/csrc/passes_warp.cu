@@ -453,6 +453,9 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) direct_warp(Scene S,
 // Gather rays that find a hit this close are resolved by the texel's leaf list (WALK 1); the others walk
 // the tree. A speed parameter only: either way a ray gets the tree walk's hit.
 constexpr float GATHER_NEAR = 2.0f;
+// a queued gather ray's flag: its list walk met no accepted triangle
+constexpr uint32_t PEND_MISSED = 0x8000u;
+static_assert(GI_CAP <= int(PEND_MISSED), "ray indices leave the flag bit free");
 
 // trace.wgsl:245-270. rec (optional): each ray's outcome ([item][ray], gather_record) for later bounces.
 // WALK 1 (BVH2): the warp gathers the leaves within GATHER_NEAR (widened by the jitter's reach) of the
@@ -532,7 +535,7 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) gather_warp(
                 const uint32_t r = ord.ray(r0 >> 5);
                 float3 o, d;
                 ray_of(r, o, d);
-                bool done = false;
+                bool done = false, missed = false;
                 const float3 v = sub(o, c0);
                 if (nl >= 0 && dot3(v, nrm) >= front) {
                     const float shift = sqrtf(dot3(v, v)) * 1.001f + 1e-6f;
@@ -544,20 +547,27 @@ __global__ void __launch_bounds__(256, (OCC < 2 ? 2 : OCC)) gather_warp(
                         finish(r, o, d, h, myback);
                     } else {
                         c.rays--;  // the tree walk counts it
+                        missed = h.tri == NONE;
                     }
                 }
                 const unsigned pm = __ballot_sync(FULL, !done);
-                if (!done) s_pend[lw][npend + __popc(pm & below)] = uint16_t(r);
+                if (!done) s_pend[lw][npend + __popc(pm & below)] = uint16_t(r | (missed ? PEND_MISSED : 0u));
                 npend += __popc(pm);
             }
+            // A ray whose list walk met no accepted triangle before rnear has none there at all (every
+            // triangle it could meet that close lies in the list), so its tree walk passes over the boxes
+            // it leaves before rnear, less a margin (1 %) far above the rounding of t and of the box test. Not
+            // when counting (the reference walk's node counts), nor in a tree deeper than the walk's stack.
+            const float skip = (!COUNT && S.depth <= uint32_t(STACK)) ? rnear * 0.99f - 1e-4f : 0.0f;
             __syncwarp();
             for (uint32_t b0 = 0; b0 < npend; b0 += 32) {
                 const uint32_t i = b0 + uint32_t(lane);
                 if (i < npend) {
-                    const uint32_t r = s_pend[lw][i];
+                    const uint32_t e = s_pend[lw][i], r = e & ~PEND_MISSED;
                     float3 o, d;
                     ray_of(r, o, d);
-                    Hit h = walk<BVH, COUNT, WT>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c);
+                    Hit h = walk<BVH, COUNT, WT>(S, o, d, P.reach[1], false, key + r + 4000u, seed, c,
+                                                 (e & PEND_MISSED) ? skip : 0.0f);
                     finish(r, o, d, h, myback);
                 }
             }
