@@ -618,8 +618,8 @@ def main():
         if ks["alg_bytes"] is None:
             ks["alg_bytes"], alg_src = ks["kernel_fetch_bytes"], "the kernel's own fetches (no frozen count)"
         achieved = ks["alg_bytes"] / (ks["ms"] / 1e3) / 1e9
-        # DRAM bytes a launch from an ncu capture (profiles/traffic.txt: workload kernel bytes source)
-        # (profiles/traffic.txt: workload kernel dram_bytes l2_bytes simt_efficiency source, a full launch each)
+        # DRAM and L2 bytes a launch from an ncu capture (profiles/traffic.txt: workload kernel dram_bytes
+        # l2_bytes simt_efficiency source, a full launch each)
         traffic, traffic_src, l2_bytes, simt = None, None, None, None
         tfile = ROOT / "profiles" / "traffic.txt"
         if tfile.exists():
