@@ -10,8 +10,9 @@ the fallback and the atlas composite: the device-resident bake's CUDA graph, inp
 memory. `value` = the rays of a step (counted on the device) / the step's time (CUDA events on the
 library's stream; L2 flushed before every step by writing 256 MB). `e2e` times the same bake through
 the C ABI from the scene file's bytes in host memory to the atlases in host memory (the host's layout,
-BVH and texels included; the median of three calls after an untimed first, each call's time listed). `plain` is the drop-in bake (the reference's structure: a pass, a host round
-trip, the host's texel passes) for the batched-vs-plain ratio. Under torchrun each rank bakes its own
+BVH and texels included; the median of three calls after an untimed first, each call's time listed).
+`plain` is the drop-in bake (the reference's structure: a pass, a host round trip, the host's texel
+passes) for the batched-vs-plain ratio. Under torchrun each rank bakes its own
 map (seed = rank): weak scaling, no collective on the data path; times are the max over ranks.
 
 --impl reference times the CPU restatement of the same passes (the oracle, OpenMP on every host core)
@@ -489,7 +490,7 @@ def main():
     # ---- end to end through the C ABI: scene bytes in host memory to atlases in host memory ----
     # (one call, as a user bakes a map once: no autotuning, the library's default shapes)
     gpu.transfer(reset=True)
-    e2e_ms, bake_seconds = [], []
+    e2e_ms, bake_seconds, e2e_parts = [], [], []
     e2e_log = []
     for i in range(args.e2e_steps + 1):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -508,6 +509,8 @@ def main():
         e2e_ms.append(e0.elapsed_time(e1))
         bake_seconds.append(wall)
         e2e_stats = b.stats
+        # where each call's time went: the library's host build and its collection (device and results)
+        e2e_parts.append([round(wall, 4), round(b.stats.t_layout, 4), round(b.stats.t_composite, 4)])
         b.close()
     h2d, d2h = gpu.transfer()
     # the median call (a call a step, after an untimed first one): the bake's host side shares the box's
@@ -668,6 +671,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "Grays/s", "h2d_bytes_per_step": h2d // max(1, args.e2e_steps),
                     "d2h_bytes_per_step": d2h // max(1, args.e2e_steps), "bake_seconds": e2e_t / 1e3,
                     "calls_s": [round(t / 1e3, 4) for t in e2e_ms], "of_calls": "median",
+                    "calls_wall_build_collect_s": e2e_parts,
                     "host_prepare_s": e2e_stats.t_layout, "collect_s": e2e_stats.t_composite,
                     "stages": [l for l in e2e_log if l.startswith("timing")],
                     "path": "lb_bake_device: scene bytes in, atlases out, one call, default shapes (no autotune)"},
