@@ -74,5 +74,6 @@ void lb_collect_counters(lb_gpu *g);
 // its size in *cap, or nullptr.
 void *lb_spare_take(lb_gpu *g, size_t bytes, size_t *cap);
 // Gives a buffer back to the handle's spares once the handle's stream has finished with it (it is
-// synchronised here), or frees it when the spares already hold their limit.
+// synchronised here); when the spares would pass their limit the oldest are freed first (a buffer larger
+// than the whole limit is freed at once).
 void lb_spare_give(lb_gpu *g, void *p, size_t cap);

@@ -89,23 +89,33 @@ void *lb_spare_take(lb_gpu *g, size_t bytes, size_t *cap) {
     void *p = g->spare[best].first;
     *cap = g->spare[best].second;
     g->spare_bytes -= *cap;
-    g->spare[best] = g->spare.back();
-    g->spare.pop_back();
+    g->spare.erase(g->spare.begin() + std::ptrdiff_t(best));  // the others keep their order, oldest first
     return p;
 }
 
 void lb_spare_give(lb_gpu *g, void *p, size_t cap) {
     if (!p) return;
     cudaStreamSynchronize(g->stream);
+    if (cap > SPARE_LIMIT) {
+        cudaFree(p);
+        return;
+    }
+    // the newest buffer stays and the oldest spares go when the limit would be passed: a caller that bakes
+    // again and again keeps its own buffers, whatever other work left spares before
+    std::vector<void *> out;
     {
         std::lock_guard<std::mutex> lock(g->spare_mu);
-        if (g->spare_bytes + cap <= SPARE_LIMIT) {
-            g->spare.emplace_back(p, cap);
-            g->spare_bytes += cap;
-            return;
+        size_t k = 0;
+        while (g->spare_bytes + cap > SPARE_LIMIT && k < g->spare.size()) {
+            out.push_back(g->spare[k].first);
+            g->spare_bytes -= g->spare[k].second;
+            k++;
         }
+        g->spare.erase(g->spare.begin(), g->spare.begin() + std::ptrdiff_t(k));
+        g->spare.emplace_back(p, cap);
+        g->spare_bytes += cap;
     }
-    cudaFree(p);
+    for (void *q : out) cudaFree(q);
 }
 
 extern "C" {
