@@ -187,8 +187,8 @@ int lb_set_near(lb_gpu *gpu, int on);
 /* Register cap of the warp kernels over the BVH2 (direct and gather, without counting): 0 (default) the
  * compiler's own budget; 3 or 4 registers capped so that this many 256-thread blocks share an SM (more
  * warps in flight, some values spilled). Same results. With 0, lb_bake_device and lb_plan_create without
- * autotuning use their own shapes: the 3-block cap for both passes, without the shared sun walk
- * (lb_set_warp_walk) for the direct pass; with 3 or 4 they use the handle's cap and walk. */
+ * autotuning use their own shapes: the 4-block cap without the shared sun walk (lb_set_warp_walk) for the
+ * direct pass, the 3-block cap for the gathers; with 3 or 4 they use the handle's cap and walk. */
 int lb_set_register_cap(lb_gpu *gpu, int blocks);
 /* Lane refill in the warp kernels' occlusion and gather rays over the BVH2 (default off): a lane whose
  * ray has ended starts the item's next one instead of waiting for its round. Same results. */

@@ -842,10 +842,11 @@ lb_plan *create_plan(lb_gpu *g, const uint8_t *scene, size_t len, const lb_bake_
         p->near_direct = p->near_gather = g->near;
         p->fetch_direct = p->fetch_gather = g->fetch;
         p->warp_walk = g->warp_walk;
-        // untuned shapes: with no register cap set on the handle, both passes run the 3-block cap and the
-        // direct pass without the sun rays' shared walk (the autotuner's usual pick on map_100m, where the
-        // leaf lists fit; the compiler's budget with the shared walk was 345 ms a step against 325)
-        p->occ_direct = g->occ ? g->occ : 3;
+        // untuned shapes: with no register cap set on the handle, the direct pass runs the 4-block cap
+        // without the sun rays' shared walk and the gathers the 3-block cap (on map_100m's whole direct pass
+        // the 4-block cap takes 219 ms against 225 for the 3-block one; the compiler's budget with the
+        // shared walk made the step 345 ms against 325)
+        p->occ_direct = g->occ ? g->occ : 4;
         p->occ_gather = g->occ ? g->occ : 3;
         if (!g->occ) p->warp_walk = 0;
         auto t0 = std::chrono::steady_clock::now();
